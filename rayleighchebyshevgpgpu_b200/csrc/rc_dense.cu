@@ -1,0 +1,717 @@
+// rc_dense.cu -- FP64 (c128) dense kernels of the orthonormalisation and Rayleigh-Ritz steps.
+//
+//  gram      C = X^H Y for tall-skinny n x m and n x nc blocks: split over row chunks, each
+//            CTA accumulates a 64x64 output tile in registers from shared-memory K-tiles,
+//            partial tiles are summed by a second kernel in a fixed order (deterministic).
+//            Replaces cublas{D,Z}gemm(OP_T/OP_C, OP_N) (RayleighChebyshevLMCuda.h:2139-2161).
+//  xt        Y = beta*Y + X*T for tall-skinny X and a small T, optionally a second pair
+//            (W*Q next to V*Q) with the residual ||W_c - lam_c V_c||^2 reduced in the epilogue.
+//            Replaces cublas{D,Z}gemm(OP_N,OP_N) + normalize + memcpy + the second SpMM +
+//            the residuals kernel (RayleighChebyshevLMCuda.h:2178-2285, cuda_kernels.cu:307-382).
+//  chol      Cholesky of a column-scaled Gram matrix and the inverse of its factor (one CTA);
+//            with xt it forms CholeskyQR, replacing cusolverDn geqrf+orgqr (:1979-2107).
+//  eigh      one-CTA parallel cyclic Jacobi for a small Hermitian matrix, replacing host
+//            DSYEV/ZHPEVX (:570-642) and JacobiDiagonalizer.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <string>
+#include "rc_common.cuh"
+#include "rc_internal.h"
+
+namespace rcb {
+
+constexpr int TB = 64;   // output tile edge
+constexpr int KT = 16;   // K-tile depth
+constexpr int TPB = 256; // 16 x 16 threads, 4 x 4 outputs each
+
+template <class T> struct Sel;
+template <> struct Sel<double> { static constexpr int dt = RC_REAL64; };
+template <> struct Sel<double2> { static constexpr int dt = RC_COMPLEX128; };
+
+// ---------------------------------------------------------------------------------------
+// Gram: partial[chunk] (m x nc, ld m) = X[rows of chunk]^H * Y[rows of chunk]
+// grid: (nchunks, tiles_m, tiles_n); block 256.
+// thread (tx,ty): output rows mi = m0 + tx + 16*i, cols nj = n0 + ty + 16*j.
+// ---------------------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(TPB)
+gram_partial_kernel(int64_t n, int64_t m, int64_t nc, const T* __restrict__ X, int64_t ldx, const T* __restrict__ Y,
+                    int64_t ldy, T* __restrict__ part, int64_t rows_per_chunk, int upper) {
+    const int tm = blockIdx.y, tn = blockIdx.z;
+    if (upper && tm > tn) return;
+    const int64_t m0 = (int64_t)tm * TB, n0 = (int64_t)tn * TB;
+    const int64_t r_begin = (int64_t)blockIdx.x * rows_per_chunk;
+    const int64_t r_end = min(n, r_begin + rows_per_chunk);
+    __shared__ T Xs[KT][TB + 1];
+    __shared__ T Ys[KT][TB + 1];
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    T acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = s_zero(T());
+    for (int64_t r0 = r_begin; r0 < r_end; r0 += KT) {
+        // load KT x 64 of X and Y; element e: kk = e % KT (row), cc = e / KT (column)
+#pragma unroll
+        for (int it = 0; it < (KT * TB) / TPB; ++it) {
+            const int e = tid + it * TPB;
+            const int kk = e % KT, cc = e / KT;
+            const int64_t r = r0 + kk;
+            const int64_t cx = m0 + cc, cy = n0 + cc;
+            Xs[kk][cc] = (r < r_end && cx < m) ? X[r + cx * ldx] : s_zero(T());
+            Ys[kk][cc] = (r < r_end && cy < nc) ? Y[r + cy * ldy] : s_zero(T());
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < KT; ++kk) {
+            T a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = Xs[kk][tx + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Ys[kk][ty + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = s_cfma(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+    T* P = part + (size_t)blockIdx.x * m * nc;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int64_t mi = m0 + tx + 16 * i, nj = n0 + ty + 16 * j;
+            if (mi < m && nj < nc) P[mi + nj * m] = acc[i][j];
+        }
+}
+
+// C[i,j] = sum over chunks; upper: use i<=j and mirror (Hermitian, real diagonal).
+template <class T>
+__global__ void gram_reduce_kernel(int64_t m, int64_t nc, int64_t nchunks, const T* __restrict__ part, T* __restrict__ C,
+                                   int upper) {
+    const int64_t total = m * nc;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e % m, j = e / m;
+        if (upper && i > j) continue;
+        T sum = s_zero(T());
+        for (int64_t c = 0; c < nchunks; ++c) sum = s_add(sum, part[(size_t)c * total + e]);
+        if (upper) {
+            if (i == j) {
+                sum = s_from<T>(s_real(sum), 0.0);
+                C[e] = sum;
+            } else {
+                C[e] = sum;
+                C[j + i * m] = s_conj(sum);
+            }
+        } else {
+            C[e] = sum;
+        }
+    }
+}
+
+template <class T>
+static rc_status gram_t(rc_ctx* ctx, int64_t n, int64_t m, int64_t nc, const T* X, int64_t ldx, const T* Y,
+                        int64_t ldy, T* C, bool upper) {
+    const int tiles_m = (int)((m + TB - 1) / TB), tiles_n = (int)((nc + TB - 1) / TB);
+    const int tiles = upper ? tiles_m * (tiles_m + 1) / 2 : tiles_m * tiles_n;
+    // about 4 CTAs per SM in total, each chunk a multiple of KT rows
+    int64_t nchunks = (4 * ctx->sm_count + tiles - 1) / tiles;
+    int64_t rows = (n + nchunks - 1) / nchunks;
+    rows = ((rows + KT - 1) / KT) * KT;
+    if (rows < KT) rows = KT;
+    nchunks = (n + rows - 1) / rows;
+    if (nchunks < 1) nchunks = 1;
+    void* part = nullptr;
+    RC_TRY(rc_slot(ctx, S_PART, (size_t)nchunks * m * nc * sizeof(T), &part));
+    dim3 grid((unsigned)nchunks, tiles_m, tiles_n);
+    gram_partial_kernel<T><<<grid, TPB, 0, ctx->stream>>>(n, m, nc, X, ldx, Y, ldy, (T*)part, rows, upper ? 1 : 0);
+    ctx->launches++;
+    RC_CU(ctx, cudaGetLastError());
+    const int64_t total = m * nc;
+    const unsigned g2 = (unsigned)std::min<int64_t>((total + 255) / 256, 4 * 148);
+    gram_reduce_kernel<T><<<g2, 256, 0, ctx->stream>>>(m, nc, nchunks, (const T*)part, C, upper ? 1 : 0);
+    ctx->launches++;
+    RC_CU(ctx, cudaGetLastError());
+    return RC_OK;
+}
+
+rc_status gram(rc_ctx* ctx, int dtype, int64_t n, int64_t m, int64_t nc, const void* X, int64_t ldx, const void* Y,
+               int64_t ldy, void* C, bool upper) {
+    if (m <= 0 || nc <= 0) return RC_OK;
+    if (upper && m != nc) return rc_fail(ctx, RC_ERR_INVALID, "gram: upper requires a square result");
+    if (dtype == RC_COMPLEX128)
+        return gram_t<double2>(ctx, n, m, nc, (const double2*)X, ldx, (const double2*)Y, ldy, (double2*)C, upper);
+    return gram_t<double>(ctx, n, m, nc, (const double*)X, ldx, (const double*)Y, ldy, (double*)C, upper);
+}
+
+// ---------------------------------------------------------------------------------------
+// XT: Y = beta*Y + X*T  (X: n x k, T: k x nc, Y: n x nc), optional dual + residuals.
+// grid: (ceil(n/64), ceil(nc/64)); thread (tx,ty): rows r0 + tx + 16 i, cols c0 + ty + 16 j.
+// ---------------------------------------------------------------------------------------
+template <class T, bool DUAL>
+__global__ void __launch_bounds__(TPB)
+xt_kernel(int64_t n, int64_t k, int64_t nc, const T* __restrict__ X, int64_t ldx, const T* __restrict__ Tm,
+          int64_t ldt, T* __restrict__ Y, int64_t ldy, double alpha, double beta, const T* __restrict__ X2, int64_t ldx2,
+          T* __restrict__ Y2, int64_t ldy2, const double* __restrict__ lam, int64_t res_count,
+          double* __restrict__ rpart) {
+    constexpr int KX = IsComplex<T>::value ? 8 : 16;  // K-tile depth (complex: 48 KB static smem limit)
+    const int64_t r0 = (int64_t)blockIdx.x * TB, c0 = (int64_t)blockIdx.y * TB;
+    __shared__ T Xs[KX][TB + 1];
+    __shared__ T X2s[DUAL ? KX : 1][TB + 1];
+    __shared__ T Ts[KX][TB + 1];
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    T acc[4][4], acc2[DUAL ? 4 : 1][DUAL ? 4 : 1];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = s_zero(T());
+    if (DUAL) {
+#pragma unroll
+        for (int i = 0; i < (DUAL ? 4 : 1); ++i)
+#pragma unroll
+            for (int j = 0; j < (DUAL ? 4 : 1); ++j) acc2[i][j] = s_zero(T());
+    }
+    for (int64_t k0 = 0; k0 < k; k0 += KX) {
+        // X tile: 64 rows x KX cols; element e: rr = e % 64 (row), kk = e / 64
+#pragma unroll
+        for (int it = 0; it < (KX * TB) / TPB; ++it) {
+            const int e = tid + it * TPB;
+            const int rr = e % TB, kk = e / TB;
+            const int64_t r = r0 + rr, kc = k0 + kk;
+            const bool ok = r < n && kc < k;
+            Xs[kk][rr] = ok ? X[r + kc * ldx] : s_zero(T());
+            if (DUAL) X2s[kk][rr] = ok ? X2[r + kc * ldx2] : s_zero(T());
+        }
+        // T tile: KX rows x 64 cols; element e: kk = e % KX, cc = e / KX
+#pragma unroll
+        for (int it = 0; it < (KX * TB) / TPB; ++it) {
+            const int e = tid + it * TPB;
+            const int kk = e % KX, cc = e / KX;
+            const int64_t kr = k0 + kk, c = c0 + cc;
+            Ts[kk][cc] = (kr < k && c < nc) ? Tm[kr + c * ldt] : s_zero(T());
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < KX; ++kk) {
+            T a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = Xs[kk][tx + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Ts[kk][ty + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = s_fma(a[i], b[j], acc[i][j]);
+            if (DUAL) {
+                T a2[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) a2[i] = X2s[kk][tx + 16 * i];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc2[i % (DUAL ? 4 : 1)][j % (DUAL ? 4 : 1)] =
+                        s_fma(a2[i], b[j], acc2[i % (DUAL ? 4 : 1)][j % (DUAL ? 4 : 1)]);
+            }
+        }
+        __syncthreads();
+    }
+    // epilogue
+    double rs[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int64_t c = c0 + ty + 16 * j;
+        const double lc = (DUAL && lam && c < res_count) ? lam[c] : 0.0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int64_t r = r0 + tx + 16 * i;
+            if (r < n && c < nc) {
+                T v = alpha == 1.0 ? acc[i][j] : s_rscale(alpha, acc[i][j]);
+                if (beta != 0.0) v = s_add(v, s_rscale(beta, Y[r + c * ldy]));
+                Y[r + c * ldy] = v;
+                if (DUAL) {
+                    const T w = acc2[i % (DUAL ? 4 : 1)][j % (DUAL ? 4 : 1)];
+                    Y2[r + c * ldy2] = w;
+                    if (lam && c < res_count) rs[j] += s_abs2(s_sub(w, s_rscale(lc, v)));
+                }
+            }
+        }
+    }
+    if (DUAL && lam) {
+        // reduce over tx (16 lanes of a half-warp share ty)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            double v = rs[j];
+#pragma unroll
+            for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            const int64_t c = c0 + ty + 16 * j;
+            if (tx == 0 && c < res_count) rpart[(size_t)blockIdx.x * res_count + c] = v;
+        }
+    }
+}
+
+__global__ void resid_reduce_kernel(int64_t nblocks, int64_t res_count, const double* __restrict__ rpart,
+                                    double* __restrict__ res) {
+    const int c = blockIdx.x;
+    __shared__ double sc[32];
+    double v = 0.0;
+    for (int64_t b = threadIdx.x; b < nblocks; b += blockDim.x) v += rpart[(size_t)b * res_count + c];
+    v = block_sum(v, sc);
+    if (threadIdx.x == 0) res[c] = sqrt(v);
+}
+
+template <class T>
+static rc_status xt_t(rc_ctx* ctx, const XtArgs& a) {
+    const unsigned gx = (unsigned)((a.n + TB - 1) / TB), gy = (unsigned)((a.nc + TB - 1) / TB);
+    dim3 grid(gx, gy);
+    const bool dual = a.X2 != nullptr;
+    double* rpart = nullptr;
+    if (dual && a.lam && a.res_count > 0) {
+        void* p = nullptr;
+        RC_TRY(rc_slot(ctx, S_RPART, (size_t)gx * a.res_count * sizeof(double), &p));
+        rpart = (double*)p;
+    }
+    if (dual)
+        xt_kernel<T, true><<<grid, TPB, 0, ctx->stream>>>(
+            a.n, a.k, a.nc, (const T*)a.X, a.ldx, (const T*)a.T, a.ldt, (T*)a.Y, a.ldy, a.alpha, a.beta, (const T*)a.X2,
+            a.ldx2, (T*)a.Y2, a.ldy2, rpart ? a.lam : nullptr, a.res_count, rpart);
+    else
+        xt_kernel<T, false><<<grid, TPB, 0, ctx->stream>>>(a.n, a.k, a.nc, (const T*)a.X, a.ldx, (const T*)a.T,
+                                                           a.ldt, (T*)a.Y, a.ldy, a.alpha, a.beta, nullptr, 0, nullptr, 0,
+                                                           nullptr, 0, nullptr);
+    ctx->launches++;
+    RC_CU(ctx, cudaGetLastError());
+    if (rpart) {
+        resid_reduce_kernel<<<(unsigned)a.res_count, 256, 0, ctx->stream>>>(gx, a.res_count, rpart, a.res);
+        ctx->launches++;
+        RC_CU(ctx, cudaGetLastError());
+    }
+    return RC_OK;
+}
+
+rc_status xt(rc_ctx* ctx, int dtype, const XtArgs& a) {
+    if (a.n <= 0 || a.nc <= 0) return RC_OK;
+    return dtype == RC_COMPLEX128 ? xt_t<double2>(ctx, a) : xt_t<double>(ctx, a);
+}
+
+// ---------------------------------------------------------------------------------------
+// Cholesky factor of the column-scaled Gram matrix (one CTA, 1024 threads).
+//   d_i = sqrt(G_ii), Gh = D^-1 G D^-1 (+ sigma I on breakdown), Gh = R^H R (R upper),
+//   Tout = D^-1 R^-1 so that V*Tout has orthonormal columns.
+// The working matrix lives in global scratch M (s x s) which stays L2-resident.
+// flags[0] |= 1 if shifted, flags[1] = 1 if failed, flags[2] = 1 if a zero column was met.
+// ---------------------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(1024)
+chol_factor_kernel(int s, int64_t nrows, const T* __restrict__ G, T* M, T* __restrict__ Tout, double* dsc,
+                   int* flags) {
+    __shared__ int s_bad;
+    __shared__ double s_piv;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int i = tid; i < s; i += nt) {
+        const double gi = s_real(G[i + (int64_t)i * s]);
+        double d = (gi > 0.0 && isfinite(gi)) ? sqrt(gi) : 0.0;
+        if (d == 0.0) {
+            atomicOr(flags + 2, 1);
+            d = 1.0;
+        }
+        dsc[i] = d;
+    }
+    if (tid == 0) s_bad = 0;
+    __syncthreads();
+    const double eps = 2.220446049250313e-16;
+    // Fukaya et al. shift 11 (m n + n (n+1)) u ||Gh||_2 with ||Gh||_2 <= trace(Gh) = s.
+    const double sigma = 11.0 * ((double)nrows * s + (double)s * (s + 1)) * eps * (double)s;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        const double shift = attempt == 0 ? 0.0 : sigma;
+        for (int64_t e = tid; e < (int64_t)s * s; e += nt) {
+            const int i = (int)(e % s), j = (int)(e / s);
+            T g = G[e];
+            if (!isfinite(s_real(g)) || !isfinite(s_imag(g))) g = s_zero(T());
+            g = s_rscale(1.0 / (dsc[i] * dsc[j]), g);
+            if (i == j) g = s_from<T>(s_real(g) + shift, 0.0);
+            M[e] = g;
+        }
+        __syncthreads();
+        // right-looking upper Cholesky: M[k,j] (j>=k) becomes R[k,j]
+        for (int k = 0; k < s; ++k) {
+            if (tid == 0) {
+                const double p = s_real(M[k + (int64_t)k * s]);
+                if (!(p > 1e-13)) s_bad = 1;
+                s_piv = sqrt(p > 1e-300 ? p : 1e-300);
+            }
+            __syncthreads();
+            if (s_bad && attempt == 0) break;
+            const double rkk = s_piv;
+            for (int j = k + 1 + tid; j < s; j += nt) M[k + (int64_t)j * s] = s_rscale(1.0 / rkk, M[k + (int64_t)j * s]);
+            if (tid == 0) M[k + (int64_t)k * s] = s_from<T>(rkk, 0.0);
+            __syncthreads();
+            const int rem = s - k - 1;
+            for (int64_t e = tid; e < (int64_t)rem * rem; e += nt) {
+                const int i = k + 1 + (int)(e % rem), j = k + 1 + (int)(e / rem);
+                if (i <= j) {
+                    // M[i,j] -= conj(R[k,i]) R[k,j]
+                    const T rki = M[k + (int64_t)i * s], rkj = M[k + (int64_t)j * s];
+                    M[i + (int64_t)j * s] = s_sub(M[i + (int64_t)j * s], s_mul(s_conj(rki), rkj));
+                }
+            }
+            __syncthreads();
+        }
+        __syncthreads();
+        if (!s_bad) break;
+        if (attempt == 0) {
+            if (tid == 0) {
+                flags[0] |= 1;
+                s_bad = 0;
+            }
+            __syncthreads();
+        } else {
+            if (tid == 0) flags[1] = 1;
+        }
+    }
+    __syncthreads();
+    // Tout = R^-1 (upper), column j solved by one thread: back substitution; then row-scale by 1/d_i.
+    for (int j = tid; j < s; j += nt) {
+        for (int i = 0; i < s; ++i)
+            if (i > j) Tout[i + (int64_t)j * s] = s_zero(T());
+        Tout[j + (int64_t)j * s] = s_from<T>(1.0 / s_real(M[j + (int64_t)j * s]), 0.0);
+        for (int i = j - 1; i >= 0; --i) {
+            T acc = s_zero(T());
+            for (int l = i + 1; l <= j; ++l) acc = s_fma(M[i + (int64_t)l * s], Tout[l + (int64_t)j * s], acc);
+            Tout[i + (int64_t)j * s] = s_rscale(-1.0 / s_real(M[i + (int64_t)i * s]), acc);
+        }
+    }
+    __syncthreads();
+    for (int64_t e = tid; e < (int64_t)s * s; e += nt) {
+        const int i = (int)(e % s);
+        Tout[e] = s_rscale(1.0 / dsc[i], Tout[e]);
+    }
+}
+
+rc_status chol_factor(rc_ctx* ctx, int dtype, int64_t s, int64_t nrows, const void* G, void* Tout, int* flags) {
+    // scratch after the Gram result in S_SMALL: M (s*s) + dsc (s)
+    const size_t esz = dtype == RC_COMPLEX128 ? 16 : 8;
+    void* base = nullptr;
+    RC_TRY(rc_slot(ctx, S_LANCZOS, (size_t)s * s * esz + (size_t)s * 8 + 256, &base));
+    double* dsc = (double*)((char*)base + (size_t)s * s * esz);
+    if (dtype == RC_COMPLEX128)
+        chol_factor_kernel<double2><<<1, 1024, 0, ctx->stream>>>((int)s, nrows, (const double2*)G, (double2*)base,
+                                                                (double2*)Tout, dsc, flags);
+    else
+        chol_factor_kernel<double><<<1, 1024, 0, ctx->stream>>>((int)s, nrows, (const double*)G, (double*)base,
+                                                               (double*)Tout, dsc, flags);
+    ctx->launches++;
+    RC_CU(ctx, cudaGetLastError());
+    return RC_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Parallel cyclic Jacobi (Brent-Luk round-robin ordering), one CTA.
+// A: s x s Hermitian (col-major, overwritten), Q: eigenvectors, evals ascending.
+// Rotation for pair (p,q), u = a_pq/|a_pq|:  G = [[c, s u], [-s conj(u), c]] on (p,q);
+// A <- G^H A G zeroes a_pq (Golub & Van Loan, Alg. 8.4.1 after removing the phase of a_pq).
+// A and Q live in dynamic shared memory when they fit, otherwise in global scratch.
+// ---------------------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(1024)
+jacobi_kernel(int s, T* __restrict__ Ag, T* __restrict__ Qg, double* __restrict__ evals, int* info, int use_smem,
+              int max_sweeps) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int sp = s + (s & 1);  // even number of players (one dummy when s is odd)
+    const int npair = sp / 2;
+    // layout: rot_c[npair], rot_s[npair], rot_u[npair] (T), then A, Q if use_smem
+    double* rc = (double*)smem_raw;
+    double* rsn = rc + npair;
+    T* ru = (T*)(rsn + npair);
+    T* A = Ag;
+    T* Q = Qg;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    if (use_smem) {
+        A = ru + npair;
+        Q = A + (size_t)s * s;
+        for (int64_t e = tid; e < (int64_t)s * s; e += nt) A[e] = Ag[e];
+    }
+    for (int64_t e = tid; e < (int64_t)s * s; e += nt) {
+        const int i = (int)(e % s), j = (int)(e / s);
+        Q[e] = s_from<T>(i == j ? 1.0 : 0.0, 0.0);
+    }
+    __shared__ double s_fro;
+    __shared__ int s_rot;
+    __shared__ double red[32];
+    __syncthreads();
+    // Frobenius norm for the absolute threshold
+    double f = 0.0;
+    for (int64_t e = tid; e < (int64_t)s * s; e += nt) f += s_abs2(A[e]);
+    f = block_sum(f, red);
+    if (tid == 0) s_fro = sqrt(f);
+    __syncthreads();
+    const double abs_tol = 1e-17 * s_fro;
+    const double rel_tol = 1e-15;
+    const int M = sp - 1;
+    int sweep = 0;
+    for (; sweep < max_sweeps; ++sweep) {
+        if (tid == 0) s_rot = 0;
+        __syncthreads();
+        for (int r = 0; r < M; ++r) {
+            // pair i: (p, q)
+            for (int i = tid; i < npair; i += nt) {
+                int p, q;
+                if (i == 0) {
+                    p = r % M;
+                    q = sp - 1;
+                } else {
+                    p = (r + i) % M;
+                    q = (r - i + M) % M;
+                }
+                if (p > q) {
+                    const int t = p;
+                    p = q;
+                    q = t;
+                }
+                double c = 1.0, sn = 0.0;
+                T u = s_from<T>(1.0, 0.0);
+                if (q < s) {
+                    const T apq = A[p + (int64_t)q * s];
+                    const double app = s_real(A[p + (int64_t)p * s]), aqq = s_real(A[q + (int64_t)q * s]);
+                    const double mag = sqrt(s_abs2(apq));
+                    if (mag > abs_tol && mag > rel_tol * sqrt(fabs(app * aqq))) {
+                        u = s_rscale(1.0 / mag, apq);
+                        const double tau = (aqq - app) / (2.0 * mag);
+                        const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+                        c = 1.0 / sqrt(1.0 + t * t);
+                        sn = t * c;
+                        s_rot = 1;
+                    }
+                }
+                rc[i] = c;
+                rsn[i] = sn;
+                ru[i] = u;
+            }
+            __syncthreads();
+            // columns: A[:,p], A[:,q] and Q[:,p], Q[:,q]
+            for (int64_t e = tid; e < (int64_t)npair * s; e += nt) {
+                const int i = (int)(e / s), row = (int)(e % s);
+                if (rsn[i] == 0.0) continue;
+                int p, q;
+                if (i == 0) {
+                    p = r % M;
+                    q = sp - 1;
+                } else {
+                    p = (r + i) % M;
+                    q = (r - i + M) % M;
+                }
+                if (p > q) {
+                    const int t = p;
+                    p = q;
+                    q = t;
+                }
+                const double c = rc[i], sn = rsn[i];
+                const T u = ru[i];
+                const T su = s_rscale(sn, u), scu = s_rscale(sn, s_conj(u));
+                {
+                    const T ap = A[row + (int64_t)p * s], aq = A[row + (int64_t)q * s];
+                    A[row + (int64_t)p * s] = s_sub(s_rscale(c, ap), s_mul(scu, aq));
+                    A[row + (int64_t)q * s] = s_add(s_mul(su, ap), s_rscale(c, aq));
+                }
+                {
+                    const T qp = Q[row + (int64_t)p * s], qq = Q[row + (int64_t)q * s];
+                    Q[row + (int64_t)p * s] = s_sub(s_rscale(c, qp), s_mul(scu, qq));
+                    Q[row + (int64_t)q * s] = s_add(s_mul(su, qp), s_rscale(c, qq));
+                }
+            }
+            __syncthreads();
+            // rows: A[p,:], A[q,:]
+            for (int64_t e = tid; e < (int64_t)npair * s; e += nt) {
+                const int i = (int)(e / s), col = (int)(e % s);
+                if (rsn[i] == 0.0) continue;
+                int p, q;
+                if (i == 0) {
+                    p = r % M;
+                    q = sp - 1;
+                } else {
+                    p = (r + i) % M;
+                    q = (r - i + M) % M;
+                }
+                if (p > q) {
+                    const int t = p;
+                    p = q;
+                    q = t;
+                }
+                const double c = rc[i], sn = rsn[i];
+                const T u = ru[i];
+                const T su = s_rscale(sn, u), scu = s_rscale(sn, s_conj(u));
+                const T ap = A[p + (int64_t)col * s], aq = A[q + (int64_t)col * s];
+                A[p + (int64_t)col * s] = s_sub(s_rscale(c, ap), s_mul(su, aq));
+                A[q + (int64_t)col * s] = s_add(s_mul(scu, ap), s_rscale(c, aq));
+            }
+            __syncthreads();
+        }
+        const int rot = s_rot;
+        __syncthreads();
+        if (!rot) break;
+    }
+    // sort eigenvalues ascending (rank sort, ties by index) and permute Q columns into Qg
+    for (int i = tid; i < s; i += nt) {
+        const double li = s_real(A[i + (int64_t)i * s]);
+        int rank = 0;
+        for (int j = 0; j < s; ++j) {
+            const double lj = s_real(A[j + (int64_t)j * s]);
+            if (lj < li || (lj == li && j < i)) ++rank;
+        }
+        evals[rank] = li;
+        if (use_smem) {
+            for (int row = 0; row < s; ++row) Qg[row + (int64_t)rank * s] = Q[row + (int64_t)i * s];
+        } else {
+            // Q is the global buffer itself: stage through A's upper triangle is unsafe; write into
+            // the tail scratch after Q (allocated by the launcher) then copy back.
+            T* Qout = Qg + (size_t)s * s;
+            for (int row = 0; row < s; ++row) Qout[row + (int64_t)rank * s] = Q[row + (int64_t)i * s];
+        }
+    }
+    __syncthreads();
+    if (!use_smem) {
+        const T* Qout = Qg + (size_t)s * s;
+        for (int64_t e = tid; e < (int64_t)s * s; e += nt) Qg[e] = Qout[e];
+    }
+    if (tid == 0 && info) info[0] = sweep;
+}
+
+rc_status small_eigh(rc_ctx* ctx, int dtype, int64_t s, void* A, void* Q, double* evals, int* info) {
+    // Q must have room for 2*s*s scalars (second half is staging when the matrices do not fit in smem).
+    const size_t esz = dtype == RC_COMPLEX128 ? 16 : 8;
+    const int64_t sp = s + (s & 1);
+    const size_t rot_bytes = (size_t)(sp / 2) * (16 + esz);
+    const size_t full = rot_bytes + 2 * (size_t)s * s * esz;
+    const bool fit = full <= (size_t)ctx->smem_optin - 2048;
+    const size_t dyn = fit ? full : rot_bytes;
+    const int sweeps = 60;
+    if (dtype == RC_COMPLEX128) {
+        if (dyn > 48 * 1024)
+            RC_CU(ctx, cudaFuncSetAttribute(jacobi_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+        jacobi_kernel<double2><<<1, 1024, dyn, ctx->stream>>>((int)s, (double2*)A, (double2*)Q, evals, info, fit ? 1 : 0,
+                                                              sweeps);
+    } else {
+        if (dyn > 48 * 1024)
+            RC_CU(ctx, cudaFuncSetAttribute(jacobi_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+        jacobi_kernel<double><<<1, 1024, dyn, ctx->stream>>>((int)s, (double*)A, (double*)Q, evals, info, fit ? 1 : 0,
+                                                             sweeps);
+    }
+    ctx->launches++;
+    RC_CU(ctx, cudaGetLastError());
+    return RC_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Elementwise helpers
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+__device__ __forceinline__ double u11(uint64_t h) { return (double)(h >> 11) * (2.0 / 9007199254740992.0) - 1.0; }
+
+template <class T>
+__global__ void fill_random_kernel(T* X, int64_t ld, int64_t n, int64_t c0, int64_t c1, uint64_t seed) {
+    const int64_t total = n * (c1 - c0);
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e % n, c = c0 + e / n;
+        const uint64_t key = seed * 0x100000001B3ull + (uint64_t)c * (uint64_t)n + (uint64_t)i;
+        const uint64_t h1 = splitmix64(key), h2 = splitmix64(key ^ 0xD1B54A32D192ED03ull);
+        X[i + c * ld] = s_from<T>(u11(h1), u11(h2));
+    }
+}
+
+rc_status fill_random(rc_ctx* ctx, int dtype, void* X, int64_t ld, int64_t n, int64_t c0, int64_t c1, uint64_t seed) {
+    if (c1 <= c0 || n <= 0) return RC_OK;
+    if (dtype == RC_COMPLEX128)
+        fill_random_kernel<double2><<<8 * 148, 256, 0, ctx->stream>>>((double2*)X, ld, n, c0, c1, seed);
+    else
+        fill_random_kernel<double><<<8 * 148, 256, 0, ctx->stream>>>((double*)X, ld, n, c0, c1, seed);
+    ctx->launches++;
+    RC_CU(ctx, cudaGetLastError());
+    return RC_OK;
+}
+
+rc_status copy_cols(rc_ctx* ctx, int dtype, const void* X, int64_t ldx, void* Y, int64_t ldy, int64_t n, int64_t s) {
+    if (s <= 0 || n <= 0) return RC_OK;
+    const size_t esz = dtype == RC_COMPLEX128 ? 16 : 8;
+    RC_CU(ctx, cudaMemcpy2DAsync(Y, (size_t)ldy * esz, X, (size_t)ldx * esz, (size_t)n * esz, (size_t)s,
+                                 cudaMemcpyDeviceToDevice, ctx->stream));
+    return RC_OK;
+}
+
+template <class T>
+__global__ void axpby_kernel(int64_t n, int64_t s, double a, const T* X, int64_t ldx, double b, T* Y, int64_t ldy) {
+    const int64_t total = n * s;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e % n, c = e / n;
+        Y[i + c * ldy] = s_add(s_rscale(a, X[i + c * ldx]), s_rscale(b, Y[i + c * ldy]));
+    }
+}
+
+rc_status axpby(rc_ctx* ctx, int dtype, double a, const void* X, int64_t ldx, double b, void* Y, int64_t ldy,
+                int64_t n, int64_t s) {
+    if (s <= 0 || n <= 0) return RC_OK;
+    if (dtype == RC_COMPLEX128)
+        axpby_kernel<double2><<<8 * 148, 256, 0, ctx->stream>>>(n, s, a, (const double2*)X, ldx, b, (double2*)Y, ldy);
+    else
+        axpby_kernel<double><<<8 * 148, 256, 0, ctx->stream>>>(n, s, a, (const double*)X, ldx, b, (double*)Y, ldy);
+    ctx->launches++;
+    RC_CU(ctx, cudaGetLastError());
+    return RC_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// CholeskyQR with escalation: pass p computes G = V^H V, T = D^-1 R^-1, V' = V T (into the
+// other buffer). Two passes (CholeskyQR2) normally; when a Cholesky pass needed the shift the
+// block is ill-conditioned and one more pass follows (shifted CholeskyQR3), up to 4 passes.
+// The result is in V when *swapped is false, else in tmp.
+// ---------------------------------------------------------------------------------------
+rc_status cholqr(rc_ctx* ctx, int dtype, void* V, int64_t ld, int64_t n, int64_t s, void* tmp, bool* swapped,
+                 int* passes) {
+    const size_t esz = dtype == RC_COMPLEX128 ? 16 : 8;
+    void* small = nullptr;
+    RC_TRY(rc_slot(ctx, S_SMALL, 4 * (size_t)s * s * esz + 1024, &small));
+    void* G = small;
+    void* Tm = (char*)small + (size_t)s * s * esz;
+    int* flags = (int*)((char*)small + 4 * (size_t)s * s * esz);
+    double* hflags = nullptr;
+    RC_TRY(rc_host_small(ctx, 64, &hflags));
+    void* cur = V;
+    void* oth = tmp;
+    int64_t ldc = ld, ldo = n;
+    int np = 0;
+    int max_pass = 2;
+    for (int p = 0; p < max_pass && p < 4; ++p) {
+        RC_CU(ctx, cudaMemsetAsync(flags, 0, 4 * sizeof(int), ctx->stream));
+        RC_TRY(gram(ctx, dtype, n, s, s, cur, ldc, cur, ldc, G, true));
+        RC_TRY(chol_factor(ctx, dtype, s, n, G, Tm, flags));
+        XtArgs xa;
+        xa.n = n; xa.k = s; xa.nc = s;
+        xa.X = cur; xa.ldx = ldc;
+        xa.T = Tm; xa.ldt = s;
+        xa.Y = oth; xa.ldy = ldo;
+        RC_TRY(xt(ctx, dtype, xa));
+        ++np;
+        // read the flags of this pass
+        RC_CU(ctx, cudaMemcpyAsync(hflags, flags, 4 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        RC_CU(ctx, cudaStreamSynchronize(ctx->stream));
+        const int* hf = (const int*)hflags;
+        if (hf[1]) return rc_fail(ctx, RC_ERR_BREAKDOWN, "CholeskyQR: Gram matrix not positive definite after shift");
+        if (hf[0] && max_pass < 4) max_pass = std::min(4, p + 3);
+        void* t = cur;
+        cur = oth;
+        oth = t;
+        const int64_t tl = ldc;
+        ldc = ldo;
+        ldo = tl;
+    }
+    *swapped = (cur != V);
+    if (passes) *passes = np;
+    return RC_OK;
+}
+
+}  // namespace rcb

@@ -1,0 +1,152 @@
+// rc_internal.h -- context/operator structs and kernel launchers shared by the library sources.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+#include "../../include/rc_b200.h"
+
+// Storage/compute precision of a block: FP64 (double / c128) or FP32 (float / c64).
+enum { P64 = 0, P32 = 1 };
+
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct rc_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    std::string err;
+    int64_t launches = 0;
+    int64_t op_bytes = 0;
+    // grow-only scratch slots, indexed by the Slot enum
+    std::vector<DevBuf> slots;
+    // pinned host staging for small read-backs
+    double* host_small = nullptr;
+    size_t host_small_bytes = 0;
+    int sm_count = 148;
+    size_t smem_optin = 232448;
+};
+
+enum Slot {
+    S_V = 0, S_W, S_T1, S_T2, S_FOUND, S_PART, S_SMALL, S_LANCZOS, S_RPART, S_IO, S_CB, S_COUNT
+};
+
+struct rc_op {
+    rc_ctx* ctx = nullptr;
+    int dtype = RC_REAL64;
+    int kind = 0;  // 0 CSR, 1 stencil, 2 callback
+    int64_t n = 0;
+    // CSR
+    int64_t nnz = 0;
+    int32_t* rowptr = nullptr;
+    int32_t* colind = nullptr;
+    void* vals64 = nullptr;
+    void* vals32 = nullptr;  // built lazily for the mixed-precision filter
+    // stencil
+    int skind = 7;
+    int64_t nx = 1, ny = 1, nz = 1;
+    double* diag64 = nullptr;
+    float* diag32 = nullptr;
+    double offdiag = 0.0;
+    double flux = 0.0;
+    // callback
+    rc_block_apply_fn fn = nullptr;
+    void* user = nullptr;
+    int64_t bytes = 0;
+};
+
+// Set the context error and return the status.
+rc_status rc_fail(rc_ctx* ctx, rc_status st, const std::string& msg);
+#define RC_CU(ctx, call)                                                                       \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return rc_fail((ctx), RC_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+#define RC_TRY(call)                   \
+    do {                               \
+        rc_status s_ = (call);         \
+        if (s_ != RC_OK) return s_;    \
+    } while (0)
+
+// Scratch slot of at least `bytes` (contents not preserved on growth).
+rc_status rc_slot(rc_ctx* ctx, int slot, size_t bytes, void** out);
+rc_status rc_host_small(rc_ctx* ctx, size_t bytes, double** out);
+inline size_t elem_bytes(int dtype, int prec) {
+    return (dtype == RC_COMPLEX128 ? 2 : 1) * (prec == P64 ? 8 : 4);
+}
+
+namespace rcb {
+
+// ---- operator steps: y = scale*(alpha*(A x) + beta*x + gamma*z) -----------------------
+// x, z, y are n x s column-major; z may be null; y may alias z (not x).
+struct StepArgs {
+    const void* x = nullptr; int xp = P64; int64_t ldx = 0;
+    const void* z = nullptr; int zp = P64; int64_t ldz = 0;
+    void* y = nullptr; int yp = P64; int64_t ldy = 0;
+    int64_t s = 0;
+    double alpha[2] = {1, 0}, beta[2] = {0, 0}, gamma[2] = {0, 0};
+    double scale = 1.0;
+    int cp = P64;  // compute precision (P32: float/c64 accumulation with FP32 matrix values)
+};
+rc_status op_step(rc_ctx* ctx, rc_op* op, const StepArgs& a);
+
+// Filter X <- P_m(A')X (in place on V, FP64/c128 in and out) with the step
+// x_k = a*A*x_{k-1} + b*x_{k-1} - x_{k-2} (a = gamma2*gamma1, b = gamma2). tmp: one n x s FP64
+// block of scratch (holds two FP32 blocks in MIXED).
+rc_status filter_apply(rc_ctx* ctx, rc_op* op, void* V, int64_t ld, int64_t s, int64_t degree,
+                       int64_t rep, double a, double b, int prec, void* tmp, int64_t* steps_done);
+
+// ---- dense FP64 kernels (T = double or double2) ------------------------------------
+// C (m x nc, ld m) = X^H Y where X is n x m, Y is n x nc. upper: only i<=j computed then mirrored
+// (requires m == nc and a Hermitian result). part: scratch for per-chunk partial sums.
+rc_status gram(rc_ctx* ctx, int dtype, int64_t n, int64_t m, int64_t nc, const void* X, int64_t ldx,
+               const void* Y, int64_t ldy, void* C, bool upper);
+// Y (n x nc) = beta*Y + alpha * X (n x k) * T (k x nc, ld ldt). Y must not alias X.
+// Optional dual: Y2 = X2 * T and residual partials ||Y2_c - lam_c Y_c||^2 for c < res_count.
+struct XtArgs {
+    int64_t n = 0, k = 0, nc = 0;
+    const void* X = nullptr; int64_t ldx = 0;
+    const void* T = nullptr; int64_t ldt = 0;
+    void* Y = nullptr; int64_t ldy = 0;
+    double alpha = 1.0;
+    double beta = 0.0;
+    const void* X2 = nullptr; int64_t ldx2 = 0;
+    void* Y2 = nullptr; int64_t ldy2 = 0;
+    const double* lam = nullptr; int64_t res_count = 0;
+    double* res = nullptr;  // device output, res_count residual norms
+};
+rc_status xt(rc_ctx* ctx, int dtype, const XtArgs& a);
+
+// Cholesky factor of Gram G (s x s) with diagonal scaling, shift on breakdown;
+// writes Tout = D^-1 R^-1 (upper). flags (device int[4]): [0] shifted, [1] failed, [2] zero column.
+rc_status chol_factor(rc_ctx* ctx, int dtype, int64_t s, int64_t nrows, const void* G, void* Tout,
+                      int* flags);
+// Hermitian eigensolve (parallel Jacobi, one CTA). A (s x s) is overwritten; evals ascending.
+rc_status small_eigh(rc_ctx* ctx, int dtype, int64_t s, void* A, void* Q, double* evals, int* info);
+
+// Elementwise helpers.
+rc_status fill_random(rc_ctx* ctx, int dtype, void* X, int64_t ld, int64_t n, int64_t c0, int64_t c1,
+                      uint64_t seed);
+rc_status copy_cols(rc_ctx* ctx, int dtype, const void* X, int64_t ldx, void* Y, int64_t ldy, int64_t n,
+                    int64_t s);
+// y = a*x + b*y (real coefficients), n x s blocks.
+rc_status axpby(rc_ctx* ctx, int dtype, double a, const void* X, int64_t ldx, double b, void* Y,
+                int64_t ldy, int64_t n, int64_t s);
+
+// ---- Lanczos -------------------------------------------------------------------------
+struct LanczosResult {
+    double lmin = 0, lmax = 0;
+    int64_t iters = 0;
+};
+rc_status lanczos_bounds(rc_ctx* ctx, rc_op* op, const void* v0_host, uint64_t seed, double tol, int which,
+                         int64_t max_iter, LanczosResult* res);
+
+// ---- cholqr over a block (uses ctx slots S_PART, S_SMALL) ---------------------------
+rc_status cholqr(rc_ctx* ctx, int dtype, void* V, int64_t ld, int64_t n, int64_t s, void* tmp, bool* swapped,
+                 int* passes);
+
+}  // namespace rcb
