@@ -343,7 +343,8 @@ def run_ours(args):
                      "max_rel_residual": max_res_rel, "found": int(res_mixed.info["found"])},
         "solve_info": {"mixed": {k2: infos[-1][k2] for k2 in ("inner_iterations", "degree_steps", "fp64_degree_steps",
                                                                "mixed_iterations", "lanczos_iterations",
-                                                               "cholqr_passes", "time_lanczos_ms", "time_filter_ms",
+                                                               "cholqr_passes", "fused_rr", "fused_rr_fallbacks",
+                                                               "time_lanczos_ms", "time_filter_ms",
                                                                "time_ortho_ms", "time_eigenvalue_ms")},
                        "fp64": {k2: info64[k2] for k2 in ("inner_iterations", "degree_steps", "time_filter_ms",
                                                            "time_ortho_ms", "time_eigenvalue_ms")} if info64 else None},

@@ -64,6 +64,7 @@ typedef struct rc_op rc_op;
  * (RayleighChebyshevLMCuda.h:2444-2471) and their set-up (:904-911).
  * ------------------------------------------------------------------------------------ */
 rc_status rc_ctx_create(int device, rc_ctx** out);
+/* Releases the context and every operator still alive on it (their handles become invalid). */
 rc_status rc_ctx_destroy(rc_ctx* ctx);
 const char* rc_ctx_last_error(const rc_ctx* ctx);
 /* stream: a cudaStream_t, or NULL for the context's own non-blocking stream. */
@@ -208,6 +209,9 @@ typedef struct rc_solve_params {
     double mixed_switch_tol;       /* MIXED: relative residual at which the FP64 sweep starts (default 1e-6) */
     int verbose;                   /* print per-iteration lines like verboseFlag */
     int phase_timing;              /* record CUDA-event time per phase (TIMING_ buckets) */
+    int orth_mode;                 /* 0: Rayleigh-Ritz on the filtered block with the Cholesky factor of its
+                                      scaled Gram matrix folded in, CholeskyQR2 when that matrix is
+                                      ill-conditioned; 1: always CholeskyQR2 then Rayleigh-Ritz */
 } rc_solve_params;
 
 typedef struct rc_solve_info {
@@ -235,6 +239,8 @@ typedef struct rc_solve_info {
     double time_eigenvalue_ms;
     int64_t kernel_launches;
     double guard_value;            /* getGuardEigenvalue */
+    int64_t fused_rr;              /* inner iterations whose Rayleigh-Ritz ran on the filtered block */
+    int64_t fused_rr_fallbacks;    /* of those, rejected for conditioning and redone after CholeskyQR2 */
 } rc_solve_info;
 
 void rc_solve_params_default(rc_solve_params* p);

@@ -58,6 +58,7 @@ class SolveParams(C.Structure):
         ("mixed_switch_tol", C.c_double),
         ("verbose", C.c_int),
         ("phase_timing", C.c_int),
+        ("orth_mode", C.c_int),
     ]
 
 
@@ -87,6 +88,8 @@ class SolveInfo(C.Structure):
         ("time_eigenvalue_ms", C.c_double),
         ("kernel_launches", c_i64),
         ("guard_value", C.c_double),
+        ("fused_rr", c_i64),
+        ("fused_rr_fallbacks", c_i64),
     ]
 
     def as_dict(self) -> dict:

@@ -68,6 +68,16 @@ rc_status rc_host_small(rc_ctx* ctx, size_t bytes, double** out) {
             return rc_fail((ctx), RC_ERR_CUDA, "cudaSetDevice failed"); \
     } while (0)
 
+static void op_release(rc_op* op) {
+    if (op->rowptr) cudaFree(op->rowptr);
+    if (op->colind) cudaFree(op->colind);
+    if (op->vals64) cudaFree(op->vals64);
+    if (op->vals32) cudaFree(op->vals32);
+    if (op->diag64) cudaFree(op->diag64);
+    if (op->diag32) cudaFree(op->diag32);
+    delete op;
+}
+
 extern "C" {
 
 int rc_abi_version(void) { return RC_B200_ABI_VERSION; }
@@ -104,6 +114,8 @@ rc_status rc_ctx_destroy(rc_ctx* ctx) {
     if (!ctx) return RC_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    for (rc_op* op : ctx->ops) op_release(op);
+    ctx->ops.clear();
     for (auto& b : ctx->slots)
         if (b.ptr) cudaFree(b.ptr);
     if (ctx->host_small) cudaFreeHost(ctx->host_small);
@@ -164,8 +176,11 @@ rc_status rc_op_csr_create(rc_ctx* ctx, int dtype, int64_t n, int64_t nnz, const
     if (n > 2147483647LL || nnz > 2147483647LL) return rc_fail(ctx, RC_ERR_INVALID, "CSR indices are int32");
     // structural checks on the host (the kernels do not bounds-check colind)
     if (rowptr[0] != 0 || rowptr[n] != nnz) return rc_fail(ctx, RC_ERR_INVALID, "rowptr[0] != 0 or rowptr[n] != nnz");
-    for (int64_t i = 0; i < n; ++i)
+    int64_t max_row = 0;
+    for (int64_t i = 0; i < n; ++i) {
         if (rowptr[i + 1] < rowptr[i]) return rc_fail(ctx, RC_ERR_INVALID, "rowptr not non-decreasing");
+        max_row = std::max<int64_t>(max_row, rowptr[i + 1] - rowptr[i]);
+    }
     for (int64_t k = 0; k < nnz; ++k)
         if (colind[k] < 0 || colind[k] >= n) return rc_fail(ctx, RC_ERR_INVALID, "column index out of range");
     rc_op* op = new (std::nothrow) rc_op();
@@ -175,6 +190,7 @@ rc_status rc_op_csr_create(rc_ctx* ctx, int dtype, int64_t n, int64_t nnz, const
     op->kind = 0;
     op->n = n;
     op->nnz = nnz;
+    op->max_row_nnz = max_row;
     const size_t vsz = (dtype == RC_COMPLEX128 ? 16 : 8);
     rc_status st = dev_copy(ctx, (void**)&op->rowptr, rowptr, (size_t)(n + 1) * 4, op);
     if (st == RC_OK) st = dev_copy(ctx, (void**)&op->colind, colind, (size_t)nnz * 4, op);
@@ -183,6 +199,7 @@ rc_status rc_op_csr_create(rc_ctx* ctx, int dtype, int64_t n, int64_t nnz, const
         rc_op_destroy(op);
         return st;
     }
+    ctx->ops.push_back(op);
     *out = op;
     return RC_OK;
 }
@@ -214,6 +231,7 @@ rc_status rc_op_stencil_create(rc_ctx* ctx, int dtype, int kind, int64_t nx, int
         rc_op_destroy(op);
         return st;
     }
+    ctx->ops.push_back(op);
     *out = op;
     return RC_OK;
 }
@@ -230,6 +248,7 @@ rc_status rc_op_callback_create(rc_ctx* ctx, int dtype, int64_t n, rc_block_appl
     op->n = n;
     op->fn = fn;
     op->user = user;
+    ctx->ops.push_back(op);
     *out = op;
     return RC_OK;
 }
@@ -241,14 +260,13 @@ rc_status rc_op_destroy(rc_op* op) {
         cudaSetDevice(ctx->device);
         cudaStreamSynchronize(ctx->stream);
         ctx->op_bytes -= op->bytes;
+        for (size_t i = 0; i < ctx->ops.size(); ++i)
+            if (ctx->ops[i] == op) {
+                ctx->ops.erase(ctx->ops.begin() + i);
+                break;
+            }
     }
-    if (op->rowptr) cudaFree(op->rowptr);
-    if (op->colind) cudaFree(op->colind);
-    if (op->vals64) cudaFree(op->vals64);
-    if (op->vals32) cudaFree(op->vals32);
-    if (op->diag64) cudaFree(op->diag64);
-    if (op->diag32) cudaFree(op->diag32);
-    delete op;
+    op_release(op);
     return RC_OK;
 }
 

@@ -299,15 +299,21 @@ rc_status xt(rc_ctx* ctx, int dtype, const XtArgs& a) {
 // Cholesky factor of the column-scaled Gram matrix (one CTA, 1024 threads).
 //   d_i = sqrt(G_ii), Gh = D^-1 G D^-1 (+ sigma I on breakdown), Gh = R^H R (R upper),
 //   Tout = D^-1 R^-1 so that V*Tout has orthonormal columns.
-// The working matrix lives in global scratch M (s x s) which stays L2-resident.
+// The factor M and the inverse X live in dynamic shared memory when they fit (mode 2: both,
+// mode 1: M only), otherwise in global scratch that stays L2-resident. The inverse is formed
+// row by row from the bottom (X[i,j] for all j >= i in parallel), so no thread walks a long
+// dependent chain.
 // flags[0] |= 1 if shifted, flags[1] = 1 if failed, flags[2] = 1 if a zero column was met.
-// ---------------------------------------------------------------------------------------
 template <class T>
 __global__ void __launch_bounds__(1024)
-chol_factor_kernel(int s, int64_t nrows, const T* __restrict__ G, T* M, T* __restrict__ Tout, double* dsc,
-                   int* flags) {
+chol_factor_kernel(int s, int64_t nrows, const T* __restrict__ G, T* Mg, T* Tout, double* dscg, int* flags, double* pivout,
+                   int mode) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_bad;
-    __shared__ double s_piv;
+    __shared__ double s_piv, s_minpiv;
+    T* M = mode >= 1 ? (T*)smem_raw : Mg;
+    T* X = mode == 2 ? M + (size_t)s * s : Tout;
+    double* dsc = mode == 2 ? (double*)(X + (size_t)s * s) : (mode == 1 ? (double*)(M + (size_t)s * s) : dscg);
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int i = tid; i < s; i += nt) {
         const double gi = s_real(G[i + (int64_t)i * s]);
@@ -325,6 +331,7 @@ chol_factor_kernel(int s, int64_t nrows, const T* __restrict__ G, T* M, T* __res
     const double sigma = 11.0 * ((double)nrows * s + (double)s * (s + 1)) * eps * (double)s;
     for (int attempt = 0; attempt < 2; ++attempt) {
         const double shift = attempt == 0 ? 0.0 : sigma;
+        if (tid == 0) s_minpiv = 1e300;
         for (int64_t e = tid; e < (int64_t)s * s; e += nt) {
             const int i = (int)(e % s), j = (int)(e / s);
             T g = G[e];
@@ -339,6 +346,7 @@ chol_factor_kernel(int s, int64_t nrows, const T* __restrict__ G, T* M, T* __res
             if (tid == 0) {
                 const double p = s_real(M[k + (int64_t)k * s]);
                 if (!(p > 1e-13)) s_bad = 1;
+                s_minpiv = fmin(s_minpiv, p);
                 s_piv = sqrt(p > 1e-300 ? p : 1e-300);
             }
             __syncthreads();
@@ -371,36 +379,56 @@ chol_factor_kernel(int s, int64_t nrows, const T* __restrict__ G, T* M, T* __res
         }
     }
     __syncthreads();
-    // Tout = R^-1 (upper), column j solved by one thread: back substitution; then row-scale by 1/d_i.
-    for (int j = tid; j < s; j += nt) {
-        for (int i = 0; i < s; ++i)
-            if (i > j) Tout[i + (int64_t)j * s] = s_zero(T());
-        Tout[j + (int64_t)j * s] = s_from<T>(1.0 / s_real(M[j + (int64_t)j * s]), 0.0);
-        for (int i = j - 1; i >= 0; --i) {
-            T acc = s_zero(T());
-            for (int l = i + 1; l <= j; ++l) acc = s_fma(M[i + (int64_t)l * s], Tout[l + (int64_t)j * s], acc);
-            Tout[i + (int64_t)j * s] = s_rscale(-1.0 / s_real(M[i + (int64_t)i * s]), acc);
-        }
-    }
+    // X = R^-1 (upper): for i = s-1 .. 0, X[i,j] = (delta_ij - sum_{l=i+1..j} R[i,l] X[l,j]) / R[i,i]
+    for (int64_t e = tid; e < (int64_t)s * s; e += nt) X[e] = s_zero(T());
     __syncthreads();
+    for (int i = s - 1; i >= 0; --i) {
+        const double inv = 1.0 / s_real(M[i + (int64_t)i * s]);
+        for (int j = i + tid; j < s; j += nt) {
+            T acc = s_from<T>(i == j ? 1.0 : 0.0, 0.0);
+            for (int l = i + 1; l <= j; ++l) acc = s_sub(acc, s_mul(M[i + (int64_t)l * s], X[l + (int64_t)j * s]));
+            X[i + (int64_t)j * s] = s_rscale(inv, acc);
+        }
+        __syncthreads();
+    }
+    if (tid == 0 && pivout) pivout[0] = s_minpiv;
+    // Tout = D^-1 X
     for (int64_t e = tid; e < (int64_t)s * s; e += nt) {
         const int i = (int)(e % s);
-        Tout[e] = s_rscale(1.0 / dsc[i], Tout[e]);
+        Tout[e] = s_rscale(1.0 / dsc[i], X[e]);
     }
 }
 
-rc_status chol_factor(rc_ctx* ctx, int dtype, int64_t s, int64_t nrows, const void* G, void* Tout, int* flags) {
-    // scratch after the Gram result in S_SMALL: M (s*s) + dsc (s)
+rc_status chol_factor(rc_ctx* ctx, int dtype, int64_t s, int64_t nrows, const void* G, void* Tout, int* flags,
+                      double* pivout) {
     const size_t esz = dtype == RC_COMPLEX128 ? 16 : 8;
     void* base = nullptr;
     RC_TRY(rc_slot(ctx, S_LANCZOS, (size_t)s * s * esz + (size_t)s * 8 + 256, &base));
     double* dsc = (double*)((char*)base + (size_t)s * s * esz);
-    if (dtype == RC_COMPLEX128)
-        chol_factor_kernel<double2><<<1, 1024, 0, ctx->stream>>>((int)s, nrows, (const double2*)G, (double2*)base,
-                                                                (double2*)Tout, dsc, flags);
-    else
-        chol_factor_kernel<double><<<1, 1024, 0, ctx->stream>>>((int)s, nrows, (const double*)G, (double*)base,
-                                                               (double*)Tout, dsc, flags);
+    const size_t budget = ctx->smem_optin > 4096 ? ctx->smem_optin - 4096 : 0;
+    const size_t mat = (size_t)s * s * esz;
+    int mode = 0;
+    size_t dyn = 0;
+    if (2 * mat + (size_t)s * 8 <= budget) {
+        mode = 2;
+        dyn = 2 * mat + (size_t)s * 8;
+    } else if (mat + (size_t)s * 8 <= budget) {
+        mode = 1;
+        dyn = mat + (size_t)s * 8;
+    }
+    if (dtype == RC_COMPLEX128) {
+        if (dyn > 48 * 1024)
+            RC_CU(ctx, cudaFuncSetAttribute(chol_factor_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)dyn));
+        chol_factor_kernel<double2><<<1, 1024, dyn, ctx->stream>>>((int)s, nrows, (const double2*)G, (double2*)base,
+                                                                  (double2*)Tout, dsc, flags, pivout, mode);
+    } else {
+        if (dyn > 48 * 1024)
+            RC_CU(ctx, cudaFuncSetAttribute(chol_factor_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)dyn));
+        chol_factor_kernel<double><<<1, 1024, dyn, ctx->stream>>>((int)s, nrows, (const double*)G, (double*)base,
+                                                                 (double*)Tout, dsc, flags, pivout, mode);
+    }
     ctx->launches++;
     RC_CU(ctx, cudaGetLastError());
     return RC_OK;
@@ -408,72 +436,83 @@ rc_status chol_factor(rc_ctx* ctx, int dtype, int64_t s, int64_t nrows, const vo
 
 // ---------------------------------------------------------------------------------------
 // Parallel cyclic Jacobi (Brent-Luk round-robin ordering), one CTA.
-// A: s x s Hermitian (col-major, overwritten), Q: eigenvectors, evals ascending.
+// A: s x s Hermitian (col-major, ld s, not modified), Q: eigenvectors (ld s), evals ascending.
 // Rotation for pair (p,q), u = a_pq/|a_pq|:  G = [[c, s u], [-s conj(u), c]] on (p,q);
 // A <- G^H A G zeroes a_pq (Golub & Van Loan, Alg. 8.4.1 after removing the phase of a_pq).
-// A and Q live in dynamic shared memory when they fit, otherwise in global scratch.
-// ---------------------------------------------------------------------------------------
+// Each round applies the s/2 disjoint rotations of the round-robin schedule at once: every
+// thread owns 2x2 blocks A[{p_i,q_i},{p_j,q_j}] <- G_i^H A G_j (rows and columns in one pass)
+// and, independently, pairs of columns of Q <- Q G_j. The working copies use an odd leading
+// dimension (bank-conflict free rows and columns) in shared memory when they fit, otherwise
+// in global scratch `work` (2*sp*(sp+1) scalars).
+template <class T>
+__device__ __forceinline__ void rr_pair(int r, int i, int M, int sp, int& p, int& q) {
+    if (i == 0) {
+        p = r % M;
+        q = sp - 1;
+    } else {
+        p = (r + i) % M;
+        q = (r - i + M) % M;
+    }
+    if (p > q) {
+        const int t = p;
+        p = q;
+        q = t;
+    }
+}
+
 template <class T>
 __global__ void __launch_bounds__(1024)
-jacobi_kernel(int s, T* __restrict__ Ag, T* __restrict__ Qg, double* __restrict__ evals, int* info, int use_smem,
-              int max_sweeps) {
+jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __restrict__ evals, int* info,
+              T* work, int use_smem, int max_sweeps) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int sp = s + (s & 1);  // even number of players (one dummy when s is odd)
+    const int sp = s + (s & 1);  // even number of indices (one zero dummy row/column when s is odd)
     const int npair = sp / 2;
-    // layout: rot_c[npair], rot_s[npair], rot_u[npair] (T), then A, Q if use_smem
+    const int ld = sp + 1;       // odd leading dimension
     double* rc = (double*)smem_raw;
     double* rsn = rc + npair;
     T* ru = (T*)(rsn + npair);
-    T* A = Ag;
-    T* Q = Qg;
-    const int tid = threadIdx.x, nt = blockDim.x;
+    int* pp = (int*)(ru + npair);
+    int* qq = pp + npair;
+    T* A;
+    T* Q;
     if (use_smem) {
-        A = ru + npair;
-        Q = A + (size_t)s * s;
-        for (int64_t e = tid; e < (int64_t)s * s; e += nt) A[e] = Ag[e];
+        A = (T*)((char*)smem_raw + (((size_t)npair * (16 + sizeof(T) + 8) + 15) / 16) * 16);
+    } else {
+        A = work;
     }
-    for (int64_t e = tid; e < (int64_t)s * s; e += nt) {
-        const int i = (int)(e % s), j = (int)(e / s);
-        Q[e] = s_from<T>(i == j ? 1.0 : 0.0, 0.0);
+    Q = A + (size_t)sp * ld;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int e = tid; e < sp * sp; e += nt) {
+        const int i = e % sp, j = e / sp;
+        A[i + j * ld] = (i < s && j < s) ? Ain[i + (int64_t)j * s] : s_zero(T());
+        Q[i + j * ld] = s_from<T>(i == j ? 1.0 : 0.0, 0.0);
     }
     __shared__ double s_fro;
     __shared__ int s_rot;
     __shared__ double red[32];
     __syncthreads();
-    // Frobenius norm for the absolute threshold
     double f = 0.0;
-    for (int64_t e = tid; e < (int64_t)s * s; e += nt) f += s_abs2(A[e]);
+    for (int e = tid; e < sp * sp; e += nt) f += s_abs2(A[(e % sp) + (e / sp) * ld]);
     f = block_sum(f, red);
     if (tid == 0) s_fro = sqrt(f);
     __syncthreads();
     const double abs_tol = 1e-17 * s_fro;
     const double rel_tol = 1e-15;
     const int M = sp - 1;
+    const int nblk = npair * npair;
     int sweep = 0;
     for (; sweep < max_sweeps; ++sweep) {
         if (tid == 0) s_rot = 0;
         __syncthreads();
         for (int r = 0; r < M; ++r) {
-            // pair i: (p, q)
             for (int i = tid; i < npair; i += nt) {
                 int p, q;
-                if (i == 0) {
-                    p = r % M;
-                    q = sp - 1;
-                } else {
-                    p = (r + i) % M;
-                    q = (r - i + M) % M;
-                }
-                if (p > q) {
-                    const int t = p;
-                    p = q;
-                    q = t;
-                }
+                rr_pair<T>(r, i, M, sp, p, q);
                 double c = 1.0, sn = 0.0;
                 T u = s_from<T>(1.0, 0.0);
                 if (q < s) {
-                    const T apq = A[p + (int64_t)q * s];
-                    const double app = s_real(A[p + (int64_t)p * s]), aqq = s_real(A[q + (int64_t)q * s]);
+                    const T apq = A[p + q * ld];
+                    const double app = s_real(A[p + p * ld]), aqq = s_real(A[q + q * ld]);
                     const double mag = sqrt(s_abs2(apq));
                     if (mag > abs_tol && mag > rel_tol * sqrt(fabs(app * aqq))) {
                         u = s_rscale(1.0 / mag, apq);
@@ -487,63 +526,54 @@ jacobi_kernel(int s, T* __restrict__ Ag, T* __restrict__ Qg, double* __restrict_
                 rc[i] = c;
                 rsn[i] = sn;
                 ru[i] = u;
+                pp[i] = p;
+                qq[i] = q;
             }
             __syncthreads();
-            // columns: A[:,p], A[:,q] and Q[:,p], Q[:,q]
-            for (int64_t e = tid; e < (int64_t)npair * s; e += nt) {
-                const int i = (int)(e / s), row = (int)(e % s);
-                if (rsn[i] == 0.0) continue;
-                int p, q;
-                if (i == 0) {
-                    p = r % M;
-                    q = sp - 1;
-                } else {
-                    p = (r + i) % M;
-                    q = (r - i + M) % M;
+            // A <- G^H A G on 2x2 blocks (row pair bi, column pair bj)
+            for (int e = tid; e < nblk; e += nt) {
+                const int bi = e % npair, bj = e / npair;
+                const double si = rsn[bi], sj = rsn[bj];
+                if (si == 0.0 && sj == 0.0) continue;
+                const int pi = pp[bi], qi = qq[bi], pj = pp[bj], qj = qq[bj];
+                const double ci = rc[bi], cj = rc[bj];
+                const T ui = ru[bi], uj = ru[bj];
+                const T a_pp = A[pi + pj * ld], a_qp = A[qi + pj * ld];
+                const T a_pq = A[pi + qj * ld], a_qq = A[qi + qj * ld];
+                // columns: [b_p b_q] = [a_p a_q] G_j
+                const T sju = s_rscale(sj, uj), sjc = s_rscale(sj, s_conj(uj));
+                const T b_pp = s_sub(s_rscale(cj, a_pp), s_mul(sjc, a_pq));
+                const T b_qp = s_sub(s_rscale(cj, a_qp), s_mul(sjc, a_qq));
+                const T b_pq = s_add(s_mul(sju, a_pp), s_rscale(cj, a_pq));
+                const T b_qq = s_add(s_mul(sju, a_qp), s_rscale(cj, a_qq));
+                // rows: G_i^H [b_p.; b_q.]
+                const T siu = s_rscale(si, ui), sic = s_rscale(si, s_conj(ui));
+                T n_pp = s_sub(s_rscale(ci, b_pp), s_mul(siu, b_qp));
+                T n_qp = s_add(s_mul(sic, b_pp), s_rscale(ci, b_qp));
+                T n_pq = s_sub(s_rscale(ci, b_pq), s_mul(siu, b_qq));
+                T n_qq = s_add(s_mul(sic, b_pq), s_rscale(ci, b_qq));
+                if (bi == bj && si != 0.0) {  // the rotated 2x2 diagonal block: exact zeros off-diagonal
+                    n_qp = s_zero(T());
+                    n_pq = s_zero(T());
+                    n_pp = s_from<T>(s_real(n_pp), 0.0);
+                    n_qq = s_from<T>(s_real(n_qq), 0.0);
                 }
-                if (p > q) {
-                    const int t = p;
-                    p = q;
-                    q = t;
-                }
-                const double c = rc[i], sn = rsn[i];
-                const T u = ru[i];
-                const T su = s_rscale(sn, u), scu = s_rscale(sn, s_conj(u));
-                {
-                    const T ap = A[row + (int64_t)p * s], aq = A[row + (int64_t)q * s];
-                    A[row + (int64_t)p * s] = s_sub(s_rscale(c, ap), s_mul(scu, aq));
-                    A[row + (int64_t)q * s] = s_add(s_mul(su, ap), s_rscale(c, aq));
-                }
-                {
-                    const T qp = Q[row + (int64_t)p * s], qq = Q[row + (int64_t)q * s];
-                    Q[row + (int64_t)p * s] = s_sub(s_rscale(c, qp), s_mul(scu, qq));
-                    Q[row + (int64_t)q * s] = s_add(s_mul(su, qp), s_rscale(c, qq));
-                }
+                A[pi + pj * ld] = n_pp;
+                A[qi + pj * ld] = n_qp;
+                A[pi + qj * ld] = n_pq;
+                A[qi + qj * ld] = n_qq;
             }
-            __syncthreads();
-            // rows: A[p,:], A[q,:]
-            for (int64_t e = tid; e < (int64_t)npair * s; e += nt) {
-                const int i = (int)(e / s), col = (int)(e % s);
-                if (rsn[i] == 0.0) continue;
-                int p, q;
-                if (i == 0) {
-                    p = r % M;
-                    q = sp - 1;
-                } else {
-                    p = (r + i) % M;
-                    q = (r - i + M) % M;
-                }
-                if (p > q) {
-                    const int t = p;
-                    p = q;
-                    q = t;
-                }
-                const double c = rc[i], sn = rsn[i];
-                const T u = ru[i];
-                const T su = s_rscale(sn, u), scu = s_rscale(sn, s_conj(u));
-                const T ap = A[p + (int64_t)col * s], aq = A[q + (int64_t)col * s];
-                A[p + (int64_t)col * s] = s_sub(s_rscale(c, ap), s_mul(su, aq));
-                A[q + (int64_t)col * s] = s_add(s_mul(scu, ap), s_rscale(c, aq));
+            // Q <- Q G_j (columns p_j, q_j of rows 0..s-1)
+            for (int e = tid; e < npair * s; e += nt) {
+                const int row = e % s, bj = e / s;
+                const double sj = rsn[bj];
+                if (sj == 0.0) continue;
+                const int pj = pp[bj], qj = qq[bj];
+                const double cj = rc[bj];
+                const T uj = ru[bj];
+                const T qp = Q[row + pj * ld], qq_ = Q[row + qj * ld];
+                Q[row + pj * ld] = s_sub(s_rscale(cj, qp), s_mul(s_rscale(sj, s_conj(uj)), qq_));
+                Q[row + qj * ld] = s_add(s_mul(s_rscale(sj, uj), qp), s_rscale(cj, qq_));
             }
             __syncthreads();
         }
@@ -551,52 +581,100 @@ jacobi_kernel(int s, T* __restrict__ Ag, T* __restrict__ Qg, double* __restrict_
         __syncthreads();
         if (!rot) break;
     }
-    // sort eigenvalues ascending (rank sort, ties by index) and permute Q columns into Qg
+    // ascending order (rank sort, ties by index) over the s real indices
     for (int i = tid; i < s; i += nt) {
-        const double li = s_real(A[i + (int64_t)i * s]);
+        const double li = s_real(A[i + i * ld]);
         int rank = 0;
         for (int j = 0; j < s; ++j) {
-            const double lj = s_real(A[j + (int64_t)j * s]);
+            const double lj = s_real(A[j + j * ld]);
             if (lj < li || (lj == li && j < i)) ++rank;
         }
         evals[rank] = li;
-        if (use_smem) {
-            for (int row = 0; row < s; ++row) Qg[row + (int64_t)rank * s] = Q[row + (int64_t)i * s];
-        } else {
-            // Q is the global buffer itself: stage through A's upper triangle is unsafe; write into
-            // the tail scratch after Q (allocated by the launcher) then copy back.
-            T* Qout = Qg + (size_t)s * s;
-            for (int row = 0; row < s; ++row) Qout[row + (int64_t)rank * s] = Q[row + (int64_t)i * s];
-        }
-    }
-    __syncthreads();
-    if (!use_smem) {
-        const T* Qout = Qg + (size_t)s * s;
-        for (int64_t e = tid; e < (int64_t)s * s; e += nt) Qg[e] = Qout[e];
+        for (int row = 0; row < s; ++row) Qout[row + (int64_t)rank * s] = Q[row + i * ld];
     }
     if (tid == 0 && info) info[0] = sweep;
 }
 
 rc_status small_eigh(rc_ctx* ctx, int dtype, int64_t s, void* A, void* Q, double* evals, int* info) {
-    // Q must have room for 2*s*s scalars (second half is staging when the matrices do not fit in smem).
     const size_t esz = dtype == RC_COMPLEX128 ? 16 : 8;
     const int64_t sp = s + (s & 1);
-    const size_t rot_bytes = (size_t)(sp / 2) * (16 + esz);
-    const size_t full = rot_bytes + 2 * (size_t)s * s * esz;
-    const bool fit = full <= (size_t)ctx->smem_optin - 2048;
-    const size_t dyn = fit ? full : rot_bytes;
+    const int64_t npair = sp / 2;
+    const size_t head = (((size_t)npair * (16 + esz + 8) + 15) / 16) * 16;
+    const size_t mats = 2 * (size_t)sp * (sp + 1) * esz;
+    const bool fit = head + mats <= (size_t)ctx->smem_optin - 2048;
+    const size_t dyn = fit ? head + mats : head;
+    void* work = nullptr;
+    if (!fit) RC_TRY(rc_slot(ctx, S_EIG, mats + 256, &work));
     const int sweeps = 60;
     if (dtype == RC_COMPLEX128) {
         if (dyn > 48 * 1024)
             RC_CU(ctx, cudaFuncSetAttribute(jacobi_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-        jacobi_kernel<double2><<<1, 1024, dyn, ctx->stream>>>((int)s, (double2*)A, (double2*)Q, evals, info, fit ? 1 : 0,
-                                                              sweeps);
+        jacobi_kernel<double2><<<1, 1024, dyn, ctx->stream>>>((int)s, (const double2*)A, (double2*)Q, evals, info,
+                                                              (double2*)work, fit ? 1 : 0, sweeps);
     } else {
         if (dyn > 48 * 1024)
             RC_CU(ctx, cudaFuncSetAttribute(jacobi_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-        jacobi_kernel<double><<<1, 1024, dyn, ctx->stream>>>((int)s, (double*)A, (double*)Q, evals, info, fit ? 1 : 0,
-                                                             sweeps);
+        jacobi_kernel<double><<<1, 1024, dyn, ctx->stream>>>((int)s, (const double*)A, (double*)Q, evals, info,
+                                                             (double*)work, fit ? 1 : 0, sweeps);
     }
+    ctx->launches++;
+    RC_CU(ctx, cudaGetLastError());
+    return RC_OK;
+}
+// ---------------------------------------------------------------------------------------
+// Small dense helpers on s x s matrices (column-major, ld s): C = op(A) B and C <- (C + C^H)/2.
+// One thread per output element; the operands stay in L1/L2.
+// ---------------------------------------------------------------------------------------
+template <class T>
+__global__ void small_gemm_kernel(int s, const T* __restrict__ A, int transA, const T* __restrict__ B,
+                                  T* __restrict__ C) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= s * s) return;
+    const int i = e % s, j = e / s;
+    T acc = s_zero(T());
+    if (transA) {
+        for (int l = 0; l < s; ++l) acc = s_cfma(A[l + (int64_t)i * s], B[l + (int64_t)j * s], acc);
+    } else {
+        for (int l = 0; l < s; ++l) acc = s_fma(A[i + (int64_t)l * s], B[l + (int64_t)j * s], acc);
+    }
+    C[e] = acc;
+}
+
+template <class T>
+__global__ void hermitize_kernel(int s, T* C) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= s * s) return;
+    const int i = e % s, j = e / s;
+    if (i > j) return;
+    const T a = C[e], b = C[j + (int64_t)i * s];
+    if (i == j) {
+        C[e] = s_from<T>(s_real(a), 0.0);
+    } else {
+        const T m = s_rscale(0.5, s_add(a, s_conj(b)));
+        C[e] = m;
+        C[j + (int64_t)i * s] = s_conj(m);
+    }
+}
+
+rc_status small_gemm(rc_ctx* ctx, int dtype, int64_t s, const void* A, bool transA, const void* B, void* C) {
+    const unsigned g = (unsigned)((s * s + 255) / 256);
+    if (dtype == RC_COMPLEX128)
+        small_gemm_kernel<double2><<<g, 256, 0, ctx->stream>>>((int)s, (const double2*)A, transA ? 1 : 0,
+                                                              (const double2*)B, (double2*)C);
+    else
+        small_gemm_kernel<double><<<g, 256, 0, ctx->stream>>>((int)s, (const double*)A, transA ? 1 : 0,
+                                                             (const double*)B, (double*)C);
+    ctx->launches++;
+    RC_CU(ctx, cudaGetLastError());
+    return RC_OK;
+}
+
+rc_status hermitize(rc_ctx* ctx, int dtype, int64_t s, void* C) {
+    const unsigned g = (unsigned)((s * s + 255) / 256);
+    if (dtype == RC_COMPLEX128)
+        hermitize_kernel<double2><<<g, 256, 0, ctx->stream>>>((int)s, (double2*)C);
+    else
+        hermitize_kernel<double><<<g, 256, 0, ctx->stream>>>((int)s, (double*)C);
     ctx->launches++;
     RC_CU(ctx, cudaGetLastError());
     return RC_OK;
@@ -688,7 +766,7 @@ rc_status cholqr(rc_ctx* ctx, int dtype, void* V, int64_t ld, int64_t n, int64_t
     for (int p = 0; p < max_pass && p < 4; ++p) {
         RC_CU(ctx, cudaMemsetAsync(flags, 0, 4 * sizeof(int), ctx->stream));
         RC_TRY(gram(ctx, dtype, n, s, s, cur, ldc, cur, ldc, G, true));
-        RC_TRY(chol_factor(ctx, dtype, s, n, G, Tm, flags));
+        RC_TRY(chol_factor(ctx, dtype, s, n, G, Tm, flags, nullptr));
         XtArgs xa;
         xa.n = n; xa.k = s; xa.nc = s;
         xa.X = cur; xa.ldx = ldc;

@@ -75,6 +75,57 @@ csr_step_kernel(int64_t n, int64_t s, const int32_t* __restrict__ rowptr, const 
     }
 }
 
+// Rows with at most MAXR entries: the row's (column, value) pairs are loaded once into
+// registers (padded with (i, 0)), so the MAXR x CB gathers of a column chunk are independent
+// loads the hardware keeps in flight together.
+template <class TA, class TX, class TZ, class TY, class TC, int CB, int MAXR>
+__global__ void __launch_bounds__(kStepThreads)
+csr_step_reg_kernel(int64_t n, int64_t s, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ colind,
+                    const TA* __restrict__ vals, const TX* __restrict__ x, int64_t ldx, const TZ* z, int64_t ldz,
+                    TY* y, int64_t ldy, TC alpha, TC beta, TC gamma, real_t<TC> scale) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int k0 = __ldg(rowptr + i), k1 = __ldg(rowptr + i + 1);
+    const int cnt = k1 - k0;
+    int js[MAXR];
+    TC as[MAXR];
+#pragma unroll
+    for (int r = 0; r < MAXR; ++r) {
+        const bool ok = r < cnt;
+        js[r] = ok ? __ldg(colind + k0 + r) : (int)i;
+        as[r] = ok ? s_cvt<TC>(vals[k0 + r]) : s_zero(TC());
+    }
+    for (int64_t c0 = 0; c0 < s; c0 += CB) {
+        const int nb = (int)((s - c0) < CB ? (s - c0) : CB);
+        TC acc[CB];
+#pragma unroll
+        for (int cc = 0; cc < CB; ++cc) acc[cc] = s_zero(TC());
+        const TX* xc = x + c0 * ldx;
+        if (nb == CB) {
+#pragma unroll
+            for (int r = 0; r < MAXR; ++r)
+#pragma unroll
+                for (int cc = 0; cc < CB; ++cc) acc[cc] = s_fma(as[r], s_cvt<TC>(xc[js[r] + cc * ldx]), acc[cc]);
+        } else {
+#pragma unroll
+            for (int r = 0; r < MAXR; ++r)
+#pragma unroll
+                for (int cc = 0; cc < CB; ++cc)
+                    if (cc < nb) acc[cc] = s_fma(as[r], s_cvt<TC>(xc[js[r] + cc * ldx]), acc[cc]);
+        }
+#pragma unroll
+        for (int cc = 0; cc < CB; ++cc) {
+            if (cc < nb) {
+                const int64_t c = c0 + cc;
+                TC v = s_mul(alpha, acc[cc]);
+                v = s_fma(beta, s_cvt<TC>(x[i + c * ldx]), v);
+                if (z) v = s_fma(gamma, s_cvt<TC>(z[i + c * ldz]), v);
+                y[i + c * ldy] = s_cvt<TY>(s_rscale(scale, v));
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------------------
 // Stencil step (matrix-free, Dirichlet boundaries)
 //   (A v)_i = diag[i]*v_i + offdiag * sum_j phase(i,j) v_j
@@ -187,11 +238,17 @@ static rc_status launch_step_t(rc_ctx* ctx, rc_op* op, const StepArgs& a) {
     const TZ* z = (const TZ*)a.z;
     TY* y = (TY*)a.y;
     constexpr int CB = CPLX ? 4 : 8;
+    // register-cached rows: fewer columns per chunk for the wider scalars keeps registers in check
+    constexpr int CBR = sizeof(TC) >= 16 ? 2 : (sizeof(TC) == 8 ? 4 : 8);
     if (op->kind == 0) {
         using TA = typename Stor<CP, CPLX>::type;
         const TA* vals = (const TA*)(CP == P64 ? op->vals64 : op->vals32);
-        csr_step_kernel<TA, TX, TZ, TY, TC, CB><<<grid, kStepThreads, 0, ctx->stream>>>(
-            n, a.s, op->rowptr, op->colind, vals, x, a.ldx, z, a.ldz, y, a.ldy, alpha, beta, gamma, scale);
+        if (op->max_row_nnz <= 8)
+            csr_step_reg_kernel<TA, TX, TZ, TY, TC, CBR, 8><<<grid, kStepThreads, 0, ctx->stream>>>(
+                n, a.s, op->rowptr, op->colind, vals, x, a.ldx, z, a.ldz, y, a.ldy, alpha, beta, gamma, scale);
+        else
+            csr_step_kernel<TA, TX, TZ, TY, TC, CB><<<grid, kStepThreads, 0, ctx->stream>>>(
+                n, a.s, op->rowptr, op->colind, vals, x, a.ldx, z, a.ldz, y, a.ldy, alpha, beta, gamma, scale);
     } else {
         const double theta = 2.0 * 3.14159265358979323846 * op->flux;
         const R offd = (R)op->offdiag;

@@ -28,10 +28,12 @@ struct rc_ctx {
     size_t host_small_bytes = 0;
     int sm_count = 148;
     size_t smem_optin = 232448;
+    // operators created on this context; rc_ctx_destroy releases the ones still alive
+    std::vector<struct rc_op*> ops;
 };
 
 enum Slot {
-    S_V = 0, S_W, S_T1, S_T2, S_FOUND, S_PART, S_SMALL, S_LANCZOS, S_RPART, S_IO, S_CB, S_COUNT
+    S_V = 0, S_W, S_T1, S_T2, S_FOUND, S_PART, S_SMALL, S_LANCZOS, S_RPART, S_IO, S_CB, S_EIG, S_COUNT
 };
 
 struct rc_op {
@@ -41,6 +43,7 @@ struct rc_op {
     int64_t n = 0;
     // CSR
     int64_t nnz = 0;
+    int64_t max_row_nnz = 0;
     int32_t* rowptr = nullptr;
     int32_t* colind = nullptr;
     void* vals64 = nullptr;
@@ -123,10 +126,14 @@ rc_status xt(rc_ctx* ctx, int dtype, const XtArgs& a);
 
 // Cholesky factor of Gram G (s x s) with diagonal scaling, shift on breakdown;
 // writes Tout = D^-1 R^-1 (upper). flags (device int[4]): [0] shifted, [1] failed, [2] zero column.
+// pivout (device, optional): smallest pivot of the scaled Cholesky (1 = orthonormal columns).
 rc_status chol_factor(rc_ctx* ctx, int dtype, int64_t s, int64_t nrows, const void* G, void* Tout,
-                      int* flags);
-// Hermitian eigensolve (parallel Jacobi, one CTA). A (s x s) is overwritten; evals ascending.
+                      int* flags, double* pivout);
+// Hermitian eigensolve (parallel Jacobi, one CTA). A (s x s) is read only; evals ascending.
 rc_status small_eigh(rc_ctx* ctx, int dtype, int64_t s, void* A, void* Q, double* evals, int* info);
+// C = op(A) B for s x s matrices (op = conjugate transpose when transA), and C <- (C + C^H)/2.
+rc_status small_gemm(rc_ctx* ctx, int dtype, int64_t s, const void* A, bool transA, const void* B, void* C);
+rc_status hermitize(rc_ctx* ctx, int dtype, int64_t s, void* C);
 
 // Elementwise helpers.
 rc_status fill_random(rc_ctx* ctx, int dtype, void* X, int64_t ld, int64_t n, int64_t c0, int64_t c1,

@@ -59,6 +59,7 @@ private:
     rc_status deflate(void* X, int64_t s);
     rc_status ortho(int64_t s);
     rc_status rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool read_back);
+    rc_status rr_fused(int64_t s, int64_t res_count, bool* ok);
     rc_status lanczos(int which, double tol, double* lmin, double* lmax);
     void tic(int ph);
     void toc(int ph);
@@ -74,9 +75,13 @@ private:
 
     void *V_ = nullptr, *W_ = nullptr, *T1_ = nullptr, *T2_ = nullptr, *E_ = nullptr;
     void *H_ = nullptr, *Q_ = nullptr, *C_ = nullptr;
+    void *G_ = nullptr, *Tt_ = nullptr, *M1_ = nullptr, *Cc_ = nullptr;  // fused Rayleigh-Ritz
     double* dlam_ = nullptr;
     double* dres_ = nullptr;
     int* dinfo_ = nullptr;
+    int* dflags_ = nullptr;
+    double* dpiv_ = nullptr;
+    int64_t fused_ok_ = 0, fused_fallback_ = 0;
     double* hbuf_ = nullptr;
     int64_t ss_cap_ = 0;
 
@@ -146,13 +151,19 @@ rc_status Solver::alloc(int64_t ss, int64_t maxDim) {
     const int64_t sq = std::max<int64_t>(ss, md);
     const size_t mat = (size_t)sq * sq * esz_;
     void* sm = nullptr;
-    RC_TRY(rc_slot(ctx_, S_IO, 4 * mat + (size_t)sq * 16 + 256, &sm));
+    RC_TRY(rc_slot(ctx_, S_IO, 8 * mat + (size_t)sq * 16 + 512, &sm));
     H_ = sm;
-    Q_ = (char*)sm + mat;            // 2 matrices (Jacobi staging)
-    C_ = (char*)sm + 3 * mat;
-    dlam_ = (double*)((char*)sm + 4 * mat);
+    Q_ = (char*)sm + mat;
+    C_ = (char*)sm + 2 * mat;
+    G_ = (char*)sm + 4 * mat;
+    Tt_ = (char*)sm + 5 * mat;
+    M1_ = (char*)sm + 6 * mat;
+    Cc_ = (char*)sm + 7 * mat;
+    dlam_ = (double*)((char*)sm + 8 * mat);
     dres_ = dlam_ + sq;
-    dinfo_ = (int*)(dres_ + sq);
+    dpiv_ = dres_ + sq;
+    dinfo_ = (int*)(dpiv_ + 2);
+    dflags_ = dinfo_ + 4;
     RC_TRY(rc_host_small(ctx_, (size_t)sq * 16 + 64, &hbuf_));
     ss_cap_ = ss;
     return RC_OK;
@@ -229,6 +240,62 @@ rc_status Solver::rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool rea
         VtAVeigValue_.assign(hbuf_, hbuf_ + s);
         subspaceResiduals_.assign(hbuf_ + s, hbuf_ + s + res_count);
     }
+    return RC_OK;
+}
+
+// Rayleigh-Ritz directly on the filtered (not orthonormalised) block V_f = V_:
+//   W = A V_f, G = V_f^H V_f, H = V_f^H W, G = D R^H R D (scaled Cholesky), T = D^-1 R^-1,
+//   C = T^H H T, C = Y L Y^H (Jacobi), Q = T Y, V <- V_f Q, W <- W Q (+ residuals).
+// V_f Q has orthonormal columns (Q^H G Q = I) and spans span(V_f), so this is the Rayleigh-Ritz
+// step of the reference on the orthonormalised block with the CholeskyQR folded into the small
+// problem. Accepted only when the scaled Gram matrix is well conditioned (smallest Cholesky pivot
+// >= 1e-3, no shift needed); otherwise *ok = false, V_ still holds V_f and the caller
+// orthonormalises and repeats the Rayleigh-Ritz step.
+rc_status Solver::rr_fused(int64_t s, int64_t res_count, bool* ok) {
+    StepArgs st;
+    st.s = s;
+    st.x = V_; st.xp = P64; st.ldx = n_;
+    st.y = W_; st.yp = P64; st.ldy = n_;
+    st.cp = P64;
+    RC_TRY(op_step(ctx_, op_, st));
+    RC_TRY(gram(ctx_, dtype_, n_, s, s, V_, n_, V_, n_, G_, true));
+    RC_TRY(gram(ctx_, dtype_, n_, s, s, V_, n_, W_, n_, H_, true));
+    RC_CU(ctx_, cudaMemsetAsync(dflags_, 0, 4 * sizeof(int), ctx_->stream));
+    RC_TRY(chol_factor(ctx_, dtype_, s, n_, G_, Tt_, dflags_, dpiv_));
+    RC_TRY(small_gemm(ctx_, dtype_, s, H_, false, Tt_, M1_));   // H T
+    RC_TRY(small_gemm(ctx_, dtype_, s, Tt_, true, M1_, Cc_));   // T^H H T
+    RC_TRY(hermitize(ctx_, dtype_, s, Cc_));
+    RC_TRY(small_eigh(ctx_, dtype_, s, Cc_, M1_, dlam_, dinfo_));  // Y into M1
+    RC_TRY(small_gemm(ctx_, dtype_, s, Tt_, false, M1_, Q_));  // Q = T Y
+    XtArgs a;
+    a.n = n_; a.k = s; a.nc = s;
+    a.X = V_; a.ldx = n_;
+    a.T = Q_; a.ldt = s;
+    a.Y = T1_; a.ldy = n_;
+    a.X2 = W_; a.ldx2 = n_;
+    a.Y2 = T2_; a.ldy2 = n_;
+    a.lam = dlam_; a.res_count = res_count; a.res = dres_;
+    RC_TRY(xt(ctx_, dtype_, a));
+    RC_CU(ctx_, cudaMemcpyAsync(hbuf_, dlam_, s * sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
+    if (res_count > 0)
+        RC_CU(ctx_, cudaMemcpyAsync(hbuf_ + s, dres_, res_count * sizeof(double), cudaMemcpyDeviceToHost,
+                                    ctx_->stream));
+    RC_CU(ctx_, cudaMemcpyAsync(hbuf_ + s + res_count, dpiv_, sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
+    RC_CU(ctx_, cudaMemcpyAsync(hbuf_ + s + res_count + 1, dflags_, 4 * sizeof(int), cudaMemcpyDeviceToHost,
+                                ctx_->stream));
+    RC_CU(ctx_, cudaStreamSynchronize(ctx_->stream));
+    const double piv = hbuf_[s + res_count];
+    const int* fl = (const int*)(hbuf_ + s + res_count + 1);
+    *ok = !(fl[0] || fl[1] || fl[2]) && piv >= 1e-3 && std::isfinite(piv);
+    if (!*ok) {
+        ++fused_fallback_;
+        return RC_OK;
+    }
+    ++fused_ok_;
+    std::swap(V_, T1_);
+    std::swap(W_, T2_);
+    VtAVeigValue_.assign(hbuf_, hbuf_ + s);
+    subspaceResiduals_.assign(hbuf_ + s, hbuf_ + s + res_count);
     return RC_OK;
 }
 
@@ -381,28 +448,29 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
             applyCount += 1;
             count_opapply_ += starDegree * subspaceSize;
 
-            // ---- orthonormalise (:1321-1338)
-            tic(PH_ORTHO);
-            RC_TRY(ortho(subspaceSize));
-            toc(PH_ORTHO);
-            count_ortho_ += 1;
-
-            // ---- Rayleigh-Ritz + residuals (:1344-1401)
+            // ---- orthonormalise (:1321-1338) and Rayleigh-Ritz + residuals (:1344-1401):
+            // fused on the filtered block when it is well conditioned, else CholeskyQR2 then RR.
             if (foundSize_ + subspaceSize < vectorDimension) residualCheckCount = subspaceIncrementSize;
             else residualCheckCount = subspaceSize;
-            tic(PH_EIG);
-            RC_TRY(rr(V_, W_, subspaceSize, residualCheckCount, false));
-            toc(PH_EIG);
+            bool fused = false;
+            if (P_.orth_mode == 0) {
+                tic(PH_EIG);
+                RC_TRY(deflate(V_, subspaceSize));
+                RC_TRY(rr_fused(subspaceSize, residualCheckCount, &fused));
+                toc(PH_EIG);
+            }
+            if (!fused) {
+                tic(PH_ORTHO);
+                RC_TRY(ortho(subspaceSize));
+                toc(PH_ORTHO);
+                tic(PH_EIG);
+                RC_TRY(rr(V_, W_, subspaceSize, residualCheckCount, true));
+                toc(PH_EIG);
+            }
+            flush();
+            count_ortho_ += 1;
             count_opapply_ += subspaceSize + residualCheckCount;
             count_eigenvalue_ += 1;
-            RC_CU(ctx_, cudaMemcpyAsync(hbuf_, dlam_, subspaceSize * sizeof(double), cudaMemcpyDeviceToHost,
-                                        ctx_->stream));
-            RC_CU(ctx_, cudaMemcpyAsync(hbuf_ + subspaceSize, dres_, residualCheckCount * sizeof(double),
-                                        cudaMemcpyDeviceToHost, ctx_->stream));
-            RC_CU(ctx_, cudaStreamSynchronize(ctx_->stream));
-            flush();
-            VtAVeigValue_.assign(hbuf_, hbuf_ + subspaceSize);
-            subspaceResiduals_.assign(hbuf_ + subspaceSize, hbuf_ + subspaceSize + residualCheckCount);
             for (double r : subspaceResiduals_)
                 if (!std::isfinite(r))
                     return rc_fail(ctx_, RC_ERR_BREAKDOWN, "non-finite residual (NaN or Inf in the operator?)");
@@ -706,6 +774,8 @@ rc_status Solver::run(const void* v0, double* evals_out, void* evecs_out, double
         r.time_eigenvalue_ms = t_[PH_EIG];
         r.kernel_launches = ctx_->launches - launches0;
         r.guard_value = guardValue_;
+        r.fused_rr = fused_ok_ + fused_fallback_;
+        r.fused_rr_fallbacks = fused_fallback_;
         std::memcpy(info, &r, std::min(sz, sizeof(r)));
     }
     return RC_OK;

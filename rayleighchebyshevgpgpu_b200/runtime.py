@@ -89,9 +89,10 @@ class Operator:
         self.dtype = capi.RC_COMPLEX128 if complex_ else capi.RC_REAL64
 
     def close(self):
-        if self.h:
+        # a destroyed context has already released its operators (rc_ctx_destroy)
+        if self.h and self.ctx.h:
             lib().rc_op_destroy(self.h)
-            self.h = C.c_void_p()
+        self.h = C.c_void_p()
 
     def __del__(self):
         try:

@@ -31,9 +31,10 @@ def _check_pairs(A, res, k, tol, rtol=1e-10):
     return dense
 
 
+@pytest.mark.parametrize("orth_mode", [0, 1])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("form", ["csr", "stencil"])
-def test_config1_matches_reference_golden(ctx, precision, form):
+def test_config1_matches_reference_golden(ctx, precision, form, orth_mode):
     g = json.load(open(os.path.join(GOLD, "config1_solve.json")))
     P = problems.config1()
     A = O.csr_matrix(*P.csr())
@@ -42,8 +43,12 @@ def test_config1_matches_reference_golden(ctx, precision, form):
     lz0 = np.random.default_rng(11).uniform(-1.0, 1.0, P.n)
     keep = np.ascontiguousarray(lz0)
     res = _solve(ctx, op, P, g["k"], g["tol"], precision, start=P.start_block(s), incr=g["incr"],
-                 buffer=g["buffer"], lanczos_v0=keep.ctypes.data)
+                 buffer=g["buffer"], lanczos_v0=keep.ctypes.data, orth_mode=orth_mode)
     np.testing.assert_allclose(res.evals, g["eigenvalues"], rtol=1e-10)
+    if orth_mode == 1:
+        assert res.info["fused_rr"] == 0
+    else:
+        assert res.info["fused_rr"] > 0
     _check_pairs(A, res, g["k"], g["tol"])
     assert res.info["lanczos_iterations"] > 0 and res.info["degree_steps"] > 0
     if precision == "mixed":
