@@ -196,7 +196,9 @@ def run_ours(args):
     s = incr + buf
     rp, ci, v = P.csr()
     ctx = R.Context(local)
-    stream = torch.cuda.current_stream()
+    # an explicit (non-default) stream: the library and the CUDA events must see the same stream
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
     op = R.CsrOperator(ctx, rp, ci, v)
     start_host = P.start_block(s)

@@ -67,7 +67,8 @@ rc_status rc_ctx_create(int device, rc_ctx** out);
 /* Releases the context and every operator still alive on it (their handles become invalid). */
 rc_status rc_ctx_destroy(rc_ctx* ctx);
 const char* rc_ctx_last_error(const rc_ctx* ctx);
-/* stream: a cudaStream_t, or NULL for the context's own non-blocking stream. */
+/* stream: a cudaStream_t, or NULL for the context's own non-blocking stream (the legacy default
+ * stream cannot be selected: events recorded there do not order against the context's work). */
 rc_status rc_ctx_set_stream(rc_ctx* ctx, void* stream);
 rc_status rc_ctx_synchronize(rc_ctx* ctx);
 /* Number of kernels this library launched through ctx since creation (or last reset). */

@@ -4,6 +4,7 @@
 // returns a status code; nothing here terminates the process (the reference's error macros
 // call exit(), cudaErrchk.h:8-51).
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -106,6 +107,10 @@ rc_status rc_ctx_create(int device, rc_ctx** out) {
         c->smem_optin = prop.sharedMemPerBlockOptin;
     }
     c->slots.resize(S_COUNT);
+    if (const char* v = std::getenv("RCB200_CSR_KERNEL")) {
+        if (!std::strcmp(v, "loop")) c->csr_variant = 1;
+        else if (!std::strcmp(v, "reg")) c->csr_variant = 2;
+    }
     *out = c;
     return RC_OK;
 }
@@ -349,7 +354,8 @@ rc_status rc_filter(rc_ctx* ctx, const rc_op* op_c, void* X, int64_t ld, int64_t
     void* tmp = nullptr;
     RC_TRY(rc_slot(ctx, S_T1, (size_t)op->n * (s > 0 ? s : 1) * elem_bytes(op->dtype, P64), &tmp));
     int64_t steps = 0;
-    return rcb::filter_apply(ctx, op, X, ld, s, degree, repetition, gamma2 * gamma1, gamma2, precision, tmp, &steps);
+    return rcb::filter_apply(ctx, op, X, ld, s, degree, repetition, gamma2 * gamma1, gamma2, precision, tmp, nullptr,
+                             (size_t)op->n * (s > 0 ? s : 1) * elem_bytes(op->dtype, P64), &steps);
 }
 
 rc_status rc_lanczos_bounds(rc_ctx* ctx, const rc_op* op_c, const void* v0, uint64_t seed, double tol, int which,

@@ -243,7 +243,8 @@ static rc_status launch_step_t(rc_ctx* ctx, rc_op* op, const StepArgs& a) {
     if (op->kind == 0) {
         using TA = typename Stor<CP, CPLX>::type;
         const TA* vals = (const TA*)(CP == P64 ? op->vals64 : op->vals32);
-        if (op->max_row_nnz <= 8)
+        const bool reg = ctx->csr_variant == 0 ? op->max_row_nnz <= 8 : (ctx->csr_variant == 2 && op->max_row_nnz <= 8);
+        if (reg)
             csr_step_reg_kernel<TA, TX, TZ, TY, TC, CBR, 8><<<grid, kStepThreads, 0, ctx->stream>>>(
                 n, a.s, op->rowptr, op->colind, vals, x, a.ldx, z, a.ldz, y, a.ldy, alpha, beta, gamma, scale);
         else
@@ -308,7 +309,7 @@ __global__ void cvt_f64_f32_kernel(const double* __restrict__ a, float* __restri
         b[i] = (float)a[i];
 }
 
-static rc_status ensure_fp32(rc_ctx* ctx, rc_op* op) {
+rc_status ensure_fp32(rc_ctx* ctx, rc_op* op) {
     if (op->kind == 0 && op->vals32 == nullptr) {
         const int64_t cnt = op->nnz * (op->dtype == RC_COMPLEX128 ? 2 : 1);
         void* p = nullptr;
@@ -385,13 +386,36 @@ rc_status op_step(rc_ctx* ctx, rc_op* op, const StepArgs& a) {
 
 // ---------------------------------------------------------------------------------------
 // Filter driver: the recurrence of LanczosCpolyOperatorLMCuda::apply with the result left in V.
+// Native operators with degree >= 2 run the row-major pipeline of rc_filter_rm.cu in the
+// two scratch blocks (tmp1, tmp2 of tmp_bytes each, or context slots when too small).
+// Foreign (callback) operators and degree 1 use the column-major steps below:
 //  FP64:  buffers V (x0) and one temporary; x_k overwrites x_{k-2}.
-//  MIXED: x_1..x_{m-1} in two FP32 blocks carved from `tmp`; x_0 read from V (FP64), x_m
+//  MIXED: x_1..x_{m-1} in two FP32 blocks carved from `tmp1`; x_0 read from V (FP64), x_m
 //         written to V (FP64) with the 1/(m+1) scale.
 // ---------------------------------------------------------------------------------------
+rc_status rm_filter(rc_ctx* ctx, rc_op* op, void* V, int64_t ldv, int64_t s, int64_t degree, double a, double b,
+                    int prec, void* bufA, void* bufB);
+int64_t rm_leading_dim(int dtype, int prec, int64_t s);
+
 rc_status filter_apply(rc_ctx* ctx, rc_op* op, void* V, int64_t ld, int64_t s, int64_t degree, int64_t rep,
-                       double a, double b, int prec, void* tmp, int64_t* steps_done) {
+                       double a, double b, int prec, void* tmp1, void* tmp2, size_t tmp_bytes,
+                       int64_t* steps_done) {
     if (degree < 1 || rep < 1 || s < 1) return RC_OK;
+    if (op->kind != 2 && degree >= 2) {
+        const int p = prec == RC_PREC_MIXED ? P32 : P64;
+        const size_t need = (size_t)op->n * rm_leading_dim(op->dtype, p, s) * elem_bytes(op->dtype, p);
+        void* bufA = tmp1;
+        void* bufB = tmp2;
+        if (!bufA || tmp_bytes < need) RC_TRY(rc_slot(ctx, S_FA, need, &bufA));
+        if (!bufB || tmp_bytes < need) RC_TRY(rc_slot(ctx, S_FB, need, &bufB));
+        if (p == P32) RC_TRY(ensure_fp32(ctx, op));
+        for (int64_t r = 0; r < rep; ++r) RC_TRY(rm_filter(ctx, op, V, ld, s, degree, a, b, prec, bufA, bufB));
+        if (steps_done) *steps_done += degree * rep;
+        return RC_OK;
+    }
+    void* tmp = tmp1;
+    if (!tmp || tmp_bytes < (size_t)op->n * s * elem_bytes(op->dtype, P64))
+        RC_TRY(rc_slot(ctx, S_FA, (size_t)op->n * s * elem_bytes(op->dtype, P64), &tmp));
     const int64_t n = op->n;
     const bool cplx = op->dtype == RC_COMPLEX128;
     if (op->kind == 2) prec = RC_PREC_FP64;

@@ -30,10 +30,14 @@ struct rc_ctx {
     size_t smem_optin = 232448;
     // operators created on this context; rc_ctx_destroy releases the ones still alive
     std::vector<struct rc_op*> ops;
+    // CSR step kernel: 0 auto (register-cached rows when every row has <= 8 entries),
+    // 1 row loop, 2 register-cached rows. Read from RCB200_CSR_KERNEL at context creation.
+    int csr_variant = 0;
 };
 
 enum Slot {
-    S_V = 0, S_W, S_T1, S_T2, S_FOUND, S_PART, S_SMALL, S_LANCZOS, S_RPART, S_IO, S_CB, S_EIG, S_COUNT
+    S_V = 0, S_W, S_T1, S_T2, S_FOUND, S_PART, S_SMALL, S_LANCZOS, S_RPART, S_IO, S_CB, S_EIG, S_FA, S_FB,
+    S_COUNT
 };
 
 struct rc_op {
@@ -101,7 +105,10 @@ rc_status op_step(rc_ctx* ctx, rc_op* op, const StepArgs& a);
 // x_k = a*A*x_{k-1} + b*x_{k-1} - x_{k-2} (a = gamma2*gamma1, b = gamma2). tmp: one n x s FP64
 // block of scratch (holds two FP32 blocks in MIXED).
 rc_status filter_apply(rc_ctx* ctx, rc_op* op, void* V, int64_t ld, int64_t s, int64_t degree,
-                       int64_t rep, double a, double b, int prec, void* tmp, int64_t* steps_done);
+                       int64_t rep, double a, double b, int prec, void* tmp1, void* tmp2, size_t tmp_bytes,
+                       int64_t* steps_done);
+// Build the FP32 (c64) copy of an operator's values/diagonal used by the MIXED filter.
+rc_status ensure_fp32(rc_ctx* ctx, rc_op* op);
 
 // ---- dense FP64 kernels (T = double or double2) ------------------------------------
 // C (m x nc, ld m) = X^H Y where X is n x m, Y is n x nc. upper: only i<=j computed then mirrored

@@ -439,7 +439,7 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
                 int64_t steps = 0;
                 // filter_apply takes (g1, g2) with a = g2*g1, b = g2
                 RC_TRY(filter_apply(ctx_, op_, V_, n_, subspaceSize, starDegree, filterRepetitionCount, fa, fb,
-                                    prec, T1_, &steps));
+                                    prec, T1_, T2_, (size_t)n_ * subspaceSize * esz_, &steps));
                 degree_steps_ += steps;
                 if (!fp32Phase) fp64_steps_ += steps;
             }

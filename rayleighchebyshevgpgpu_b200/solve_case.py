@@ -54,7 +54,9 @@ def main(argv=None):
         X = torch.from_numpy(v0).cuda()
         g1, g2 = R.cpoly_gammas(a.filter_only, 16.0, -0.5)
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+        ctx.set_stream(stream.cuda_stream)
         times = []
         for _ in range(a.repeat):
             ev0.record()

@@ -97,6 +97,24 @@ def test_filter_fp64_and_mixed_vs_oracle(ctx, degree, complex_):
             assert err < tol, (prec, err)
 
 
+@pytest.mark.parametrize("kind,dims,s", [(27, (9, 8, 7), 12), (5, (23, 19), 6), (7, (6, 7, 9), 5)])
+@pytest.mark.parametrize("degree", [2, 9])
+def test_filter_stencil_kinds_vs_oracle(ctx, kind, dims, s, degree):
+    n = int(np.prod(dims))
+    diag = 1.0 + np.random.default_rng(kind).uniform(0, 2, n)
+    Q = problems.Problem("t", dims, kind, diag, -1.0 / 26.0 if kind == 27 else -1.0)
+    A = O.csr_matrix(*Q.csr())
+    X = np.random.default_rng(3).standard_normal((s, n))
+    g1, g2 = O.gammas(degree, 9.0, -0.5)
+    ref = O.filter_block(A, X.T, degree, g1, g2).T
+    for op in _ops(ctx, Q):
+        for prec, tol in (("fp64", 1e-12), ("mixed", 1e-5)):
+            Xd = _dev(X)
+            R.filter_block(ctx, op, Xd, s, degree, g1, g2, prec)
+            ctx.synchronize()
+            assert np.abs(_host(Xd) - ref).max() / np.abs(ref).max() < tol
+
+
 def test_cholqr_orthonormal_and_same_span(ctx):
     rng = np.random.default_rng(7)
     n, s = 5000, 40
