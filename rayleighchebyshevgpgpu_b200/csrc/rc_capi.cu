@@ -111,6 +111,11 @@ rc_status rc_ctx_create(int device, rc_ctx** out) {
         if (!std::strcmp(v, "loop")) c->csr_variant = 1;
         else if (!std::strcmp(v, "reg")) c->csr_variant = 2;
     }
+    if (const char* v = std::getenv("RCB200_RM_MAP")) {
+        if (!std::strcmp(v, "persist")) c->rm_map = 1;
+    }
+    c->pf_rows = 4096;
+    if (const char* v = std::getenv("RCB200_PF_ROWS")) c->pf_rows = std::max<int64_t>(0, std::atoll(v));
     *out = c;
     return RC_OK;
 }
@@ -188,6 +193,9 @@ rc_status rc_op_csr_create(rc_ctx* ctx, int dtype, int64_t n, int64_t nnz, const
     }
     for (int64_t k = 0; k < nnz; ++k)
         if (colind[k] < 0 || colind[k] >= n) return rc_fail(ctx, RC_ERR_INVALID, "column index out of range");
+    int64_t band = 0;
+    for (int64_t i = 0; i < n; ++i)
+        for (int32_t k = rowptr[i]; k < rowptr[i + 1]; ++k) band = std::max<int64_t>(band, colind[k] - i);
     rc_op* op = new (std::nothrow) rc_op();
     if (!op) return RC_ERR_NOMEM;
     op->ctx = ctx;
@@ -196,6 +204,7 @@ rc_status rc_op_csr_create(rc_ctx* ctx, int dtype, int64_t n, int64_t nnz, const
     op->n = n;
     op->nnz = nnz;
     op->max_row_nnz = max_row;
+    op->band = band;
     const size_t vsz = (dtype == RC_COMPLEX128 ? 16 : 8);
     rc_status st = dev_copy(ctx, (void**)&op->rowptr, rowptr, (size_t)(n + 1) * 4, op);
     if (st == RC_OK) st = dev_copy(ctx, (void**)&op->colind, colind, (size_t)nnz * 4, op);

@@ -141,6 +141,8 @@ rc_status gram(rc_ctx* ctx, int dtype, int64_t n, int64_t m, int64_t nc, const v
                int64_t ldy, void* C, bool upper) {
     if (m <= 0 || nc <= 0) return RC_OK;
     if (upper && m != nc) return rc_fail(ctx, RC_ERR_INVALID, "gram: upper requires a square result");
+    if (upper && gram2_supported(dtype, m))
+        return gram2(ctx, n, m, (const double*)X, ldx, (const double*)Y, ldy, (double*)C, nullptr, 0, nullptr);
     if (dtype == RC_COMPLEX128)
         return gram_t<double2>(ctx, n, m, nc, (const double2*)X, ldx, (const double2*)Y, ldy, (double2*)C, upper);
     return gram_t<double>(ctx, n, m, nc, (const double*)X, ldx, (const double*)Y, ldy, (double*)C, upper);
@@ -232,7 +234,7 @@ xt_kernel(int64_t n, int64_t k, int64_t nc, const T* __restrict__ X, int64_t ldx
                 Y[r + c * ldy] = v;
                 if (DUAL) {
                     const T w = acc2[i % (DUAL ? 4 : 1)][j % (DUAL ? 4 : 1)];
-                    Y2[r + c * ldy2] = w;
+                    if (Y2) Y2[r + c * ldy2] = w;
                     if (lam && c < res_count) rs[j] += s_abs2(s_sub(w, s_rscale(lc, v)));
                 }
             }
@@ -292,6 +294,12 @@ static rc_status xt_t(rc_ctx* ctx, const XtArgs& a) {
 
 rc_status xt(rc_ctx* ctx, int dtype, const XtArgs& a) {
     if (a.n <= 0 || a.nc <= 0) return RC_OK;
+    // real fast path: plain products and residual-only dual products
+    const bool plain = a.alpha == 1.0 && a.beta == 0.0;
+    const bool dual_res_only = a.X2 != nullptr && a.Y2 == nullptr && a.lam != nullptr && a.res_count > 0;
+    if (plain && (a.X2 == nullptr || dual_res_only) && xt2_supported(dtype, a.k, a.nc))
+        return xt2(ctx, a.n, a.k, a.nc, (const double*)a.X, a.ldx, (const double*)a.T, a.ldt, (double*)a.Y, a.ldy,
+                   (const double*)a.X2, a.ldx2, a.lam, dual_res_only ? a.res_count : 0, a.res);
     return dtype == RC_COMPLEX128 ? xt_t<double2>(ctx, a) : xt_t<double>(ctx, a);
 }
 

@@ -48,35 +48,103 @@ __device__ __forceinline__ void st16(TS* p, const Pack16<TS>& v) {
 
 constexpr int kRmThreads = 256;
 
-// Middle step: thread t -> row i = t / nseg, slice seg = t % nseg (V = 16/sizeof(TS) columns).
+// Middle step. Persistent grid (one wave): CTA b owns the contiguous rows
+// [b*chunk, (b+1)*chunk) and walks them in order, rows_per_iter rows at a time; thread
+// (r, seg) of an iteration owns the 16-byte slice seg of row r (V = 16/sizeof(TS) columns).
+// Walking rows in order keeps the nearby neighbour rows (+-1, +-nx) in this SM's L1; the far
+// ones (+-nx*ny) are fetched at about the same moment by a CTA a few chunks away (L2 hit).
+// pf_z > 0: each 128-byte line of row i + pf_z of x_{k-2} and of row i + pf_x of x_{k-1} (the
+// rows first touched from DRAM that many rows later) is prefetched into L2.
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 template <class Pol, class TS, class TC>
 __global__ void __launch_bounds__(kRmThreads)
-rm_step_kernel(Pol op, int64_t n, int nseg, int64_t ld, const TS* __restrict__ x, const TS* z, TS* y, TC alpha,
-               TC beta, TC gamma) {
+rm_step_kernel(Pol op, int64_t n, int nseg, int64_t ld, int64_t chunk, const TS* __restrict__ x, const TS* z, TS* y,
+               TC alpha, TC beta, TC gamma, int64_t pf_z, int64_t pf_x) {
     constexpr int V = Pack16<TS>::V;
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t i = t / nseg;
-    if (i >= n) return;
-    const int64_t off = (t - i * nseg) * V;
-    TC acc[V];
+    const int rows_per_iter = blockDim.x / nseg;
+    const int rloc = threadIdx.x / nseg;
+    if (rloc >= rows_per_iter) return;
+    const int64_t off = (int64_t)(threadIdx.x - rloc * nseg) * V;
+    const bool line_head = ((off * (int64_t)sizeof(TS)) & 127) == 0;
+    const int64_t r_begin = (int64_t)blockIdx.x * chunk;
+    const int64_t r_end = min(n, r_begin + chunk);
+    for (int64_t i = r_begin + rloc; i < r_end; i += rows_per_iter) {
+        if (pf_z > 0 && line_head) {
+            if (i + pf_z < n) prefetch_l2(z + (i + pf_z) * ld + off);
+            if (i + pf_x < n) prefetch_l2(x + (i + pf_x) * ld + off);
+        }
+        TC acc[V];
 #pragma unroll
-    for (int v = 0; v < V; ++v) acc[v] = s_zero(TC());
-    op.row(i, [&](int64_t j, TC a) {
-        const Pack16<TS> p = ld16_ro(x + j * ld + off);
+        for (int v = 0; v < V; ++v) acc[v] = s_zero(TC());
+        op.row(i, [&](int64_t j, TC a) {
+            const Pack16<TS> p = ld16_ro(x + j * ld + off);
 #pragma unroll
-        for (int v = 0; v < V; ++v) acc[v] = s_fma(a, s_cvt<TC>(p.v[v]), acc[v]);
-    });
-    const Pack16<TS> xi = ld16_ro(x + i * ld + off);
-    const Pack16<TS> zi = ld16(z + i * ld + off);
-    Pack16<TS> out;
+            for (int v = 0; v < V; ++v) acc[v] = s_fma(a, s_cvt<TC>(p.v[v]), acc[v]);
+        });
+        const Pack16<TS> xi = ld16_ro(x + i * ld + off);
+        const Pack16<TS> zi = ld16(z + i * ld + off);
+        Pack16<TS> out;
 #pragma unroll
-    for (int v = 0; v < V; ++v) {
-        TC r = s_mul(alpha, acc[v]);
-        r = s_fma(beta, s_cvt<TC>(xi.v[v]), r);
-        r = s_fma(gamma, s_cvt<TC>(zi.v[v]), r);
-        out.v[v] = s_cvt<TS>(r);
+        for (int v = 0; v < V; ++v) {
+            TC r = s_mul(alpha, acc[v]);
+            r = s_fma(beta, s_cvt<TC>(xi.v[v]), r);
+            r = s_fma(gamma, s_cvt<TC>(zi.v[v]), r);
+            out.v[v] = s_cvt<TS>(r);
+        }
+        st16(y + i * ld + off, out);
     }
-    st16(y + i * ld + off, out);
+}
+
+// Middle step with the row's N entries gathered up front (padding (i, 0)); the 16-byte slices
+// of up to 9 neighbour rows are then loaded back to back before any arithmetic, so every
+// thread keeps several independent loads in flight.
+template <class Pol, class TS, class TC, int N>
+__global__ void __launch_bounds__(kRmThreads)
+rm_step_batched_kernel(Pol op, int64_t n, int nseg, int64_t ld, int64_t chunk, const TS* __restrict__ x,
+                       const TS* z, TS* y, TC alpha, TC beta, TC gamma) {
+    constexpr int V = Pack16<TS>::V;
+    constexpr int G = N <= 9 ? N : 9;
+    const int rows_per_iter = blockDim.x / nseg;
+    const int rloc = threadIdx.x / nseg;
+    if (rloc >= rows_per_iter) return;
+    const int64_t off = (int64_t)(threadIdx.x - rloc * nseg) * V;
+    const int64_t r_begin = (int64_t)blockIdx.x * chunk;
+    const int64_t r_end = min(n, r_begin + chunk);
+    for (int64_t i = r_begin + rloc; i < r_end; i += rows_per_iter) {
+        int64_t js[N];
+        TC as[N];
+        op.template gather<N>(i, js, as);
+        const Pack16<TS> zi = ld16(z + i * ld + off);
+        const Pack16<TS> xi = ld16_ro(x + i * ld + off);
+        TC acc[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) acc[v] = s_zero(TC());
+#pragma unroll
+        for (int b0 = 0; b0 < N; b0 += G) {
+            Pack16<TS> p[G];
+#pragma unroll
+            for (int g = 0; g < G; ++g)
+                if (b0 + g < N) p[g] = ld16_ro(x + js[b0 + g] * ld + off);
+#pragma unroll
+            for (int g = 0; g < G; ++g)
+                if (b0 + g < N) {
+#pragma unroll
+                    for (int v = 0; v < V; ++v) acc[v] = s_fma(as[b0 + g], s_cvt<TC>(p[g].v[v]), acc[v]);
+                }
+        }
+        Pack16<TS> out;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            TC r = s_mul(alpha, acc[v]);
+            r = s_fma(beta, s_cvt<TC>(xi.v[v]), r);
+            r = s_fma(gamma, s_cvt<TC>(zi.v[v]), r);
+            out.v[v] = s_cvt<TS>(r);
+        }
+        st16(y + i * ld + off, out);
+    }
 }
 
 // First step: one thread per row, CB columns per pass; reads the column-major input.
@@ -143,9 +211,13 @@ rm2cm_step_kernel(Pol op, int64_t n, int64_t s, int64_t ld, const TS* __restrict
 // ---------------------------------------------------------------------------------------
 // Driver
 // ---------------------------------------------------------------------------------------
-template <class Pol, class TS, class TC>
+// NB > 0: middle steps gather the row's NB entries up front (rm_step_batched_kernel);
+// NB == 0: middle steps walk the row entry by entry (rm_step_kernel).
+template <class Pol, class TS, class TC, int NB>
 static rc_status run_rm_filter(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, int64_t ldv, int64_t s,
-                               int64_t degree, double a, double b, void* bufA, void* bufB, int64_t ld) {
+                               int64_t degree, double a, double b, void* bufA, void* bufB, int64_t ld, int64_t band) {
+    const int64_t pf_z = ctx->pf_rows;
+    const int64_t pf_x = pf_z > 0 ? pf_z + band : 0;
     using TY = typename std::conditional<IsComplex<TC>::value, double2, double>::type;
     using R = real_t<TC>;
     constexpr int VEC = Pack16<TS>::V;
@@ -153,8 +225,24 @@ static rc_status run_rm_filter(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, 
     const TC ta = s_from<TC>(a, 0.0), tb = s_from<TC>(b, 0.0), tm1 = s_from<TC>(-1.0, 0.0);
     const unsigned grid_rows = (unsigned)((n + kRmThreads - 1) / kRmThreads);
     const int nseg = (int)(ld / VEC);
-    const int64_t nthreads = n * nseg;
-    const unsigned grid_seg = (unsigned)((nthreads + kRmThreads - 1) / kRmThreads);
+    if (nseg > kRmThreads) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "row-major filter: block too wide");
+    const int rows_per_iter = kRmThreads / nseg;
+    int64_t chunk, nblk;
+    if (ctx->rm_map == 1) {
+        // one wave of persistent CTAs, each owning a contiguous chunk of rows
+        int per_sm = 0;
+        RC_CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rm_step_kernel<Pol, TS, TC>, kRmThreads, 0));
+        if (per_sm < 1) per_sm = 1;
+        nblk = (int64_t)per_sm * ctx->sm_count;
+        chunk = (n + nblk - 1) / nblk;
+        chunk = ((chunk + rows_per_iter - 1) / rows_per_iter) * rows_per_iter;
+    } else {
+        // grid order: CTA b owns rows_per_iter consecutive rows, so the rows in flight form one
+        // contiguous band and a row's far neighbours were read one band earlier (still in L2)
+        chunk = rows_per_iter;
+    }
+    nblk = (n + chunk - 1) / chunk;
+    const unsigned grid_seg = (unsigned)nblk;
     TS* A = (TS*)bufA;  // even k (x0 copy, x2, x4, ...)
     TS* B = (TS*)bufB;  // odd k (x1, x3, ...)
     cm2rm_step_kernel<Pol, TY, TS, TC, CB><<<grid_rows, kRmThreads, 0, ctx->stream>>>(
@@ -164,8 +252,12 @@ static rc_status run_rm_filter(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, 
     for (int64_t k = 2; k < degree; ++k) {
         TS* xk1 = (k - 1) % 2 ? B : A;
         TS* xk2 = (k - 2) % 2 ? B : A;
-        rm_step_kernel<Pol, TS, TC><<<grid_seg, kRmThreads, 0, ctx->stream>>>(pol, n, nseg, ld, xk1, xk2, xk2, ta,
-                                                                               tb, tm1);
+        if constexpr (NB > 0)
+            rm_step_batched_kernel<Pol, TS, TC, NB><<<grid_seg, kRmThreads, 0, ctx->stream>>>(
+                pol, n, nseg, ld, chunk, xk1, xk2, xk2, ta, tb, tm1);
+        else
+            rm_step_kernel<Pol, TS, TC><<<grid_seg, kRmThreads, 0, ctx->stream>>>(pol, n, nseg, ld, chunk, xk1, xk2,
+                                                                                   xk2, ta, tb, tm1, pf_z, pf_x);
         ctx->launches++;
     }
     RC_CU(ctx, cudaGetLastError());
@@ -185,23 +277,41 @@ template <class TS, class TC>
 static rc_status rm_filter_dispatch(rc_ctx* ctx, rc_op* op, void* V, int64_t ldv, int64_t s, int64_t degree,
                                     double a, double b, void* bufA, void* bufB, int64_t ld) {
     const int64_t n = op->n;
+    const int64_t band = op->kind == 0 ? op->band : (op->skind == 5 ? op->nx : op->nx * op->ny);
     if (op->kind == 0) {
         CsrRows<TS, TC> pol{op->rowptr, op->colind, (const TS*)(sizeof(real_t<TS>) == 8 ? op->vals64 : op->vals32)};
-        return run_rm_filter<CsrRows<TS, TC>, TS, TC>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld);
+        using P = CsrRows<TS, TC>;
+        if (ctx->csr_variant == 2 && op->max_row_nnz <= 8)
+            return run_rm_filter<P, TS, TC, 8>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band);
+        if (ctx->csr_variant == 2 && op->max_row_nnz <= 32)
+            return run_rm_filter<P, TS, TC, 32>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band);
+        return run_rm_filter<P, TS, TC, 0>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band);
     }
     using TD = real_t<TS>;
     const TD* dg = (const TD*)(sizeof(TD) == 8 ? (const void*)op->diag64 : (const void*)op->diag32);
     const double theta = 2.0 * 3.14159265358979323846 * op->flux;
     if (op->skind == 27) {
         StencilRows<TD, TC, 27> pol{op->nx, op->ny, op->nz, dg, op->offdiag, theta};
-        return run_rm_filter<StencilRows<TD, TC, 27>, TS, TC>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld);
+        return ctx->csr_variant != 2
+                   ? run_rm_filter<StencilRows<TD, TC, 27>, TS, TC, 0>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld,
+                                                                     band)
+                   : run_rm_filter<StencilRows<TD, TC, 27>, TS, TC, 27>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB,
+                                                                      ld, band);
     }
     if (op->skind == 7) {
         StencilRows<TD, TC, 7> pol{op->nx, op->ny, op->nz, dg, op->offdiag, theta};
-        return run_rm_filter<StencilRows<TD, TC, 7>, TS, TC>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld);
+        return ctx->csr_variant != 2
+                   ? run_rm_filter<StencilRows<TD, TC, 7>, TS, TC, 0>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld,
+                                                                     band)
+                   : run_rm_filter<StencilRows<TD, TC, 7>, TS, TC, 7>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB,
+                                                                      ld, band);
     }
     StencilRows<TD, TC, 5> pol{op->nx, op->ny, op->nz, dg, op->offdiag, theta};
-    return run_rm_filter<StencilRows<TD, TC, 5>, TS, TC>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld);
+    return ctx->csr_variant != 2
+                   ? run_rm_filter<StencilRows<TD, TC, 5>, TS, TC, 0>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld,
+                                                                     band)
+                   : run_rm_filter<StencilRows<TD, TC, 5>, TS, TC, 5>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB,
+                                                                      ld, band);
 }
 
 int64_t rm_leading_dim(int dtype, int prec, int64_t s) {

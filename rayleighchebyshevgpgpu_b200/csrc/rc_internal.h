@@ -33,6 +33,11 @@ struct rc_ctx {
     // CSR step kernel: 0 auto (register-cached rows when every row has <= 8 entries),
     // 1 row loop, 2 register-cached rows. Read from RCB200_CSR_KERNEL at context creation.
     int csr_variant = 0;
+    // row-major filter step mapping: 0 grid order (default), 1 persistent contiguous chunks.
+    // Read from RCB200_RM_MAP ("grid" / "persist") at context creation.
+    int rm_map = 0;
+    // L2 prefetch distance (rows) of the row-major filter steps; 0 = off. RCB200_PF_ROWS.
+    int64_t pf_rows = 0;
 };
 
 enum Slot {
@@ -48,6 +53,7 @@ struct rc_op {
     // CSR
     int64_t nnz = 0;
     int64_t max_row_nnz = 0;
+    int64_t band = 0;  // max over entries of (column - row): distance to the farthest later neighbour
     int32_t* rowptr = nullptr;
     int32_t* colind = nullptr;
     void* vals64 = nullptr;
@@ -116,7 +122,8 @@ rc_status ensure_fp32(rc_ctx* ctx, rc_op* op);
 rc_status gram(rc_ctx* ctx, int dtype, int64_t n, int64_t m, int64_t nc, const void* X, int64_t ldx,
                const void* Y, int64_t ldy, void* C, bool upper);
 // Y (n x nc) = beta*Y + alpha * X (n x k) * T (k x nc, ld ldt). Y must not alias X.
-// Optional dual: Y2 = X2 * T and residual partials ||Y2_c - lam_c Y_c||^2 for c < res_count.
+// Optional dual: X2 * T (stored in Y2 unless Y2 is null) and residual norms
+// ||(X2 T)_c - lam_c Y_c|| for c < res_count.
 struct XtArgs {
     int64_t n = 0, k = 0, nc = 0;
     const void* X = nullptr; int64_t ldx = 0;
@@ -130,6 +137,16 @@ struct XtArgs {
     double* res = nullptr;  // device output, res_count residual norms
 };
 rc_status xt(rc_ctx* ctx, int dtype, const XtArgs& a);
+
+// FP64 real fast paths (s <= 96), rc_gemm.cu. gram2: C0 = X^T Y0 (and C1 = X^T Y1 when Y1),
+// symmetric results. xt2: Y = X T, plus residual norms of W T against lam when W is given.
+bool gram2_supported(int dtype, int64_t m);
+rc_status gram2(rc_ctx* ctx, int64_t n, int64_t m, const double* X, int64_t ldx, const double* Y0, int64_t ldy0,
+                double* C0, const double* Y1, int64_t ldy1, double* C1);
+bool xt2_supported(int dtype, int64_t k, int64_t nc);
+rc_status xt2(rc_ctx* ctx, int64_t n, int64_t k, int64_t nc, const double* X, int64_t ldx, const double* T,
+              int64_t ldt, double* Y, int64_t ldy, const double* W, int64_t ldw, const double* lam, int64_t res_count,
+              double* res);
 
 // Cholesky factor of Gram G (s x s) with diagonal scaling, shift on breakdown;
 // writes Tout = D^-1 R^-1 (upper). flags (device int[4]): [0] shifted, [1] failed, [2] zero column.

@@ -226,11 +226,10 @@ rc_status Solver::rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool rea
     a.T = Q_; a.ldt = s;
     a.Y = T1_; a.ldy = n_;
     a.X2 = AX; a.ldx2 = n_;
-    a.Y2 = T2_; a.ldy2 = n_;
+    a.Y2 = nullptr;  // only the residual norms of (A X) Q are needed
     a.lam = dlam_; a.res_count = res_count; a.res = dres_;
     RC_TRY(xt(ctx_, dtype_, a));
     std::swap(X, T1_);
-    std::swap(AX, T2_);
     if (read_back) {
         RC_CU(ctx_, cudaMemcpyAsync(hbuf_, dlam_, s * sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
         if (res_count > 0)
@@ -258,8 +257,13 @@ rc_status Solver::rr_fused(int64_t s, int64_t res_count, bool* ok) {
     st.y = W_; st.yp = P64; st.ldy = n_;
     st.cp = P64;
     RC_TRY(op_step(ctx_, op_, st));
-    RC_TRY(gram(ctx_, dtype_, n_, s, s, V_, n_, V_, n_, G_, true));
-    RC_TRY(gram(ctx_, dtype_, n_, s, s, V_, n_, W_, n_, H_, true));
+    if (gram2_supported(dtype_, s)) {
+        RC_TRY(gram2(ctx_, n_, s, (const double*)V_, n_, (const double*)V_, n_, (double*)G_, (const double*)W_, n_,
+                     (double*)H_));
+    } else {
+        RC_TRY(gram(ctx_, dtype_, n_, s, s, V_, n_, V_, n_, G_, true));
+        RC_TRY(gram(ctx_, dtype_, n_, s, s, V_, n_, W_, n_, H_, true));
+    }
     RC_CU(ctx_, cudaMemsetAsync(dflags_, 0, 4 * sizeof(int), ctx_->stream));
     RC_TRY(chol_factor(ctx_, dtype_, s, n_, G_, Tt_, dflags_, dpiv_));
     RC_TRY(small_gemm(ctx_, dtype_, s, H_, false, Tt_, M1_));   // H T
@@ -273,7 +277,7 @@ rc_status Solver::rr_fused(int64_t s, int64_t res_count, bool* ok) {
     a.T = Q_; a.ldt = s;
     a.Y = T1_; a.ldy = n_;
     a.X2 = W_; a.ldx2 = n_;
-    a.Y2 = T2_; a.ldy2 = n_;
+    a.Y2 = nullptr;  // only the residual norms of W Q are needed
     a.lam = dlam_; a.res_count = res_count; a.res = dres_;
     RC_TRY(xt(ctx_, dtype_, a));
     RC_CU(ctx_, cudaMemcpyAsync(hbuf_, dlam_, s * sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
@@ -293,7 +297,6 @@ rc_status Solver::rr_fused(int64_t s, int64_t res_count, bool* ok) {
     }
     ++fused_ok_;
     std::swap(V_, T1_);
-    std::swap(W_, T2_);
     VtAVeigValue_.assign(hbuf_, hbuf_ + s);
     subspaceResiduals_.assign(hbuf_ + s, hbuf_ + s + res_count);
     return RC_OK;

@@ -133,6 +133,20 @@ def test_cholqr_orthonormal_and_same_span(ctx):
         assert (np.linalg.norm(resid, axis=0) / np.linalg.norm(X, axis=0)).max() < 1e-6
 
 
+@pytest.mark.parametrize("s", [96, 70, 33, 17])
+def test_cholqr_block_widths(ctx, s):
+    """Tall-skinny Gram / X*T paths at the widths of the benchmark blocks (24, 48, 96) and ragged ones."""
+    rng = np.random.default_rng(s)
+    n = 20011
+    V = rng.standard_normal((n, s)) * np.logspace(0, 3, s)
+    Xd = _dev(V.T)
+    R.cholqr(ctx, Xd, n, s, False)
+    Qm = _host(Xd).T
+    assert np.abs(Qm.T @ Qm - np.eye(s)).max() < 1e-12
+    resid = V - Qm @ (Qm.T @ V)
+    assert (np.linalg.norm(resid, axis=0) / np.linalg.norm(V, axis=0)).max() < 1e-10
+
+
 @pytest.mark.parametrize("s,complex_", [(24, False), (96, False), (150, False), (40, True), (130, True), (7, False)])
 def test_small_eigh_matches_lapack(ctx, s, complex_):
     rng = np.random.default_rng(s)
