@@ -8,9 +8,9 @@
 // neighbour row is one contiguous run and each thread of the middle steps owns a 16-byte slice
 // of a row: every gather is a coalesced 128-bit load, and the matrix entries of a row are
 // broadcast to the threads of that row.
-//   step 1     (cm2rm): X column-major -> x1 row-major, plus a row-major copy of x0
-//   step k<m   (rm):    x_k over x_{k-2}, both row-major (one pass: read x_{k-1}, x_{k-2}, write x_k)
-//   step m     (rm2cm): x_m (scaled by 1/(m+1)) into X column-major
+//   to_rm:     X column-major (FP64) -> x0 row-major (storage precision), 32x32 smem tiles
+//   step k:    x_k over x_{k-2}, row-major (one pass: read x_{k-1}, x_{k-2}, write x_k)
+//   to_cm:     x_m/(m+1) row-major -> X column-major (FP64)
 // Storage/compute: FP32 (c64) in MIXED precision, FP64 (c128) otherwise.
 #include <cstring>
 #include "rc_common.cuh"
@@ -147,129 +147,107 @@ rm_step_batched_kernel(Pol op, int64_t n, int nseg, int64_t ld, int64_t chunk, c
     }
 }
 
-// First step: one thread per row, CB columns per pass; reads the column-major input.
-template <class Pol, class TX, class TS, class TC, int CB>
-__global__ void __launch_bounds__(kRmThreads)
-cm2rm_step_kernel(Pol op, int64_t n, int64_t s, const TX* __restrict__ x, int64_t ldx, TS* __restrict__ y,
-                  TS* __restrict__ x0c, int64_t ld, TC alpha, TC beta) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    for (int64_t c0 = 0; c0 < s; c0 += CB) {
-        const int nb = (int)((s - c0) < CB ? (s - c0) : CB);
-        TC acc[CB];
+// Layout change between the caller's column-major FP64 block and the row-major scratch, through
+// 32x32 shared-memory tiles (coalesced on both sides), converting precision and scaling.
+//   to_rm:  R[i*ld + c] = (TS) V[i + c*ldv]
+//   to_cm:  V[i + c*ldv] = scale * R[i*ld + c]
+template <class TV, class TS>
+__global__ void __launch_bounds__(256)
+to_rm_kernel(int64_t n, int64_t s, const TV* __restrict__ Vc, int64_t ldv, TS* __restrict__ Rr, int64_t ld) {
+    __shared__ TS tile[32][33];
+    const int64_t r0 = (int64_t)blockIdx.y * 32, c0 = (int64_t)blockIdx.x * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
 #pragma unroll
-        for (int cc = 0; cc < CB; ++cc) acc[cc] = s_zero(TC());
-        const TX* xc = x + c0 * ldx;
-        op.row(i, [&](int64_t j, TC a) {
+    for (int j = 0; j < 4; ++j) {
+        const int64_t c = c0 + ty + 8 * j, r = r0 + tx;
+        tile[ty + 8 * j][tx] = (r < n && c < s) ? s_cvt<TS>(Vc[r + c * ldv]) : s_zero(TS());
+    }
+    __syncthreads();
 #pragma unroll
-            for (int cc = 0; cc < CB; ++cc)
-                if (cc < nb) acc[cc] = s_fma(a, s_cvt<TC>(xc[j + cc * ldx]), acc[cc]);
-        });
-#pragma unroll
-        for (int cc = 0; cc < CB; ++cc) {
-            if (cc < nb) {
-                const TC xv = s_cvt<TC>(xc[i + cc * ldx]);
-                TC r = s_mul(alpha, acc[cc]);
-                r = s_fma(beta, xv, r);
-                y[i * ld + c0 + cc] = s_cvt<TS>(r);
-                x0c[i * ld + c0 + cc] = s_cvt<TS>(xv);
-            }
-        }
+    for (int j = 0; j < 4; ++j) {
+        const int64_t r = r0 + ty + 8 * j, c = c0 + tx;
+        if (r < n && c < s) Rr[r * ld + c] = tile[tx][ty + 8 * j];
     }
 }
 
-// Last step: one thread per row; gathers row-major slices, writes the column-major output.
-template <class Pol, class TS, class TY, class TC, int CB>
-__global__ void __launch_bounds__(kRmThreads)
-rm2cm_step_kernel(Pol op, int64_t n, int64_t s, int64_t ld, const TS* __restrict__ x, const TS* __restrict__ z,
-                  TY* __restrict__ y, int64_t ldy, TC alpha, TC beta, TC gamma, real_t<TC> scale) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    for (int64_t c0 = 0; c0 < s; c0 += CB) {
-        const int nb = (int)((s - c0) < CB ? (s - c0) : CB);
-        TC acc[CB];
+template <class TS, class TV>
+__global__ void __launch_bounds__(256)
+to_cm_kernel(int64_t n, int64_t s, const TS* __restrict__ Rr, int64_t ld, TV* __restrict__ Vc, int64_t ldv,
+             double scale) {
+    __shared__ TS tile[32][33];
+    const int64_t r0 = (int64_t)blockIdx.y * 32, c0 = (int64_t)blockIdx.x * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
 #pragma unroll
-        for (int cc = 0; cc < CB; ++cc) acc[cc] = s_zero(TC());
-        op.row(i, [&](int64_t j, TC a) {
-            const TS* xr = x + j * ld + c0;
+    for (int j = 0; j < 4; ++j) {
+        const int64_t r = r0 + ty + 8 * j, c = c0 + tx;
+        tile[ty + 8 * j][tx] = (r < n && c < s) ? Rr[r * ld + c] : s_zero(TS());
+    }
+    __syncthreads();
 #pragma unroll
-            for (int cc = 0; cc < CB; ++cc)
-                if (cc < nb) acc[cc] = s_fma(a, s_cvt<TC>(xr[cc]), acc[cc]);
-        });
-#pragma unroll
-        for (int cc = 0; cc < CB; ++cc) {
-            if (cc < nb) {
-                TC r = s_mul(alpha, acc[cc]);
-                r = s_fma(beta, s_cvt<TC>(x[i * ld + c0 + cc]), r);
-                r = s_fma(gamma, s_cvt<TC>(z[i * ld + c0 + cc]), r);
-                y[i + (c0 + cc) * ldy] = s_cvt<TY>(s_rscale(scale, r));
-            }
-        }
+    for (int j = 0; j < 4; ++j) {
+        const int64_t c = c0 + ty + 8 * j, r = r0 + tx;
+        if (r < n && c < s) Vc[r + c * ldv] = s_rscale((real_t<TV>)scale, s_cvt<TV>(tile[tx][ty + 8 * j]));
     }
 }
 
 // ---------------------------------------------------------------------------------------
 // Driver
 // ---------------------------------------------------------------------------------------
-// NB > 0: middle steps gather the row's NB entries up front (rm_step_batched_kernel);
-// NB == 0: middle steps walk the row entry by entry (rm_step_kernel).
+// NB > 0: steps gather the row's NB entries up front (rm_step_batched_kernel);
+// NB == 0: steps walk the row entry by entry (rm_step_kernel, with L2 prefetch).
+//   A <- X (row-major copy of x0); x_k (k = 1..m) into B, A, B, ... (x_k over x_{k-2});
+//   X <- x_m / (m+1) (column-major).
 template <class Pol, class TS, class TC, int NB>
 static rc_status run_rm_filter(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, int64_t ldv, int64_t s,
                                int64_t degree, double a, double b, void* bufA, void* bufB, int64_t ld, int64_t band) {
     const int64_t pf_z = ctx->pf_rows;
     const int64_t pf_x = pf_z > 0 ? pf_z + band : 0;
     using TY = typename std::conditional<IsComplex<TC>::value, double2, double>::type;
-    using R = real_t<TC>;
     constexpr int VEC = Pack16<TS>::V;
-    constexpr int CB = sizeof(TS) >= 16 ? 2 : (sizeof(TS) == 8 ? 4 : 8);
     const TC ta = s_from<TC>(a, 0.0), tb = s_from<TC>(b, 0.0), tm1 = s_from<TC>(-1.0, 0.0);
-    const unsigned grid_rows = (unsigned)((n + kRmThreads - 1) / kRmThreads);
     const int nseg = (int)(ld / VEC);
     if (nseg > kRmThreads) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "row-major filter: block too wide");
     const int rows_per_iter = kRmThreads / nseg;
-    int64_t chunk, nblk;
+    int64_t chunk;
     if (ctx->rm_map == 1) {
         // one wave of persistent CTAs, each owning a contiguous chunk of rows
         int per_sm = 0;
         RC_CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rm_step_kernel<Pol, TS, TC>, kRmThreads, 0));
         if (per_sm < 1) per_sm = 1;
-        nblk = (int64_t)per_sm * ctx->sm_count;
-        chunk = (n + nblk - 1) / nblk;
+        const int64_t nb0 = (int64_t)per_sm * ctx->sm_count;
+        chunk = (n + nb0 - 1) / nb0;
         chunk = ((chunk + rows_per_iter - 1) / rows_per_iter) * rows_per_iter;
     } else {
         // grid order: CTA b owns rows_per_iter consecutive rows, so the rows in flight form one
         // contiguous band and a row's far neighbours were read one band earlier (still in L2)
         chunk = rows_per_iter;
     }
-    nblk = (n + chunk - 1) / chunk;
-    const unsigned grid_seg = (unsigned)nblk;
-    TS* A = (TS*)bufA;  // even k (x0 copy, x2, x4, ...)
-    TS* B = (TS*)bufB;  // odd k (x1, x3, ...)
-    cm2rm_step_kernel<Pol, TY, TS, TC, CB><<<grid_rows, kRmThreads, 0, ctx->stream>>>(
-        pol, n, s, (const TY*)V, ldv, B, A, ld, ta, tb);
+    const unsigned grid_seg = (unsigned)((n + chunk - 1) / chunk);
+    const dim3 tgrid((unsigned)((s + 31) / 32), (unsigned)((n + 31) / 32)), tblk(32, 8);
+    TS* A = (TS*)bufA;
+    TS* B = (TS*)bufB;
+    to_rm_kernel<TY, TS><<<tgrid, tblk, 0, ctx->stream>>>(n, s, (const TY*)V, ldv, A, ld);
     ctx->launches++;
     RC_CU(ctx, cudaGetLastError());
-    for (int64_t k = 2; k < degree; ++k) {
-        TS* xk1 = (k - 1) % 2 ? B : A;
-        TS* xk2 = (k - 2) % 2 ? B : A;
+    for (int64_t k = 1; k <= degree; ++k) {
+        TS* xk1 = (k - 1) % 2 ? B : A;  // x_{k-1}
+        TS* y = k % 2 ? B : A;          // x_k overwrites x_{k-2}
+        // k = 1 has no x_{k-2}: z = x0 (finite data) with gamma = 0
+        const TS* z = k >= 2 ? y : A;
+        const TC g = k >= 2 ? tm1 : s_zero(TC());
         if constexpr (NB > 0)
             rm_step_batched_kernel<Pol, TS, TC, NB><<<grid_seg, kRmThreads, 0, ctx->stream>>>(
-                pol, n, nseg, ld, chunk, xk1, xk2, xk2, ta, tb, tm1);
+                pol, n, nseg, ld, chunk, xk1, z, y, ta, tb, g);
         else
-            rm_step_kernel<Pol, TS, TC><<<grid_seg, kRmThreads, 0, ctx->stream>>>(pol, n, nseg, ld, chunk, xk1, xk2,
-                                                                                   xk2, ta, tb, tm1, pf_z, pf_x);
+            rm_step_kernel<Pol, TS, TC><<<grid_seg, kRmThreads, 0, ctx->stream>>>(pol, n, nseg, ld, chunk, xk1, z, y,
+                                                                                   ta, tb, g, pf_z, pf_x);
         ctx->launches++;
     }
     RC_CU(ctx, cudaGetLastError());
-    {
-        const int64_t k = degree;
-        TS* xk1 = (k - 1) % 2 ? B : A;
-        TS* xk2 = (k - 2) % 2 ? B : A;
-        rm2cm_step_kernel<Pol, TS, TY, TC, CB><<<grid_rows, kRmThreads, 0, ctx->stream>>>(
-            pol, n, s, ld, xk1, xk2, (TY*)V, ldv, ta, tb, tm1, (R)(1.0 / (double)(degree + 1)));
-        ctx->launches++;
-        RC_CU(ctx, cudaGetLastError());
-    }
+    TS* xm = degree % 2 ? B : A;
+    to_cm_kernel<TS, TY><<<tgrid, tblk, 0, ctx->stream>>>(n, s, xm, ld, (TY*)V, ldv, 1.0 / (double)(degree + 1));
+    ctx->launches++;
+    RC_CU(ctx, cudaGetLastError());
     return RC_OK;
 }
 
