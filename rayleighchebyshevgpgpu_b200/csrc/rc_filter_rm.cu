@@ -155,7 +155,7 @@ template <class TV, class TS>
 __global__ void __launch_bounds__(256)
 to_rm_kernel(int64_t n, int64_t s, const TV* __restrict__ Vc, int64_t ldv, TS* __restrict__ Rr, int64_t ld) {
     __shared__ TS tile[32][33];
-    const int64_t r0 = (int64_t)blockIdx.y * 32, c0 = (int64_t)blockIdx.x * 32;
+    const int64_t r0 = (int64_t)blockIdx.x * 32, c0 = (int64_t)blockIdx.y * 32;  // rows on x (no 65535 cap)
     const int tx = threadIdx.x, ty = threadIdx.y;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(256)
 to_cm_kernel(int64_t n, int64_t s, const TS* __restrict__ Rr, int64_t ld, TV* __restrict__ Vc, int64_t ldv,
              double scale) {
     __shared__ TS tile[32][33];
-    const int64_t r0 = (int64_t)blockIdx.y * 32, c0 = (int64_t)blockIdx.x * 32;
+    const int64_t r0 = (int64_t)blockIdx.x * 32, c0 = (int64_t)blockIdx.y * 32;  // rows on x (no 65535 cap)
     const int tx = threadIdx.x, ty = threadIdx.y;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -223,7 +223,8 @@ static rc_status run_rm_filter(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, 
         chunk = rows_per_iter;
     }
     const unsigned grid_seg = (unsigned)((n + chunk - 1) / chunk);
-    const dim3 tgrid((unsigned)((s + 31) / 32), (unsigned)((n + 31) / 32)), tblk(32, 8);
+    if ((s + 31) / 32 > 65535) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "row-major filter: too many columns");
+    const dim3 tgrid((unsigned)((n + 31) / 32), (unsigned)((s + 31) / 32)), tblk(32, 8);
     TS* A = (TS*)bufA;
     TS* B = (TS*)bufB;
     to_rm_kernel<TY, TS><<<tgrid, tblk, 0, ctx->stream>>>(n, s, (const TY*)V, ldv, A, ld);
