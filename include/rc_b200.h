@@ -172,6 +172,17 @@ rc_status rc_rayleigh_ritz(rc_ctx* ctx, const rc_op* op, void* V, void* W, int64
  * Replaces DSYEV/ZHPEVX (RayleighChebyshevLMCuda.h:614,618) and JacobiDiagonalizer. */
 rc_status rc_small_eigh(rc_ctx* ctx, int dtype, int64_t s, const void* H, double* evals, void* Q);
 
+/* rc_small_eigh for callers that must not allocate device memory (for example inside a CUDA
+ * stream capture, under a fixed memory budget, or from a callback of another library): same
+ * arguments and results, but the device staging and work memory come from one fixed array of
+ * this library (about 1 MiB, held on every GPU that loads the library until the process exits),
+ * and no cudaMalloc/cudaFree is called. s must be at most 128 (RC_ERR_INVALID otherwise). The
+ * first call on a device looks up the array's device address, so make that first call before
+ * any stream capture. All calls share the array: calls whose GPU work overlaps (several host
+ * threads, or several contexts on one device) race on it and must be serialised by the caller.
+ * This entry point has no counterpart in the reference. */
+rc_status rc_small_eigh_noalloc(rc_ctx* ctx, int dtype, int64_t s, const void* H, double* evals, void* Q);
+
 /* ------------------------------------------------------------------------------------
  * Whole solve: RayleighChebyshevLMCuda::getMinEigenSystem / getMinIntervalEigenSystem
  * (RayleighChebyshevLMCuda.h:775,794,827,876; base routine :896-1973).

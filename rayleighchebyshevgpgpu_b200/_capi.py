@@ -123,6 +123,7 @@ SIGNATURES = {
     "rc_cholqr": (C.c_int, [c_vp, C.c_int, c_vp, c_i64, c_i64, c_i64, C.POINTER(C.c_int)]),
     "rc_rayleigh_ritz": (C.c_int, [c_vp, c_vp, c_vp, c_vp, c_i64, c_i64, c_i64, c_dp, c_dp, c_vp]),
     "rc_small_eigh": (C.c_int, [c_vp, C.c_int, c_i64, c_vp, c_dp, c_vp]),
+    "rc_small_eigh_noalloc": (C.c_int, [c_vp, C.c_int, c_i64, c_vp, c_dp, c_vp]),
     "rc_solve_params_default": (None, [C.POINTER(SolveParams)]),
     "rc_solve": (C.c_int, [c_vp, c_vp, C.POINTER(SolveParams), c_vp, c_dp, c_vp, c_dp, C.POINTER(SolveInfo)]),
 }

@@ -21,7 +21,7 @@ NVCC_FLAGS = ARCH_FLAGS + [
     "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
     "--expt-relaxed-constexpr", "-Xptxas", "-O3",
 ]
-SOURCES = ["rc_filter.cu", "rc_filter_rm.cu", "rc_dense.cu", "rc_gemm.cu", "rc_lanczos.cu", "rc_solver.cu", "rc_capi.cu"]
+SOURCES = ["rc_filter.cu", "rc_filter_rm.cu", "rc_dense.cu", "rc_gemm.cu", "rc_noalloc.cu", "rc_lanczos.cu", "rc_solver.cu", "rc_capi.cu"]
 
 
 def _nvcc() -> str:

@@ -603,7 +603,23 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
     if (tid == 0 && info) info[0] = sweep;
 }
 
+size_t small_eigh_work_bytes(rc_ctx* ctx, int dtype, int64_t s) {
+    const size_t esz = dtype == RC_COMPLEX128 ? 16 : 8;
+    const int64_t sp = s + (s & 1);
+    const int64_t npair = sp / 2;
+    const size_t head = (((size_t)npair * (16 + esz + 8) + 15) / 16) * 16;
+    const size_t mats = 2 * (size_t)sp * (sp + 1) * esz;
+    return head + mats <= (size_t)ctx->smem_optin - 2048 ? 0 : mats;
+}
+
 rc_status small_eigh(rc_ctx* ctx, int dtype, int64_t s, void* A, void* Q, double* evals, int* info) {
+    void* work = nullptr;
+    const size_t wb = small_eigh_work_bytes(ctx, dtype, s);
+    if (wb) RC_TRY(rc_slot(ctx, S_EIG, wb + 256, &work));
+    return small_eigh_work(ctx, dtype, s, A, Q, evals, info, work);
+}
+
+rc_status small_eigh_work(rc_ctx* ctx, int dtype, int64_t s, void* A, void* Q, double* evals, int* info, void* work) {
     const size_t esz = dtype == RC_COMPLEX128 ? 16 : 8;
     const int64_t sp = s + (s & 1);
     const int64_t npair = sp / 2;
@@ -611,8 +627,7 @@ rc_status small_eigh(rc_ctx* ctx, int dtype, int64_t s, void* A, void* Q, double
     const size_t mats = 2 * (size_t)sp * (sp + 1) * esz;
     const bool fit = head + mats <= (size_t)ctx->smem_optin - 2048;
     const size_t dyn = fit ? head + mats : head;
-    void* work = nullptr;
-    if (!fit) RC_TRY(rc_slot(ctx, S_EIG, mats + 256, &work));
+    if (!fit && !work) return rc_fail(ctx, RC_ERR_INVALID, "small_eigh: work memory required");
     const int sweeps = 60;
     if (dtype == RC_COMPLEX128) {
         if (dyn > 48 * 1024)

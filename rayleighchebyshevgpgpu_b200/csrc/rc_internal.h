@@ -155,6 +155,10 @@ rc_status chol_factor(rc_ctx* ctx, int dtype, int64_t s, int64_t nrows, const vo
                       int* flags, double* pivout);
 // Hermitian eigensolve (parallel Jacobi, one CTA). A (s x s) is read only; evals ascending.
 rc_status small_eigh(rc_ctx* ctx, int dtype, int64_t s, void* A, void* Q, double* evals, int* info);
+// Same with caller-provided work memory (small_eigh_work_bytes(...) bytes, 0 when the working
+// copies fit in shared memory; 256-byte aligned).
+size_t small_eigh_work_bytes(rc_ctx* ctx, int dtype, int64_t s);
+rc_status small_eigh_work(rc_ctx* ctx, int dtype, int64_t s, void* A, void* Q, double* evals, int* info, void* work);
 // C = op(A) B for s x s matrices (op = conjugate transpose when transA), and C <- (C + C^H)/2.
 rc_status small_gemm(rc_ctx* ctx, int dtype, int64_t s, const void* A, bool transA, const void* B, void* C);
 rc_status hermitize(rc_ctx* ctx, int dtype, int64_t s, void* C);
