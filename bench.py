@@ -32,7 +32,21 @@ METRIC = "time-to-solution & eigenpairs/s at resid<=1e-10, mixed vs FP64 on 1 B2
 # Degree-steps of a whole FP64 solve of configuration 2 on the GPU path: multiplies the reference CPU
 # per-degree-step time into its time-to-solution estimate (the CPU solve itself runs for hours).
 # Measured by this bench (fp64 leg, info.degree_steps); refreshed when the solver changes.
-CONFIG2_FP64_DEGREE_STEPS = 2400
+CONFIG2_FP64_DEGREE_STEPS = 1659
+
+
+def profile_dram_bytes_per_row():
+    """DRAM bytes per grid row of one filter degree-step, from the committed ncu summary
+    (a line "dram-bytes-per-row fp32=<B> fp64=<B>"), or None."""
+    path = os.path.join(ROOT, "profiles", "rm_step_kernel_csr_96cube_s96.md")
+    try:
+        for line in open(path):
+            if line.startswith("dram-bytes-per-row"):
+                kv = dict(t.split("=") for t in line.split()[1:])
+                return {"fp32": float(kv["fp32"]), "fp64": float(kv["fp64"])}
+    except (OSError, ValueError, KeyError):
+        return None
+    return None
 
 
 def parse():
@@ -290,7 +304,12 @@ def run_ours(args):
     e2e_value = P.k * world / max_over_ranks(statistics.median(e2e_t))
     assert np.array_equal(res_e.evals, res_mixed.evals)
 
-    # ---- roofline of the dominant kernel (the fused filter step), from the timed solves ----
+    # ---- roofline of the dominant kernel: the fused filter degree-step (rm_step_kernel) ----
+    # Algorithmic bytes of one degree-step over the n x s block: the matrix once (values + column
+    # indices + row pointers) and three block passes (read x_{k-1}, read x_{k-2}, write x_k).
+    # The step time is the CUDA-event time of the degree-step launches inside the timed solves
+    # (info.time_filter_steps_ms, transposes excluded). Degree-1 filters (column-major path, at
+    # most a few per solve) are counted in degree_steps but not timed, a < 0.1 % overstatement.
     nnz = ci.size
     b_a32 = nnz * (4 + 4) + (P.n + 1) * 4
     b_a64 = nnz * (8 + 4) + (P.n + 1) * 4
@@ -298,23 +317,21 @@ def run_ours(args):
     bytes_fp64_step = b_a64 + 3 * P.n * s * 8
     fsteps = sum(i["degree_steps"] for i in infos)
     f64steps = sum(i["fp64_degree_steps"] for i in infos)
-    ftime = sum(i["time_filter_ms"] for i in infos) * 1e-3
+    tsteps = sum(i["time_filter_steps_ms"] for i in infos) * 1e-3
     alg_bytes = (fsteps - f64steps) * bytes_fp32_step + f64steps * bytes_fp64_step
-    achieved = alg_bytes / ftime / 1e9 if ftime > 0 else None
+    achieved = alg_bytes / tsteps / 1e9 if tsteps > 0 else None
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         peak, peak_src = float(peaks["hbm_gbs"]), "measured"
     except Exception:
         peak, peak_src = 6650.0, "fallback"
+    # DRAM bytes per launch: the per-row figures of the ncu capture of the same kernel on the
+    # 96^3 grid (profiles/), scaled to this block by its row count, mixed by precision like achieved
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "filter_step_traffic.json")
-    if os.path.exists(tp):
-        try:
-            traffic = json.load(open(tp)).get("dram_bytes_per_launch")
-        except Exception:
-            traffic = None
-
+    per_row = profile_dram_bytes_per_row()
+    if per_row and fsteps:
+        traffic = P.n * ((fsteps - f64steps) * per_row["fp32"] + f64steps * per_row["fp64"]) / fsteps
     # ---- CPU baseline (rank 0, N = 1) ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -347,12 +364,16 @@ def run_ours(args):
                                                                "mixed_iterations", "lanczos_iterations",
                                                                "cholqr_passes", "fused_rr", "fused_rr_fallbacks",
                                                                "time_lanczos_ms", "time_filter_ms",
+                                                               "time_filter_steps_ms",
                                                                "time_ortho_ms", "time_eigenvalue_ms")},
                        "fp64": {k2: info64[k2] for k2 in ("inner_iterations", "degree_steps", "time_filter_ms",
+                                                           "time_filter_steps_ms",
                                                            "time_ortho_ms", "time_eigenvalue_ms")} if info64 else None},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "peak_source": peak_src, "kernel": "csr_step_kernel (fused filter degree-step)",
+                     "peak_source": peak_src, "kernel": "rm_step_kernel (fused filter degree-step, CSR)",
+                     "algorithmic_bytes_per_launch": alg_bytes / fsteps if fsteps else None,
+                     "launches": fsteps, "fp64_launches": f64steps,
                      "bytes_per_launch_fp32": bytes_fp32_step, "bytes_per_launch_fp64": bytes_fp64_step},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "eigenpairs/s", "h2d_bytes_per_step": int(h2d),

@@ -253,6 +253,8 @@ typedef struct rc_solve_info {
     double guard_value;            /* getGuardEigenvalue */
     int64_t fused_rr;              /* inner iterations whose Rayleigh-Ritz ran on the filtered block */
     int64_t fused_rr_fallbacks;    /* of those, rejected for conditioning and redone after CholeskyQR2 */
+    double time_filter_steps_ms;   /* part of time_filter_ms spent in the fused degree-step launches
+                                      themselves (row-major filter, transposes excluded; phase_timing = 1) */
 } rc_solve_info;
 
 void rc_solve_params_default(rc_solve_params* p);

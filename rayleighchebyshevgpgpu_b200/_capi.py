@@ -90,6 +90,7 @@ class SolveInfo(C.Structure):
         ("guard_value", C.c_double),
         ("fused_rr", c_i64),
         ("fused_rr_fallbacks", c_i64),
+        ("time_filter_steps_ms", C.c_double),
     ]
 
     def as_dict(self) -> dict:

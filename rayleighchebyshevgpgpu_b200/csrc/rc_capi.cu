@@ -111,11 +111,10 @@ rc_status rc_ctx_create(int device, rc_ctx** out) {
         if (!std::strcmp(v, "loop")) c->csr_variant = 1;
         else if (!std::strcmp(v, "reg")) c->csr_variant = 2;
     }
-    if (const char* v = std::getenv("RCB200_RM_MAP")) {
-        if (!std::strcmp(v, "persist")) c->rm_map = 1;
-    }
     c->pf_rows = 4096;
     if (const char* v = std::getenv("RCB200_PF_ROWS")) c->pf_rows = std::max<int64_t>(0, std::atoll(v));
+    if (const char* v = std::getenv("RCB200_RM_SLICES")) c->rm_slices = std::atoi(v) == 1 ? 1 : 2;
+    if (const char* v = std::getenv("RCB200_RM_GROUPS")) c->rm_groups = std::max(1, std::min(64, std::atoi(v)));
     *out = c;
     return RC_OK;
 }
@@ -129,6 +128,7 @@ rc_status rc_ctx_destroy(rc_ctx* ctx) {
     for (auto& b : ctx->slots)
         if (b.ptr) cudaFree(b.ptr);
     if (ctx->host_small) cudaFreeHost(ctx->host_small);
+    for (cudaEvent_t e : ctx->step_events) cudaEventDestroy(e);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return RC_OK;

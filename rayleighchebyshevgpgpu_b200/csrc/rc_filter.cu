@@ -303,6 +303,27 @@ static rc_status launch_step_c(rc_ctx* ctx, rc_op* op, const StepArgs& a) {
     }
 }
 
+void step_mark(rc_ctx* ctx) {
+    if (!ctx->step_timing) return;
+    if (ctx->step_events_used == ctx->step_events.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return;
+        ctx->step_events.push_back(e);
+    }
+    cudaEventRecord(ctx->step_events[ctx->step_events_used++], ctx->stream);
+}
+
+void step_flush(rc_ctx* ctx) {
+    // events come in (begin, end) pairs, one pair per degree-step loop
+    for (size_t i = 0; i + 1 < ctx->step_events_used; i += 2) {
+        float ms = 0.f;
+        cudaEventSynchronize(ctx->step_events[i + 1]);
+        if (cudaEventElapsedTime(&ms, ctx->step_events[i], ctx->step_events[i + 1]) == cudaSuccess)
+            ctx->step_ms += ms;
+    }
+    ctx->step_events_used = 0;
+}
+
 // Build the FP32 copy of the operator's values on first use.
 __global__ void cvt_f64_f32_kernel(const double* __restrict__ a, float* __restrict__ b, int64_t count) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)

@@ -47,103 +47,101 @@ __device__ __forceinline__ void st16(TS* p, const Pack16<TS>& v) {
 }
 
 constexpr int kRmThreads = 256;
+// Resident CTAs per SM the register budget must allow: 8 (32 registers) for FP32 storage, 6 for
+// FP64 (the FP64 steps spill at 32).
+template <class TS>
+constexpr int rm_min_blocks() {
+    return sizeof(real_t<TS>) == 4 ? 8 : 6;
+}
 
-// Middle step. Persistent grid (one wave): CTA b owns the contiguous rows
-// [b*chunk, (b+1)*chunk) and walks them in order, rows_per_iter rows at a time; thread
-// (r, seg) of an iteration owns the 16-byte slice seg of row r (V = 16/sizeof(TS) columns).
-// Walking rows in order keeps the nearby neighbour rows (+-1, +-nx) in this SM's L1; the far
-// ones (+-nx*ny) are fetched at about the same moment by a CTA a few chunks away (L2 hit).
+// Middle step. Row groups of rows_per_iter consecutive rows; CTA b takes the `groups`
+// consecutive groups starting at group b*groups and walks them in order. CTAs are dispatched
+// in index order, so the rows in flight at any moment form one contiguous band that moves down
+// the block, and a row's far neighbours (i +- band) were read by the band shortly before (an L2
+// hit). Thread (r, seg) of a group owns row r's W 16-byte slices seg, seg + nseg, ...,
+// seg + (W-1)*nseg (V = 16/sizeof(TS) columns each), so one warp-wide load covers contiguous
+// 16-byte slices and the row's index data serve W*V columns. Within a CTA the index data of
+// a row are fetched ahead (Pol::fetch1 two groups early, Pol::fetch2 one group early), so
+// only the gathers wait on memory.
+// IX is the element-offset type: uint32_t when every offset of the block fits, else int64_t.
 // pf_z > 0: each 128-byte line of row i + pf_z of x_{k-2} and of row i + pf_x of x_{k-1} (the
 // rows first touched from DRAM that many rows later) is prefetched into L2.
+// z == nullptr (the first step, gamma = 0): x_{k-2} is not read.
 __device__ __forceinline__ void prefetch_l2(const void* p) {
     asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
-template <class Pol, class TS, class TC>
-__global__ void __launch_bounds__(kRmThreads)
-rm_step_kernel(Pol op, int64_t n, int nseg, int64_t ld, int64_t chunk, const TS* __restrict__ x, const TS* z, TS* y,
+template <class Pol, class TS, class TC, int W, class IX>
+__global__ void __launch_bounds__(kRmThreads, rm_min_blocks<TS>())
+rm_step_kernel(Pol op, int64_t n, int nseg, int64_t ld, int groups, const TS* __restrict__ x, const TS* z, TS* y,
                TC alpha, TC beta, TC gamma, int64_t pf_z, int64_t pf_x) {
     constexpr int V = Pack16<TS>::V;
     const int rows_per_iter = blockDim.x / nseg;
     const int rloc = threadIdx.x / nseg;
     if (rloc >= rows_per_iter) return;
-    const int64_t off = (int64_t)(threadIdx.x - rloc * nseg) * V;
-    const bool line_head = ((off * (int64_t)sizeof(TS)) & 127) == 0;
-    const int64_t r_begin = (int64_t)blockIdx.x * chunk;
-    const int64_t r_end = min(n, r_begin + chunk);
-    for (int64_t i = r_begin + rloc; i < r_end; i += rows_per_iter) {
-        if (pf_z > 0 && line_head) {
-            if (i + pf_z < n) prefetch_l2(z + (i + pf_z) * ld + off);
-            if (i + pf_x < n) prefetch_l2(x + (i + pf_x) * ld + off);
-        }
-        TC acc[V];
-#pragma unroll
-        for (int v = 0; v < V; ++v) acc[v] = s_zero(TC());
-        op.row(i, [&](int64_t j, TC a) {
-            const Pack16<TS> p = ld16_ro(x + j * ld + off);
-#pragma unroll
-            for (int v = 0; v < V; ++v) acc[v] = s_fma(a, s_cvt<TC>(p.v[v]), acc[v]);
-        });
-        const Pack16<TS> xi = ld16_ro(x + i * ld + off);
-        const Pack16<TS> zi = ld16(z + i * ld + off);
-        Pack16<TS> out;
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-            TC r = s_mul(alpha, acc[v]);
-            r = s_fma(beta, s_cvt<TC>(xi.v[v]), r);
-            r = s_fma(gamma, s_cvt<TC>(zi.v[v]), r);
-            out.v[v] = s_cvt<TS>(r);
-        }
-        st16(y + i * ld + off, out);
+    const IX off = (IX)(threadIdx.x - rloc * nseg) * (IX)V;
+    const IX wstride = (IX)nseg * (IX)V;
+    const IX ldx = (IX)ld;
+    const int64_t stride = rows_per_iter;
+    int64_t i = (int64_t)blockIdx.x * groups * rows_per_iter + rloc;
+    const int64_t i_end = min(n, (int64_t)(blockIdx.x + 1) * groups * rows_per_iter);
+    typename Pol::Pre p0, p1;
+    if (i < i_end) {
+        op.fetch1(i, p0);
+        op.fetch2(i, p0);
     }
-}
-
-// Middle step with the row's N entries gathered up front (padding (i, 0)); the 16-byte slices
-// of up to 9 neighbour rows are then loaded back to back before any arithmetic, so every
-// thread keeps several independent loads in flight.
-template <class Pol, class TS, class TC, int N>
-__global__ void __launch_bounds__(kRmThreads)
-rm_step_batched_kernel(Pol op, int64_t n, int nseg, int64_t ld, int64_t chunk, const TS* __restrict__ x,
-                       const TS* z, TS* y, TC alpha, TC beta, TC gamma) {
-    constexpr int V = Pack16<TS>::V;
-    constexpr int G = N <= 9 ? N : 9;
-    const int rows_per_iter = blockDim.x / nseg;
-    const int rloc = threadIdx.x / nseg;
-    if (rloc >= rows_per_iter) return;
-    const int64_t off = (int64_t)(threadIdx.x - rloc * nseg) * V;
-    const int64_t r_begin = (int64_t)blockIdx.x * chunk;
-    const int64_t r_end = min(n, r_begin + chunk);
-    for (int64_t i = r_begin + rloc; i < r_end; i += rows_per_iter) {
-        int64_t js[N];
-        TC as[N];
-        op.template gather<N>(i, js, as);
-        const Pack16<TS> zi = ld16(z + i * ld + off);
-        const Pack16<TS> xi = ld16_ro(x + i * ld + off);
-        TC acc[V];
+    if (i + stride < i_end) op.fetch1(i + stride, p1);
+    for (; i < i_end; i += stride) {
+        typename Pol::Pre p2;
+        if (i + stride < i_end) op.fetch2(i + stride, p1);
+        if (i + 2 * stride < i_end) op.fetch1(i + 2 * stride, p2);
+        const IX oi = (IX)i * ldx + off;
+        if (pf_z > 0) {
 #pragma unroll
-        for (int v = 0; v < V; ++v) acc[v] = s_zero(TC());
+            for (int w = 0; w < W; ++w) {
+                if ((((off + w * wstride) * (IX)sizeof(TS)) & 127) != 0) continue;  // one per 128-byte line
+                if (z && i + pf_z < n) prefetch_l2(z + (IX)(i + pf_z) * ldx + off + w * wstride);
+                if (i + pf_x < n) prefetch_l2(x + (IX)(i + pf_x) * ldx + off + w * wstride);
+            }
+        }
+        TC acc[W * V];
 #pragma unroll
-        for (int b0 = 0; b0 < N; b0 += G) {
-            Pack16<TS> p[G];
+        for (int v = 0; v < W * V; ++v) acc[v] = s_zero(TC());
+        op.row(i, p0, [&](int64_t j, TC a) {
+            const TS* xj = x + ((IX)j * ldx + off);
 #pragma unroll
-            for (int g = 0; g < G; ++g)
-                if (b0 + g < N) p[g] = ld16_ro(x + js[b0 + g] * ld + off);
+            for (int w = 0; w < W; ++w) {
+                const Pack16<TS> p = ld16_ro(xj + w * wstride);
 #pragma unroll
-            for (int g = 0; g < G; ++g)
-                if (b0 + g < N) {
+                for (int v = 0; v < V; ++v) acc[w * V + v] = s_fma(a, s_cvt<TC>(p.v[v]), acc[w * V + v]);
+            }
+        });
 #pragma unroll
-                    for (int v = 0; v < V; ++v) acc[v] = s_fma(as[b0 + g], s_cvt<TC>(p[g].v[v]), acc[v]);
+        for (int w = 0; w < W; ++w) {
+            const IX o = oi + w * wstride;
+            const Pack16<TS> xi = ld16_ro(x + o);
+            Pack16<TS> out;
+            if (z) {
+                const Pack16<TS> zi = ld16(z + o);
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    TC r = s_mul(alpha, acc[w * V + v]);
+                    r = s_fma(beta, s_cvt<TC>(xi.v[v]), r);
+                    r = s_fma(gamma, s_cvt<TC>(zi.v[v]), r);
+                    out.v[v] = s_cvt<TS>(r);
                 }
-        }
-        Pack16<TS> out;
+            } else {
 #pragma unroll
-        for (int v = 0; v < V; ++v) {
-            TC r = s_mul(alpha, acc[v]);
-            r = s_fma(beta, s_cvt<TC>(xi.v[v]), r);
-            r = s_fma(gamma, s_cvt<TC>(zi.v[v]), r);
-            out.v[v] = s_cvt<TS>(r);
+                for (int v = 0; v < V; ++v) {
+                    TC r = s_mul(alpha, acc[w * V + v]);
+                    r = s_fma(beta, s_cvt<TC>(xi.v[v]), r);
+                    out.v[v] = s_cvt<TS>(r);
+                }
+            }
+            st16(y + o, out);
         }
-        st16(y + i * ld + off, out);
+        p0 = p1;
+        p1 = p2;
     }
 }
 
@@ -193,11 +191,9 @@ to_cm_kernel(int64_t n, int64_t s, const TS* __restrict__ Rr, int64_t ld, TV* __
 // ---------------------------------------------------------------------------------------
 // Driver
 // ---------------------------------------------------------------------------------------
-// NB > 0: steps gather the row's NB entries up front (rm_step_batched_kernel);
-// NB == 0: steps walk the row entry by entry (rm_step_kernel, with L2 prefetch).
 //   A <- X (row-major copy of x0); x_k (k = 1..m) into B, A, B, ... (x_k over x_{k-2});
 //   X <- x_m / (m+1) (column-major).
-template <class Pol, class TS, class TC, int NB>
+template <class Pol, class TS, class TC, int W, class IX>
 static rc_status run_rm_filter(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, int64_t ldv, int64_t s,
                                int64_t degree, double a, double b, void* bufA, void* bufB, int64_t ld, int64_t band) {
     const int64_t pf_z = ctx->pf_rows;
@@ -205,24 +201,17 @@ static rc_status run_rm_filter(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, 
     using TY = typename std::conditional<IsComplex<TC>::value, double2, double>::type;
     constexpr int VEC = Pack16<TS>::V;
     const TC ta = s_from<TC>(a, 0.0), tb = s_from<TC>(b, 0.0), tm1 = s_from<TC>(-1.0, 0.0);
-    const int nseg = (int)(ld / VEC);
+    if (ld % (VEC * W) != 0) return rc_fail(ctx, RC_ERR_INVALID, "row-major filter: leading dimension not padded");
+    const int nseg = (int)(ld / (VEC * W));
     if (nseg > kRmThreads) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "row-major filter: block too wide");
     const int rows_per_iter = kRmThreads / nseg;
-    int64_t chunk;
-    if (ctx->rm_map == 1) {
-        // one wave of persistent CTAs, each owning a contiguous chunk of rows
-        int per_sm = 0;
-        RC_CU(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rm_step_kernel<Pol, TS, TC>, kRmThreads, 0));
-        if (per_sm < 1) per_sm = 1;
-        const int64_t nb0 = (int64_t)per_sm * ctx->sm_count;
-        chunk = (n + nb0 - 1) / nb0;
-        chunk = ((chunk + rows_per_iter - 1) / rows_per_iter) * rows_per_iter;
-    } else {
-        // grid order: CTA b owns rows_per_iter consecutive rows, so the rows in flight form one
-        // contiguous band and a row's far neighbours were read one band earlier (still in L2)
-        chunk = rows_per_iter;
-    }
-    const unsigned grid_seg = (unsigned)((n + chunk - 1) / chunk);
+    // consecutive row groups per CTA (measured on 128^3 7-point operators, 96 columns):
+    // CSR 4 (FP32) / 2 (FP64), stencil 8 (FP32) / 4 (FP64)
+    constexpr bool kCsr = Pol::kIsCsr;
+    constexpr bool kF32 = sizeof(real_t<TS>) == 4;
+    const int groups = ctx->rm_groups > 0 ? ctx->rm_groups : (kCsr ? (kF32 ? 4 : 2) : (kF32 ? 8 : 4));
+    const int64_t rows_per_cta = (int64_t)groups * rows_per_iter;
+    const unsigned grid_seg = (unsigned)((n + rows_per_cta - 1) / rows_per_cta);
     if ((s + 31) / 32 > 65535) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "row-major filter: too many columns");
     const dim3 tgrid((unsigned)((n + 31) / 32), (unsigned)((s + 31) / 32)), tblk(32, 8);
     TS* A = (TS*)bufA;
@@ -230,26 +219,39 @@ static rc_status run_rm_filter(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, 
     to_rm_kernel<TY, TS><<<tgrid, tblk, 0, ctx->stream>>>(n, s, (const TY*)V, ldv, A, ld);
     ctx->launches++;
     RC_CU(ctx, cudaGetLastError());
+    step_mark(ctx);
     for (int64_t k = 1; k <= degree; ++k) {
-        TS* xk1 = (k - 1) % 2 ? B : A;  // x_{k-1}
-        TS* y = k % 2 ? B : A;          // x_k overwrites x_{k-2}
-        // k = 1 has no x_{k-2}: z = x0 (finite data) with gamma = 0
-        const TS* z = k >= 2 ? y : A;
-        const TC g = k >= 2 ? tm1 : s_zero(TC());
-        if constexpr (NB > 0)
-            rm_step_batched_kernel<Pol, TS, TC, NB><<<grid_seg, kRmThreads, 0, ctx->stream>>>(
-                pol, n, nseg, ld, chunk, xk1, z, y, ta, tb, g);
-        else
-            rm_step_kernel<Pol, TS, TC><<<grid_seg, kRmThreads, 0, ctx->stream>>>(pol, n, nseg, ld, chunk, xk1, z, y,
-                                                                                   ta, tb, g, pf_z, pf_x);
+        const TS* xk1 = (k - 1) % 2 ? B : A;  // x_{k-1}
+        TS* y = k % 2 ? B : A;                // x_k overwrites x_{k-2}
+        // k = 1 has no x_{k-2} (gamma = 0): z is not read
+        const TS* z = k >= 2 ? y : nullptr;
+        rm_step_kernel<Pol, TS, TC, W, IX><<<grid_seg, kRmThreads, 0, ctx->stream>>>(
+            pol, n, nseg, ld, groups, xk1, z, y, ta, tb, k >= 2 ? tm1 : s_zero(TC()), pf_z, pf_x);
         ctx->launches++;
     }
     RC_CU(ctx, cudaGetLastError());
-    TS* xm = degree % 2 ? B : A;
+    step_mark(ctx);
+    const TS* xm = degree % 2 ? B : A;
     to_cm_kernel<TS, TY><<<tgrid, tblk, 0, ctx->stream>>>(n, s, xm, ld, (TY*)V, ldv, 1.0 / (double)(degree + 1));
     ctx->launches++;
     RC_CU(ctx, cudaGetLastError());
     return RC_OK;
+}
+
+// Offset type and slices per thread: 32-bit offsets when the block's last element offset fits;
+// two 16-byte slices per thread for CSR with FP64 storage and one otherwise (the faster choice
+// on 128^3 7-point operators with 96 columns), unless the context sets the count
+// (RCB200_RM_SLICES=1 or 2).
+template <class Pol, class TS, class TC>
+static rc_status run_rm_select(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, int64_t ldv, int64_t s,
+                               int64_t degree, double a, double b, void* bufA, void* bufB, int64_t ld, int64_t band) {
+    const bool small = (n + 1) * ld < ((int64_t)1 << 32);
+    const int slices = ctx->rm_slices ? ctx->rm_slices : (Pol::kIsCsr && sizeof(real_t<TS>) == 8 ? 2 : 1);
+    if (slices == 1)
+        return small ? run_rm_filter<Pol, TS, TC, 1, uint32_t>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band)
+                     : run_rm_filter<Pol, TS, TC, 1, int64_t>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band);
+    return small ? run_rm_filter<Pol, TS, TC, 2, uint32_t>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band)
+                 : run_rm_filter<Pol, TS, TC, 2, int64_t>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band);
 }
 
 template <class TS, class TC>
@@ -259,42 +261,32 @@ static rc_status rm_filter_dispatch(rc_ctx* ctx, rc_op* op, void* V, int64_t ldv
     const int64_t band = op->kind == 0 ? op->band : (op->skind == 5 ? op->nx : op->nx * op->ny);
     if (op->kind == 0) {
         CsrRows<TS, TC> pol{op->rowptr, op->colind, (const TS*)(sizeof(real_t<TS>) == 8 ? op->vals64 : op->vals32)};
-        using P = CsrRows<TS, TC>;
-        if (ctx->csr_variant == 2 && op->max_row_nnz <= 8)
-            return run_rm_filter<P, TS, TC, 8>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band);
-        if (ctx->csr_variant == 2 && op->max_row_nnz <= 32)
-            return run_rm_filter<P, TS, TC, 32>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band);
-        return run_rm_filter<P, TS, TC, 0>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band);
+        return run_rm_select<CsrRows<TS, TC>, TS, TC>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band);
     }
     using TD = real_t<TS>;
     const TD* dg = (const TD*)(sizeof(TD) == 8 ? (const void*)op->diag64 : (const void*)op->diag32);
     const double theta = 2.0 * 3.14159265358979323846 * op->flux;
     if (op->skind == 27) {
-        StencilRows<TD, TC, 27> pol{op->nx, op->ny, op->nz, dg, op->offdiag, theta};
-        return ctx->csr_variant != 2
-                   ? run_rm_filter<StencilRows<TD, TC, 27>, TS, TC, 0>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld,
-                                                                     band)
-                   : run_rm_filter<StencilRows<TD, TC, 27>, TS, TC, 27>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB,
-                                                                      ld, band);
+        if constexpr (IsComplex<TC>::value) {
+            return rc_fail(ctx, RC_ERR_UNSUPPORTED, "27-point stencil is real only");
+        } else {
+            StencilRows<TD, TC, 27> pol{op->nx, op->ny, op->nz, dg, op->offdiag, theta};
+            return run_rm_select<StencilRows<TD, TC, 27>, TS, TC>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB,
+                                                                  ld, band);
+        }
     }
     if (op->skind == 7) {
         StencilRows<TD, TC, 7> pol{op->nx, op->ny, op->nz, dg, op->offdiag, theta};
-        return ctx->csr_variant != 2
-                   ? run_rm_filter<StencilRows<TD, TC, 7>, TS, TC, 0>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld,
-                                                                     band)
-                   : run_rm_filter<StencilRows<TD, TC, 7>, TS, TC, 7>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB,
-                                                                      ld, band);
+        return run_rm_select<StencilRows<TD, TC, 7>, TS, TC>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld,
+                                                             band);
     }
     StencilRows<TD, TC, 5> pol{op->nx, op->ny, op->nz, dg, op->offdiag, theta};
-    return ctx->csr_variant != 2
-                   ? run_rm_filter<StencilRows<TD, TC, 5>, TS, TC, 0>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld,
-                                                                     band)
-                   : run_rm_filter<StencilRows<TD, TC, 5>, TS, TC, 5>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB,
-                                                                      ld, band);
+    return run_rm_select<StencilRows<TD, TC, 5>, TS, TC>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band);
 }
 
+// Row length padded to 32 bytes (two 16-byte slices); the padding columns are never read back.
 int64_t rm_leading_dim(int dtype, int prec, int64_t s) {
-    const int64_t v = 16 / (int64_t)elem_bytes(dtype, prec);
+    const int64_t v = 32 / (int64_t)elem_bytes(dtype, prec);
     return ((s + v - 1) / v) * v;
 }
 

@@ -33,11 +33,20 @@ struct rc_ctx {
     // CSR step kernel: 0 auto (register-cached rows when every row has <= 8 entries),
     // 1 row loop, 2 register-cached rows. Read from RCB200_CSR_KERNEL at context creation.
     int csr_variant = 0;
-    // row-major filter step mapping: 0 grid order (default), 1 persistent contiguous chunks.
-    // Read from RCB200_RM_MAP ("grid" / "persist") at context creation.
-    int rm_map = 0;
     // L2 prefetch distance (rows) of the row-major filter steps; 0 = off. RCB200_PF_ROWS.
     int64_t pf_rows = 0;
+    // 16-byte slices per thread in the row-major filter steps: 0 = by storage precision (two
+    // for FP32, one for FP64), else 1 or 2. RCB200_RM_SLICES.
+    int rm_slices = 0;
+    // consecutive row groups per CTA in the row-major filter steps: 0 = by operator kind and
+    // storage precision, else 1..64. RCB200_RM_GROUPS.
+    int rm_groups = 0;
+    // CUDA-event pairs around the degree-step loops of the row-major filter (no transposes),
+    // recorded while step_timing is set; step_flush() waits for them and adds to step_ms.
+    bool step_timing = false;
+    std::vector<cudaEvent_t> step_events;
+    size_t step_events_used = 0;
+    double step_ms = 0.0;
 };
 
 enum Slot {
@@ -115,6 +124,10 @@ rc_status filter_apply(rc_ctx* ctx, rc_op* op, void* V, int64_t ld, int64_t s, i
                        int64_t* steps_done);
 // Build the FP32 (c64) copy of an operator's values/diagonal used by the MIXED filter.
 rc_status ensure_fp32(rc_ctx* ctx, rc_op* op);
+// Degree-step timing (ctx->step_timing): record an event on the context stream; step_flush
+// waits for the recorded pairs and adds their elapsed time to ctx->step_ms.
+void step_mark(rc_ctx* ctx);
+void step_flush(rc_ctx* ctx);
 
 // ---- dense FP64 kernels (T = double or double2) ------------------------------------
 // C (m x nc, ld m) = X^H Y where X is n x m, Y is n x nc. upper: only i<=j computed then mirrored

@@ -7,29 +7,31 @@
 
 namespace rcb {
 
-// gather<N>(i, js, as): the row's entries as N (column, value) pairs padded with (i, 0), for
-// rows with at most N entries (the caller guarantees it). All loads are independent, so the
-// kernel can issue the N gathers of a row back to back.
+// Index data fetched ahead of use. A kernel that walks rows calls fetch1 for a row two
+// iterations before it is processed and fetch2 one iteration before, so loads that feed the
+// gather addresses are off the critical path:
+//   fetch1(i, p): loads that need only i (CSR: the row's extent from rowptr)
+//   fetch2(i, p): loads that need fetch1's result (none for the policies here)
+//   row(i, p, f): f(j, a_ij) for every entry (CSR: column indices and values loaded here, four
+//                 entries unrolled so their gathers overlap)
 template <class TA, class TC>
 struct CsrRows {
+    static constexpr bool kIsCsr = true;
     const int32_t* __restrict__ rowptr;
     const int32_t* __restrict__ colind;
     const TA* __restrict__ vals;
-    template <class F>
-    __device__ __forceinline__ void row(int64_t i, F&& f) const {
-        const int k0 = __ldg(rowptr + i), k1 = __ldg(rowptr + i + 1);
-#pragma unroll 4
-        for (int k = k0; k < k1; ++k) f((int64_t)__ldg(colind + k), s_cvt<TC>(vals[k]));
+    struct Pre {
+        int k0, k1;
+    };
+    __device__ __forceinline__ void fetch1(int64_t i, Pre& p) const {
+        p.k0 = __ldg(rowptr + i);
+        p.k1 = __ldg(rowptr + i + 1);
     }
-    template <int N>
-    __device__ __forceinline__ void gather(int64_t i, int64_t (&js)[N], TC (&as)[N]) const {
-        const int k0 = __ldg(rowptr + i), cnt = __ldg(rowptr + i + 1) - k0;
-#pragma unroll
-        for (int r = 0; r < N; ++r) {
-            const bool ok = r < cnt;
-            js[r] = ok ? (int64_t)__ldg(colind + k0 + r) : i;
-            as[r] = ok ? s_cvt<TC>(vals[k0 + r]) : s_zero(TC());
-        }
+    __device__ __forceinline__ void fetch2(int64_t, Pre&) const {}
+    template <class F>
+    __device__ __forceinline__ void row(int64_t, const Pre& p, F&& f) const {
+#pragma unroll 4
+        for (int k = p.k0; k < p.k1; ++k) f((int64_t)__ldg(colind + k), s_cvt<TC>(__ldg(vals + k)));
     }
 };
 
@@ -52,6 +54,7 @@ template <> __device__ __forceinline__ float2 unit_phase<float2>(double t, bool 
 // (x,y)<-(x,y+1). KIND 5 (2D), 7 (3D), 27 (3D, real).
 template <class TD, class TC, int KIND>
 struct StencilRows {
+    static constexpr bool kIsCsr = false;
     int64_t nx, ny, nz;
     const TD* __restrict__ diag;
     double offd;
@@ -97,53 +100,12 @@ struct StencilRows {
             if (KIND == 7 && iz + 1 < nz) f(i + sz, w);
         }
     }
-    // All entries of row i as N = KIND pairs (diagonal first), invalid neighbours as (i, 0).
-    template <int N>
-    __device__ __forceinline__ void gather(int64_t i, int64_t (&js)[N], TC (&as)[N]) const {
-        static_assert(N == KIND, "stencil gather width must equal its point count");
-        const int64_t ix = i % nx;
-        const int64_t t = i / nx;
-        const int64_t iy = t % ny;
-        const int64_t iz = t / ny;
-        const int64_t sy = nx, sz = nx * ny;
-        const TC w = s_from<TC>(offd, 0.0);
-        const TC zero = s_zero(TC());
-        js[0] = i;
-        as[0] = s_from<TC>((double)diag[i], 0.0);
-        if (KIND == 27) {
-            int r = 1;
-#pragma unroll
-            for (int dz = -1; dz <= 1; ++dz) {
-                const bool vz = dz < 0 ? iz > 0 : (dz > 0 ? iz + 1 < nz : true);
-#pragma unroll
-                for (int dy = -1; dy <= 1; ++dy) {
-                    const bool vy = dy < 0 ? iy > 0 : (dy > 0 ? iy + 1 < ny : true);
-#pragma unroll
-                    for (int dx = -1; dx <= 1; ++dx) {
-                        if (dx == 0 && dy == 0 && dz == 0) continue;
-                        const bool vx = dx < 0 ? ix > 0 : (dx > 0 ? ix + 1 < nx : true);
-                        const bool ok = vx && vy && vz;
-                        js[r] = ok ? i + dx + dy * sy + dz * sz : i;
-                        as[r] = ok ? w : zero;
-                        ++r;
-                    }
-                }
-            }
-        } else {
-            TC wym = w, wyp = w;
-            if (IsComplex<TC>::value) {
-                wym = s_mul(w, unit_phase<TC>(theta * (double)ix, false));
-                wyp = s_mul(w, unit_phase<TC>(theta * (double)ix, true));
-            }
-            js[1] = ix > 0 ? i - 1 : i;            as[1] = ix > 0 ? w : zero;
-            js[2] = ix + 1 < nx ? i + 1 : i;       as[2] = ix + 1 < nx ? w : zero;
-            js[3] = iy > 0 ? i - sy : i;           as[3] = iy > 0 ? wym : zero;
-            js[4] = iy + 1 < ny ? i + sy : i;      as[4] = iy + 1 < ny ? wyp : zero;
-            if (KIND == 7) {
-                js[5 % N] = iz > 0 ? i - sz : i;           as[5 % N] = iz > 0 ? w : zero;
-                js[6 % N] = iz + 1 < nz ? i + sz : i;      as[6 % N] = iz + 1 < nz ? w : zero;
-            }
-        }
+    struct Pre {};
+    __device__ __forceinline__ void fetch1(int64_t, Pre&) const {}
+    __device__ __forceinline__ void fetch2(int64_t, Pre&) const {}
+    template <class F>
+    __device__ __forceinline__ void row(int64_t i, const Pre&, F&& f) const {
+        row(i, f);
     }
 };
 

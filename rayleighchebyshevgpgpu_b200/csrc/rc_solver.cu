@@ -97,6 +97,7 @@ private:
     double minEst_ = 0.0, maxEst_ = 0.0;
 
     double t_[PH_N] = {0, 0, 0, 0, 0};
+    double step_ms0_ = 0.0;
     std::vector<cudaEvent_t> pool_;
     size_t pool_used_ = 0;
     struct Pending { int ph; cudaEvent_t a, b; };
@@ -129,6 +130,7 @@ void Solver::toc(int ph) {
 }
 void Solver::flush() {
     if (!P_.phase_timing) return;
+    step_flush(ctx_);
     for (auto& p : pending_) {
         float ms = 0.f;
         cudaEventSynchronize(p.b);
@@ -689,6 +691,17 @@ rc_status Solver::run(const void* v0, double* evals_out, void* evecs_out, double
         cudaEventRecord(t0, ctx_->stream);
     }
     const int64_t launches0 = ctx_->launches;
+    // degree-step timing for this solve only, switched off on every return path
+    struct StepTimingScope {
+        rc_ctx* c;
+        ~StepTimingScope() {
+            c->step_timing = false;
+            c->step_events_used = 0;
+        }
+    } step_scope{ctx_};
+    ctx_->step_timing = P_.phase_timing != 0;
+    ctx_->step_events_used = 0;
+    step_ms0_ = ctx_->step_ms;
     const double maxMinTol = P_.max_min_tol > 0 ? P_.max_min_tol : 1.0e-6;
     rc_status st = RC_OK;
     int64_t maxDim = P_.eig_count;
@@ -779,6 +792,7 @@ rc_status Solver::run(const void* v0, double* evals_out, void* evecs_out, double
         r.guard_value = guardValue_;
         r.fused_rr = fused_ok_ + fused_fallback_;
         r.fused_rr_fallbacks = fused_fallback_;
+        r.time_filter_steps_ms = ctx_->step_ms - step_ms0_;
         std::memcpy(info, &r, std::min(sz, sizeof(r)));
     }
     return RC_OK;
