@@ -265,6 +265,83 @@ void rc_solve_params_default(rc_solve_params* p);
 rc_status rc_solve(rc_ctx* ctx, const rc_op* op, const rc_solve_params* params, const void* v0,
                    double* evals_out, void* evecs_out, double* residuals_out, rc_solve_info* info);
 
+/* ------------------------------------------------------------------------------------
+ * Request server (no reference counterpart; the reference solves one problem per call,
+ * RayleighChebyshevLMCuda::getMinEigenSystem, RayleighChebyshevLMCuda.h:794).
+ *
+ * A server owns one GPU's worth of solve slots. Each admitted request runs the same solver as
+ * rc_solve, with its subspace, spectral bounds and Ritz state resident in that slot until it
+ * finishes. Requests are admitted first-fit while a slot is free and the request's device
+ * footprint fits the HBM budget (working blocks n*(4*(incr+buffer) + eig_count) scalars, the
+ * small Rayleigh-Ritz buffers, and the operator's storage, charged once per operator in use).
+ * Filter applications of the running solves that are ready at the same time are packed into
+ * one batched launch per degree step (replayed from a captured CUDA graph), so the filter
+ * sweeps of concurrent solves overlap on the device; each solve's arithmetic is the same as
+ * when it runs alone or through rc_solve.
+ * ------------------------------------------------------------------------------------ */
+typedef struct rc_server rc_server;
+
+typedef struct rc_server_params {
+    size_t struct_size;            /* sizeof(rc_server_params) */
+    int device;
+    int64_t hbm_budget_bytes;      /* 0: 90 % of the device memory free at creation */
+    int max_active;                /* solves resident at once, 1..64 (default 16) */
+    double batch_window_us;        /* longest wait for more solves to join a filter batch (default 200) */
+    int use_graphs;                /* 1 (default): batches replay captured CUDA graphs; 0: direct launches */
+    double starvation_ms;          /* admission passes over a queued request for at most this long,
+                                      then holds back later ones until it fits (default 2000) */
+} rc_server_params;
+
+enum { RC_REQ_QUEUED = 0, RC_REQ_RUNNING = 1, RC_REQ_DONE = 2, RC_REQ_FAILED = 3, RC_REQ_CANCELLED = 4 };
+
+typedef struct rc_request_info {
+    size_t struct_size;
+    int state;                     /* RC_REQ_* */
+    rc_status status;              /* the solve's status once finished */
+    double queue_ms;               /* submit -> admitted to a slot */
+    double run_ms;                 /* admitted -> finished */
+    double latency_ms;             /* submit -> finished */
+    int64_t batches;               /* batched filter launches the request joined */
+    int64_t reserved_bytes;        /* device bytes charged to the budget (operator excluded) */
+    int64_t device_bytes;          /* scratch the solve actually held at its peak */
+} rc_request_info;
+
+typedef struct rc_server_stats {
+    size_t struct_size;
+    int64_t submitted, completed, failed, cancelled, queued, running;
+    int64_t batches;               /* batched filter launches */
+    int64_t batched_jobs;          /* filter applications in them */
+    int64_t max_jobs_in_batch;
+    int64_t graph_launches, graphs_built;
+    int64_t kernel_launches;       /* kernels of the batched filter */
+    int64_t bytes_in_use, bytes_peak, budget;
+} rc_server_stats;
+
+void rc_server_params_default(rc_server_params* p);
+rc_status rc_server_create(const rc_server_params* params, rc_server** out);
+/* Cancels queued and running requests, waits for the running ones to stop, frees everything. */
+rc_status rc_server_destroy(rc_server* server);
+const char* rc_server_last_error(const rc_server* server);
+/* Queue a solve of op (created on a context of the server's device; it must outlive the
+ * request) with rc_solve's parameters and arguments. The output buffers are written when the
+ * request finishes and must stay valid until then. RC_ERR_NOMEM when the request alone
+ * exceeds the budget. */
+rc_status rc_serve_submit(rc_server* server, const rc_op* op, const rc_solve_params* params, const void* v0,
+                          double* evals_out, void* evecs_out, double* residuals_out, int64_t* request_id);
+rc_status rc_serve_poll(rc_server* server, int64_t request_id, int* state);
+/* Wait up to timeout_ms (< 0: no limit) for the request to finish; RC_ERR_NOT_READY on timeout. */
+rc_status rc_serve_wait(rc_server* server, int64_t request_id, double timeout_ms, int* state);
+/* The finished request's solve info, timings and error text (errbuf may be NULL). Returns the
+ * request's own status, or RC_ERR_NOT_READY while it is queued or running. */
+rc_status rc_serve_result(rc_server* server, int64_t request_id, rc_solve_info* info, rc_request_info* rinfo,
+                          char* errbuf, size_t errbuf_len);
+/* A queued request is dropped at once; a running one stops at its next inner iteration
+ * (status RC_ERR_CANCELLED). */
+rc_status rc_serve_cancel(rc_server* server, int64_t request_id);
+/* Forget a finished request (its id becomes invalid). */
+rc_status rc_serve_release(rc_server* server, int64_t request_id);
+rc_status rc_server_stats_get(rc_server* server, rc_server_stats* out);
+
 #ifdef __cplusplus
 }
 #endif

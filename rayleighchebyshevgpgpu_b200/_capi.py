@@ -97,6 +97,49 @@ class SolveInfo(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "struct_size"}
 
 
+class ServerParams(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_size_t),
+        ("device", C.c_int),
+        ("hbm_budget_bytes", c_i64),
+        ("max_active", C.c_int),
+        ("batch_window_us", C.c_double),
+        ("use_graphs", C.c_int),
+        ("starvation_ms", C.c_double),
+    ]
+
+
+RC_REQ_QUEUED, RC_REQ_RUNNING, RC_REQ_DONE, RC_REQ_FAILED, RC_REQ_CANCELLED = 0, 1, 2, 3, 4
+REQ_STATE_NAMES = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_size_t),
+        ("state", C.c_int),
+        ("status", C.c_int),
+        ("queue_ms", C.c_double),
+        ("run_ms", C.c_double),
+        ("latency_ms", C.c_double),
+        ("batches", c_i64),
+        ("reserved_bytes", c_i64),
+        ("device_bytes", c_i64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "struct_size"}
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("struct_size", C.c_size_t)] + [(name, c_i64) for name in (
+        "submitted", "completed", "failed", "cancelled", "queued", "running", "batches", "batched_jobs",
+        "max_jobs_in_batch", "graph_launches", "graphs_built", "kernel_launches", "bytes_in_use", "bytes_peak",
+        "budget")]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "struct_size"}
+
+
 # Every symbol the header declares, with (restype, argtypes).
 SIGNATURES = {
     "rc_abi_version": (C.c_int, []),
@@ -127,6 +170,18 @@ SIGNATURES = {
     "rc_small_eigh_noalloc": (C.c_int, [c_vp, C.c_int, c_i64, c_vp, c_dp, c_vp]),
     "rc_solve_params_default": (None, [C.POINTER(SolveParams)]),
     "rc_solve": (C.c_int, [c_vp, c_vp, C.POINTER(SolveParams), c_vp, c_dp, c_vp, c_dp, C.POINTER(SolveInfo)]),
+    "rc_server_params_default": (None, [C.POINTER(ServerParams)]),
+    "rc_server_create": (C.c_int, [C.POINTER(ServerParams), C.POINTER(c_vp)]),
+    "rc_server_destroy": (C.c_int, [c_vp]),
+    "rc_server_last_error": (C.c_char_p, [c_vp]),
+    "rc_serve_submit": (C.c_int, [c_vp, c_vp, C.POINTER(SolveParams), c_vp, c_dp, c_vp, c_dp, C.POINTER(c_i64)]),
+    "rc_serve_poll": (C.c_int, [c_vp, c_i64, C.POINTER(C.c_int)]),
+    "rc_serve_wait": (C.c_int, [c_vp, c_i64, C.c_double, C.POINTER(C.c_int)]),
+    "rc_serve_result": (C.c_int, [c_vp, c_i64, C.POINTER(SolveInfo), C.POINTER(RequestInfo), C.c_char_p,
+                                  C.c_size_t]),
+    "rc_serve_cancel": (C.c_int, [c_vp, c_i64]),
+    "rc_serve_release": (C.c_int, [c_vp, c_i64]),
+    "rc_server_stats_get": (C.c_int, [c_vp, C.POINTER(ServerStats)]),
 }
 
 _lib = None

@@ -21,7 +21,8 @@ NVCC_FLAGS = ARCH_FLAGS + [
     "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
     "--expt-relaxed-constexpr", "-Xptxas", "-O3",
 ]
-SOURCES = ["rc_filter.cu", "rc_filter_rm.cu", "rc_dense.cu", "rc_gemm.cu", "rc_noalloc.cu", "rc_lanczos.cu", "rc_solver.cu", "rc_capi.cu"]
+SOURCES = ["rc_filter.cu", "rc_filter_rm.cu", "rc_dense.cu", "rc_gemm.cu", "rc_noalloc.cu", "rc_lanczos.cu", "rc_solver.cu", "rc_capi.cu",
+           "rc_batch.cu", "rc_serve.cu"]
 
 
 def _nvcc() -> str:
@@ -67,7 +68,7 @@ def build(verbose: bool = False, force: bool = False, extra_flags: list[str] | N
     with cf.ThreadPoolExecutor(max_workers=min(8, max(1, len(jobs)))) as ex:
         list(ex.map(run, jobs))
     if jobs or not os.path.exists(LIB_PATH):
-        run([nvcc] + ARCH_FLAGS + ["-shared", "-o", LIB_PATH] + objs + ["-lcudart"])
+        run([nvcc] + ARCH_FLAGS + ["-shared", "-o", LIB_PATH] + objs + ["-lcudart", "-lpthread"])
     return LIB_PATH
 
 

@@ -27,14 +27,20 @@ rc_status rc_slot(rc_ctx* ctx, int slot, size_t bytes, void** out) {
     DevBuf& b = ctx->slots[slot];
     if (b.bytes < bytes) {
         if (b.ptr) {
-            cudaStreamSynchronize(ctx->stream);
-            cudaFree(b.ptr);
+            if (ctx->pool) {
+                cudaFreeAsync(b.ptr, ctx->stream);
+            } else {
+                cudaStreamSynchronize(ctx->stream);
+                cudaFree(b.ptr);
+            }
             b.ptr = nullptr;
             b.bytes = 0;
         }
         // round up to 2 MiB so repeated small growth does not thrash the allocator
         const size_t want = ((bytes + (2u << 20) - 1) / (2u << 20)) * (2u << 20);
-        if (cudaMalloc(&b.ptr, want) != cudaSuccess) {
+        const cudaError_t e = ctx->pool ? cudaMallocFromPoolAsync(&b.ptr, want, ctx->pool, ctx->stream)
+                                        : cudaMalloc(&b.ptr, want);
+        if (e != cudaSuccess) {
             cudaGetLastError();
             b.ptr = nullptr;
             return rc_fail(ctx, RC_ERR_NOMEM, "cudaMalloc of " + std::to_string(want) + " bytes failed");
@@ -43,6 +49,21 @@ rc_status rc_slot(rc_ctx* ctx, int slot, size_t bytes, void** out) {
     }
     *out = b.ptr;
     return RC_OK;
+}
+
+void rc_release_slots(rc_ctx* ctx) {
+    for (auto& b : ctx->slots) {
+        if (b.ptr) {
+            if (ctx->pool) {
+                cudaFreeAsync(b.ptr, ctx->stream);
+            } else {
+                cudaStreamSynchronize(ctx->stream);
+                cudaFree(b.ptr);
+            }
+        }
+        b.ptr = nullptr;
+        b.bytes = 0;
+    }
 }
 
 rc_status rc_host_small(rc_ctx* ctx, size_t bytes, double** out) {
@@ -125,8 +146,8 @@ rc_status rc_ctx_destroy(rc_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     for (rc_op* op : ctx->ops) op_release(op);
     ctx->ops.clear();
-    for (auto& b : ctx->slots)
-        if (b.ptr) cudaFree(b.ptr);
+    rc_release_slots(ctx);
+    cudaStreamSynchronize(ctx->stream);
     if (ctx->host_small) cudaFreeHost(ctx->host_small);
     for (cudaEvent_t e : ctx->step_events) cudaEventDestroy(e);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);

@@ -430,7 +430,11 @@ rc_status filter_apply(rc_ctx* ctx, rc_op* op, void* V, int64_t ld, int64_t s, i
         if (!bufA || tmp_bytes < need) RC_TRY(rc_slot(ctx, S_FA, need, &bufA));
         if (!bufB || tmp_bytes < need) RC_TRY(rc_slot(ctx, S_FB, need, &bufB));
         if (p == P32) RC_TRY(ensure_fp32(ctx, op));
-        for (int64_t r = 0; r < rep; ++r) RC_TRY(rm_filter(ctx, op, V, ld, s, degree, a, b, prec, bufA, bufB));
+        for (int64_t r = 0; r < rep; ++r) {
+            bool handled = false;
+            if (ctx->serve) RC_TRY(serve_filter(ctx, op, V, ld, s, degree, a, b, prec, bufA, bufB, need, &handled));
+            if (!handled) RC_TRY(rm_filter(ctx, op, V, ld, s, degree, a, b, prec, bufA, bufB));
+        }
         if (steps_done) *steps_done += degree * rep;
         return RC_OK;
     }

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <atomic>
 #include <string>
 #include <vector>
 #include "../../include/rc_b200.h"
@@ -47,6 +48,12 @@ struct rc_ctx {
     std::vector<cudaEvent_t> step_events;
     size_t step_events_used = 0;
     double step_ms = 0.0;
+    // Request-server hooks, null outside the server (rc_serve.cu): filter applications go to the
+    // server's batcher, the solver checks the cancel flag once per inner iteration, and scratch
+    // slots come from the server's stream-ordered memory pool and go back to it after a request.
+    struct ServeHook* serve = nullptr;
+    const std::atomic<int>* cancel = nullptr;
+    cudaMemPool_t pool = nullptr;
 };
 
 enum Slot {
@@ -96,6 +103,8 @@ rc_status rc_fail(rc_ctx* ctx, rc_status st, const std::string& msg);
 
 // Scratch slot of at least `bytes` (contents not preserved on growth).
 rc_status rc_slot(rc_ctx* ctx, int slot, size_t bytes, void** out);
+// Free every scratch slot (stream-ordered when the context has a memory pool).
+void rc_release_slots(rc_ctx* ctx);
 rc_status rc_host_small(rc_ctx* ctx, size_t bytes, double** out);
 inline size_t elem_bytes(int dtype, int prec) {
     return (dtype == RC_COMPLEX128 ? 2 : 1) * (prec == P64 ? 8 : 4);
@@ -122,6 +131,11 @@ rc_status op_step(rc_ctx* ctx, rc_op* op, const StepArgs& a);
 rc_status filter_apply(rc_ctx* ctx, rc_op* op, void* V, int64_t ld, int64_t s, int64_t degree,
                        int64_t rep, double a, double b, int prec, void* tmp1, void* tmp2, size_t tmp_bytes,
                        int64_t* steps_done);
+// Inside the request server: hand a row-major filter application to the server's batcher and
+// make ctx->stream wait for its batch. *handled = false when the application needs the
+// single-solve path (rc_serve.cu).
+rc_status serve_filter(rc_ctx* ctx, rc_op* op, void* V, int64_t ld, int64_t s, int64_t degree, double a, double b,
+                       int prec, void* bufA, void* bufB, size_t buf_bytes, bool* handled);
 // Build the FP32 (c64) copy of an operator's values/diagonal used by the MIXED filter.
 rc_status ensure_fp32(rc_ctx* ctx, rc_op* op);
 // Degree-step timing (ctx->step_timing): record an event on the context stream; step_flush

@@ -1,0 +1,182 @@
+// rc_rmstep.cuh -- the degree-step and layout-change arithmetic of the row-major filter.
+//
+// Device functions shared by the single-solve kernels (rc_filter_rm.cu) and the batched kernels
+// that serve several solves in one launch (rc_batch.cu), so both launch forms compute the same
+// values in the same order.
+#pragma once
+#include <cstring>
+#include "rc_common.cuh"
+#include "rc_rowops.cuh"
+
+namespace rcb {
+
+template <class TS>
+struct alignas(16) Pack16 {
+    static constexpr int V = 16 / sizeof(TS);
+    TS v[V];
+};
+
+template <class TS>
+__device__ __forceinline__ Pack16<TS> ld16_ro(const TS* p) {
+    const uint4 u = __ldg(reinterpret_cast<const uint4*>(p));
+    Pack16<TS> r;
+    memcpy(&r, &u, 16);
+    return r;
+}
+template <class TS>
+__device__ __forceinline__ Pack16<TS> ld16(const TS* p) {
+    const uint4 u = *reinterpret_cast<const uint4*>(p);
+    Pack16<TS> r;
+    memcpy(&r, &u, 16);
+    return r;
+}
+template <class TS>
+__device__ __forceinline__ void st16(TS* p, const Pack16<TS>& v) {
+    uint4 u;
+    memcpy(&u, &v, 16);
+    *reinterpret_cast<uint4*>(p) = u;
+}
+
+constexpr int kRmThreads = 256;
+// Resident CTAs per SM the register budget must allow: 8 (32 registers) for FP32 storage, 6 for
+// FP64 (the FP64 steps spill at 32).
+template <class TS>
+constexpr int rm_min_blocks() {
+    return sizeof(real_t<TS>) == 4 ? 8 : 6;
+}
+
+// Middle step. Row groups of rows_per_iter consecutive rows; CTA b takes the `groups`
+// consecutive groups starting at group b*groups and walks them in order. CTAs are dispatched
+// in index order, so the rows in flight at any moment form one contiguous band that moves down
+// the block, and a row's far neighbours (i +- band) were read by the band shortly before (an L2
+// hit). Thread (r, seg) of a group owns row r's W 16-byte slices seg, seg + nseg, ...,
+// seg + (W-1)*nseg (V = 16/sizeof(TS) columns each), so one warp-wide load covers contiguous
+// 16-byte slices and the row's index data serve W*V columns. Within a CTA the index data of
+// a row are fetched ahead (Pol::fetch1 two groups early, Pol::fetch2 one group early), so
+// only the gathers wait on memory.
+// IX is the element-offset type: uint32_t when every offset of the block fits, else int64_t.
+// pf_z > 0: each 128-byte line of row i + pf_z of x_{k-2} and of row i + pf_x of x_{k-1} (the
+// rows first touched from DRAM that many rows later) is prefetched into L2.
+// z == nullptr (the first step, gamma = 0): x_{k-2} is not read.
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+// The rows of virtual CTA `cta` (the kernel below passes blockIdx.x; the batched kernel of
+// rc_batch.cu passes its own CTA numbering), so one arithmetic serves both launch forms.
+template <class Pol, class TS, class TC, int W, class IX>
+__device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg, int64_t ld, int groups, int64_t cta,
+                                             const TS* __restrict__ x, const TS* z, TS* y, TC alpha, TC beta,
+                                             TC gamma, int64_t pf_z, int64_t pf_x) {
+    constexpr int V = Pack16<TS>::V;
+    const int rows_per_iter = blockDim.x / nseg;
+    const int rloc = threadIdx.x / nseg;
+    if (rloc >= rows_per_iter) return;
+    const IX off = (IX)(threadIdx.x - rloc * nseg) * (IX)V;
+    const IX wstride = (IX)nseg * (IX)V;
+    const IX ldx = (IX)ld;
+    const int64_t stride = rows_per_iter;
+    int64_t i = cta * groups * rows_per_iter + rloc;
+    const int64_t i_end = min(n, (cta + 1) * groups * rows_per_iter);
+    typename Pol::Pre p0, p1;
+    if (i < i_end) {
+        op.fetch1(i, p0);
+        op.fetch2(i, p0);
+    }
+    if (i + stride < i_end) op.fetch1(i + stride, p1);
+    for (; i < i_end; i += stride) {
+        typename Pol::Pre p2;
+        if (i + stride < i_end) op.fetch2(i + stride, p1);
+        if (i + 2 * stride < i_end) op.fetch1(i + 2 * stride, p2);
+        const IX oi = (IX)i * ldx + off;
+        if (pf_z > 0) {
+#pragma unroll
+            for (int w = 0; w < W; ++w) {
+                if ((((off + w * wstride) * (IX)sizeof(TS)) & 127) != 0) continue;  // one per 128-byte line
+                if (z && i + pf_z < n) prefetch_l2(z + (IX)(i + pf_z) * ldx + off + w * wstride);
+                if (i + pf_x < n) prefetch_l2(x + (IX)(i + pf_x) * ldx + off + w * wstride);
+            }
+        }
+        TC acc[W * V];
+#pragma unroll
+        for (int v = 0; v < W * V; ++v) acc[v] = s_zero(TC());
+        op.row(i, p0, [&](int64_t j, TC a) {
+            const TS* xj = x + ((IX)j * ldx + off);
+#pragma unroll
+            for (int w = 0; w < W; ++w) {
+                const Pack16<TS> p = ld16_ro(xj + w * wstride);
+#pragma unroll
+                for (int v = 0; v < V; ++v) acc[w * V + v] = s_fma(a, s_cvt<TC>(p.v[v]), acc[w * V + v]);
+            }
+        });
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            const IX o = oi + w * wstride;
+            const Pack16<TS> xi = ld16_ro(x + o);
+            Pack16<TS> out;
+            if (z) {
+                const Pack16<TS> zi = ld16(z + o);
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    TC r = s_mul(alpha, acc[w * V + v]);
+                    r = s_fma(beta, s_cvt<TC>(xi.v[v]), r);
+                    r = s_fma(gamma, s_cvt<TC>(zi.v[v]), r);
+                    out.v[v] = s_cvt<TS>(r);
+                }
+            } else {
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    TC r = s_mul(alpha, acc[w * V + v]);
+                    r = s_fma(beta, s_cvt<TC>(xi.v[v]), r);
+                    out.v[v] = s_cvt<TS>(r);
+                }
+            }
+            st16(y + o, out);
+        }
+        p0 = p1;
+        p1 = p2;
+    }
+}
+
+// Layout change between the caller's column-major FP64 block and the row-major scratch, through
+// 32x32 shared-memory tiles (coalesced on both sides), converting precision and scaling.
+//   to_rm:  R[i*ld + c] = (TS) V[i + c*ldv]
+//   to_cm:  V[i + c*ldv] = scale * R[i*ld + c]
+// One 32x32 tile with row origin r0 and column origin c0 (threads 32 x 8).
+template <class TV, class TS>
+__device__ __forceinline__ void to_rm_tile(int64_t n, int64_t s, const TV* __restrict__ Vc, int64_t ldv,
+                                           TS* __restrict__ Rr, int64_t ld, int64_t r0, int64_t c0,
+                                           TS (&tile)[32][33]) {
+    const int tx = threadIdx.x, ty = threadIdx.y;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int64_t c = c0 + ty + 8 * j, r = r0 + tx;
+        tile[ty + 8 * j][tx] = (r < n && c < s) ? s_cvt<TS>(Vc[r + c * ldv]) : s_zero(TS());
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int64_t r = r0 + ty + 8 * j, c = c0 + tx;
+        if (r < n && c < s) Rr[r * ld + c] = tile[tx][ty + 8 * j];
+    }
+}
+
+template <class TS, class TV>
+__device__ __forceinline__ void to_cm_tile(int64_t n, int64_t s, const TS* __restrict__ Rr, int64_t ld,
+                                           TV* __restrict__ Vc, int64_t ldv, double scale, int64_t r0, int64_t c0,
+                                           TS (&tile)[32][33]) {
+    const int tx = threadIdx.x, ty = threadIdx.y;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int64_t r = r0 + ty + 8 * j, c = c0 + tx;
+        tile[ty + 8 * j][tx] = (r < n && c < s) ? Rr[r * ld + c] : s_zero(TS());
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int64_t c = c0 + ty + 8 * j, r = r0 + tx;
+        if (r < n && c < s) Vc[r + c * ldv] = s_rscale((real_t<TV>)scale, s_cvt<TV>(tile[tx][ty + 8 * j]));
+    }
+}
+
+}  // namespace rcb

@@ -413,6 +413,8 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
         int stallCount = 0;
 
         while ((stopCheckValue > subspaceTol) && (innerLoopCount < maxInnerLoopCount)) {
+            if (ctx_->cancel && ctx_->cancel->load(std::memory_order_relaxed))
+                return rc_fail(ctx_, RC_ERR_CANCELLED, "request cancelled");
             // ---- filter parameters (:1233-1296)
             const double shift = -minEigValue;
             starDegreeSave = starDegree;

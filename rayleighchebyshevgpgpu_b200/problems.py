@@ -166,3 +166,39 @@ def small_laplacian(dims, seed: int = 0, vmax: float = 1.0, k: int = 8, complex_
     if len(dims) == 1:
         dims = (dims[0], 1)
     return Problem(f"lap{dims}", tuple(dims), kind, d0 + V, -1.0, k=k, start_seed=seed + 100)
+
+
+@dataclass
+class ServeRequest:
+    """One request of the serving stream: its operator, eigenpair count, tolerance and arrival."""
+    index: int
+    problem: Problem
+    arrival_gap: float   # unit-rate exponential gap before this arrival (scale by 1/rate)
+
+
+def serve_stream(count: int = 256, seed: int = 5, nmin: float = 1e4, nmax: float = 2e6) -> list:
+    """Configuration 4: a Poisson stream of random-potential Laplacians.
+
+    Each request draws, from one generator seeded with `seed`: the operator (2D 5-point or 3D
+    7-point, equal odds), n log-uniform in [nmin, nmax] (grid side round(n^(1/d))), the disorder
+    W ~ U[1, 8], k from {8, 16, 32, 64} and tol from {1e-8, 1e-10}, and a unit-rate exponential
+    arrival gap. Its potential V ~ U[0, W) comes from its own generator seeded (seed, index).
+    """
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        kind = 5 if rng.random() < 0.5 else 7
+        n_target = float(np.exp(rng.uniform(np.log(nmin), np.log(nmax))))
+        W = float(rng.uniform(1.0, 8.0))
+        k = int(rng.choice([8, 16, 32, 64]))
+        tol = float(rng.choice([1e-8, 1e-10]))
+        gap = float(rng.exponential(1.0))
+        d = 2 if kind == 5 else 3
+        side = max(2, int(round(n_target ** (1.0 / d))))
+        dims = (side, side) if d == 2 else (side, side, side)
+        n = int(np.prod(dims))
+        V = np.random.default_rng([seed, i]).uniform(0.0, W, n)
+        P = Problem(f"serve{i}_{d}d{kind}pt_{side}", dims, kind, 2.0 * d + V, -1.0, k=k, tol=tol,
+                    start_seed=1000 + i, meta={"W": W})
+        out.append(ServeRequest(i, P, gap))
+    return out

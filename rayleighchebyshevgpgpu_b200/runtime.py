@@ -238,6 +238,130 @@ def solve(ctx: Context, op: Operator, params: capi.SolveParams, v0=None, host: b
     return SolveResult(evals[:f].copy(), ev, resid[:f].copy(), info.as_dict())
 
 
+# ---- request server (rc_server_*, rc_serve_*) ---------------------------------------------------
+class Request:
+    """One submitted solve. The server writes the eigenvalues, residuals and (host) eigenvectors
+    into the arrays held here when the request finishes."""
+
+    def __init__(self, server: "Server", rid: int, op: Operator, evals, resid, evecs, keep):
+        self.server = server
+        self.id = rid
+        self.op = op
+        self._evals = evals
+        self._resid = resid
+        self._evecs = evecs
+        self._keep = keep
+
+    def state(self) -> str:
+        st = C.c_int()
+        self.server._check(lib().rc_serve_poll(self.server.h, self.id, C.byref(st)), "rc_serve_poll")
+        return capi.REQ_STATE_NAMES[st.value]
+
+    def wait(self, timeout_ms: float = -1.0) -> str:
+        """Block until the request finishes (or timeout_ms passes); returns its state."""
+        st = C.c_int()
+        rc = lib().rc_serve_wait(self.server.h, self.id, float(timeout_ms), C.byref(st))
+        if rc not in (capi.RC_OK, 10):
+            self.server._check(rc, "rc_serve_wait")
+        return capi.REQ_STATE_NAMES[st.value]
+
+    def cancel(self):
+        self.server._check(lib().rc_serve_cancel(self.server.h, self.id), "rc_serve_cancel")
+
+    def info(self) -> dict:
+        """Timings and memory of the request (rc_request_info), available in every state."""
+        ri = capi.RequestInfo()
+        ri.struct_size = C.sizeof(capi.RequestInfo)
+        lib().rc_serve_result(self.server.h, self.id, None, C.byref(ri), None, 0)
+        return ri.as_dict()
+
+    def result(self) -> SolveResult:
+        """The finished solve; raises RCError with the request's own status when it failed."""
+        info = capi.SolveInfo()
+        info.struct_size = C.sizeof(capi.SolveInfo)
+        ri = capi.RequestInfo()
+        ri.struct_size = C.sizeof(capi.RequestInfo)
+        err = C.create_string_buffer(512)
+        rc = lib().rc_serve_result(self.server.h, self.id, C.byref(info), C.byref(ri), err, 512)
+        if rc != capi.RC_OK:
+            raise capi.RCError(rc, err.value.decode())
+        f = info.found
+        ev = self._evecs[:f] if isinstance(self._evecs, np.ndarray) else self._evecs
+        d = info.as_dict()
+        d["request"] = ri.as_dict()
+        return SolveResult(self._evals[:f].copy(), ev, self._resid[:f].copy(), d)
+
+    def release(self):
+        self.server._check(lib().rc_serve_release(self.server.h, self.id), "rc_serve_release")
+
+
+class Server:
+    """Continuous-batching eigen-solve server on one GPU (rc_server)."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 0, max_active: int = 16, batch_window_us: float = 200.0,
+                 use_graphs: bool = True, starvation_ms: float = 2000.0):
+        p = capi.ServerParams()
+        lib().rc_server_params_default(C.byref(p))
+        p.device = device
+        p.hbm_budget_bytes = int(budget_bytes)
+        p.max_active = int(max_active)
+        p.batch_window_us = float(batch_window_us)
+        p.use_graphs = 1 if use_graphs else 0
+        p.starvation_ms = float(starvation_ms)
+        self.h = C.c_void_p()
+        check(lib().rc_server_create(C.byref(p), C.byref(self.h)), None, "rc_server_create")
+
+    def _check(self, rc: int, what: str):
+        if rc != capi.RC_OK:
+            raw = lib().rc_server_last_error(self.h) if self.h else b""
+            raise capi.RCError(rc, f"{what}: {raw.decode() if raw else ''}")
+
+    def submit(self, op: Operator, params: capi.SolveParams, v0=None, want_vectors: bool = True) -> Request:
+        """Queue a solve; v0 and the eigenvectors are host numpy arrays (column-major blocks, given
+        and returned as (columns, n) C-ordered arrays)."""
+        k = int(params.eig_count if params.mode in (0, 1) else max(params.eig_count, 1))
+        params.host_buffers = 1
+        keep = [params]
+        if v0 is not None:
+            v0 = np.ascontiguousarray(v0, dtype=op.scalar)
+            keep.append(v0)
+            params.non_random_start = 1
+            params.v0_cols = v0.shape[0] if v0.ndim == 2 else 1
+        evals = np.zeros(max(k, 1), dtype=np.float64)
+        resid = np.zeros(max(k, 1), dtype=np.float64)
+        evecs = np.zeros((max(k, 1), op.n), dtype=op.scalar) if want_vectors else None
+        params.struct_size = C.sizeof(capi.SolveParams)
+        rid = C.c_int64()
+        self._check(lib().rc_serve_submit(self.h, op.h, C.byref(params), C.c_void_p(_ptr(v0)),
+                                          evals.ctypes.data_as(C.POINTER(C.c_double)), C.c_void_p(_ptr(evecs)),
+                                          resid.ctypes.data_as(C.POINTER(C.c_double)), C.byref(rid)),
+                    "rc_serve_submit")
+        return Request(self, rid.value, op, evals, resid, evecs, keep)
+
+    def stats(self) -> dict:
+        st = capi.ServerStats()
+        st.struct_size = C.sizeof(capi.ServerStats)
+        self._check(lib().rc_server_stats_get(self.h, C.byref(st)), "rc_server_stats_get")
+        return st.as_dict()
+
+    def close(self):
+        if self.h:
+            lib().rc_server_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # ---- kernel-level calls -------------------------------------------------------------------
 def spmm(ctx: Context, op: Operator, X, Y, s: int, alpha=1.0, beta=0.0, ldx=None, ldy=None):
     a = (C.c_double * 2)(complex(alpha).real, complex(alpha).imag)

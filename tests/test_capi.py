@@ -56,6 +56,67 @@ def test_struct_layouts_match_header(built_lib):
     assert int(out[3]) == _capi.SolveInfo.guard_value.offset
 
 
+def test_server_struct_layouts_match_header(built_lib):
+    import subprocess
+    import tempfile
+    src = ('#include "rc_b200.h"\n#include <stdio.h>\n#include <stddef.h>\nint main(){printf("%zu %zu %zu %zu %zu",'
+           'sizeof(rc_server_params), sizeof(rc_request_info), sizeof(rc_server_stats),'
+           'offsetof(rc_server_params, starvation_ms), offsetof(rc_request_info, device_bytes));return 0;}\n')
+    d = tempfile.mkdtemp()
+    with open(os.path.join(d, "t.c"), "w") as f:
+        f.write(src)
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), os.path.join(d, "t.c"), "-o",
+                           os.path.join(d, "t")])
+    out = [int(x) for x in subprocess.check_output([os.path.join(d, "t")]).decode().split()]
+    from rayleighchebyshevgpgpu_b200 import _capi
+    assert out[0] == ctypes.sizeof(_capi.ServerParams)
+    assert out[1] == ctypes.sizeof(_capi.RequestInfo)
+    assert out[2] == ctypes.sizeof(_capi.ServerStats)
+    assert out[3] == _capi.ServerParams.starvation_ms.offset
+    assert out[4] == _capi.RequestInfo.device_bytes.offset
+
+
+def test_server_calls_without_a_server_return_status(built_lib):
+    from rayleighchebyshevgpgpu_b200 import _capi
+    L = _capi.lib()
+    p = _capi.ServerParams()
+    L.rc_server_params_default(ctypes.byref(p))
+    assert p.max_active == 16 and p.use_graphs == 1 and p.struct_size == ctypes.sizeof(p)
+    assert L.rc_server_create(None, None) == 1
+    rid = ctypes.c_int64()
+    assert L.rc_serve_submit(None, None, None, None, None, None, None, ctypes.byref(rid)) == 1
+    assert L.rc_serve_poll(None, 1, None) == 1
+    assert L.rc_serve_cancel(None, 1) == 1
+    assert L.rc_server_destroy(None) == 0
+    bad = _capi.ServerParams()
+    L.rc_server_params_default(ctypes.byref(bad))
+    bad.max_active = 0
+    h = ctypes.c_void_p()
+    assert L.rc_server_create(ctypes.byref(bad), ctypes.byref(h)) == 1 and not h
+
+
+def test_serve_stream_matches_its_specification():
+    """Configuration 4's request stream: 256 requests, n log-uniform in [1e4, 2e6], k in
+    {8, 16, 32, 64}, tol in {1e-8, 1e-10}, W in [1, 8), and reproducible from its seed."""
+    from rayleighchebyshevgpgpu_b200 import problems
+    S = problems.serve_stream()
+    T = problems.serve_stream()
+    assert len(S) == 256
+    ns = np.array([r.problem.n for r in S])
+    assert ns.min() >= 0.95e4 and ns.max() <= 2.05e6
+    assert {r.problem.k for r in S} == {8, 16, 32, 64}
+    assert {r.problem.tol for r in S} == {1e-8, 1e-10}
+    assert {r.problem.kind for r in S} == {5, 7}
+    for a, b in zip(S[:5], T[:5]):
+        assert a.problem.dims == b.problem.dims and np.array_equal(a.problem.diag, b.problem.diag)
+        W = a.problem.meta["W"]
+        d0 = 4.0 if a.problem.kind == 5 else 6.0
+        assert 1.0 <= W < 8.0 and a.problem.diag.min() >= d0 and a.problem.diag.max() < d0 + W
+    # log-uniform: about half the requests below the geometric midpoint
+    mid = np.sqrt(1e4 * 2e6)
+    assert 0.35 < np.mean(ns < mid) < 0.65
+
+
 def test_cpoly_xstar_matches_reference_golden(built_lib):
     from rayleighchebyshevgpgpu_b200 import runtime as R
     g = json.load(open(os.path.join(GOLD, "cpoly.json")))
