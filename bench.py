@@ -36,17 +36,17 @@ CONFIG2_FP64_DEGREE_STEPS = 1659
 
 
 def profile_dram_bytes_per_row():
-    """DRAM bytes per grid row of one filter degree-step, from the committed ncu summary
-    (a line "dram-bytes-per-row fp32=<B> fp64=<B>"), or None."""
-    path = os.path.join(ROOT, "profiles", "rm_step_kernel_csr_96cube_s96.md")
-    try:
-        for line in open(path):
-            if line.startswith("dram-bytes-per-row"):
-                kv = dict(t.split("=") for t in line.split()[1:])
-                return {"fp32": float(kv["fp32"]), "fp64": float(kv["fp64"])}
-    except (OSError, ValueError, KeyError):
-        return None
-    return None
+    """DRAM bytes per grid row of one filter degree-step, from the committed ncu summaries
+    (lines "dram-bytes-per-row fp32=<B> fp64=<B>" and "dram-bytes-per-row corr=<B>"), or None."""
+    out = {}
+    for name in ("rm_step_kernel_csr_96cube_s96.md", "rm_step_src_kernel_csr_96cube_s96.md"):
+        try:
+            for line in open(os.path.join(ROOT, "profiles", name)):
+                if line.startswith("dram-bytes-per-row"):
+                    out.update({k: float(v) for k, v in (t.split("=") for t in line.split()[1:])})
+        except (OSError, ValueError):
+            pass
+    return out if "fp32" in out and "fp64" in out else None
 
 
 def parse():
@@ -306,7 +306,8 @@ def run_ours(args):
 
     # ---- roofline of the dominant kernel: the fused filter degree-step (rm_step_kernel) ----
     # Algorithmic bytes of one degree-step over the n x s block: the matrix once (values + column
-    # indices + row pointers) and three block passes (read x_{k-1}, read x_{k-2}, write x_k).
+    # indices + row pointers) and three block passes (read x_{k-1}, read x_{k-2}, write x_k); the
+    # correction filter's step (rm_step_src_kernel) also reads the residual block: four passes.
     # The step time is the CUDA-event time of the degree-step launches inside the timed solves
     # (info.time_filter_steps_ms, transposes excluded). Degree-1 filters (column-major path, at
     # most a few per solve) are counted in degree_steps but not timed, a < 0.1 % overstatement.
@@ -314,11 +315,14 @@ def run_ours(args):
     b_a32 = nnz * (4 + 4) + (P.n + 1) * 4
     b_a64 = nnz * (8 + 4) + (P.n + 1) * 4
     bytes_fp32_step = b_a32 + 3 * P.n * s * 4
+    bytes_corr_step = b_a32 + 4 * P.n * s * 4
     bytes_fp64_step = b_a64 + 3 * P.n * s * 8
     fsteps = sum(i["degree_steps"] for i in infos)
     f64steps = sum(i["fp64_degree_steps"] for i in infos)
+    csteps = sum(i["correction_degree_steps"] for i in infos)
+    p32steps = fsteps - f64steps - csteps
     tsteps = sum(i["time_filter_steps_ms"] for i in infos) * 1e-3
-    alg_bytes = (fsteps - f64steps) * bytes_fp32_step + f64steps * bytes_fp64_step
+    alg_bytes = p32steps * bytes_fp32_step + csteps * bytes_corr_step + f64steps * bytes_fp64_step
     achieved = alg_bytes / tsteps / 1e9 if tsteps > 0 else None
     peaks = {}
     try:
@@ -331,7 +335,10 @@ def run_ours(args):
     traffic = None
     per_row = profile_dram_bytes_per_row()
     if per_row and fsteps:
-        traffic = P.n * ((fsteps - f64steps) * per_row["fp32"] + f64steps * per_row["fp64"]) / fsteps
+        # without a capture of the correction step, its rows count as FP32 rows plus one more
+        # FP32 block row (the residual block)
+        corr_row = per_row.get("corr", per_row["fp32"] + s * 4)
+        traffic = P.n * (p32steps * per_row["fp32"] + csteps * corr_row + f64steps * per_row["fp64"]) / fsteps
     # ---- CPU baseline (rank 0, N = 1) ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -361,20 +368,23 @@ def run_ours(args):
         "accuracy": {"max_rel_eig_diff_mixed_vs_fp64": eig_err, "max_subspace_angle_mixed_vs_fp64": angle,
                      "max_rel_residual": max_res_rel, "found": int(res_mixed.info["found"])},
         "solve_info": {"mixed": {k2: infos[-1][k2] for k2 in ("inner_iterations", "degree_steps", "fp64_degree_steps",
+                                                               "correction_iterations", "correction_degree_steps",
                                                                "mixed_iterations", "lanczos_iterations",
                                                                "cholqr_passes", "fused_rr", "fused_rr_fallbacks",
                                                                "time_lanczos_ms", "time_filter_ms",
                                                                "time_filter_steps_ms",
                                                                "time_ortho_ms", "time_eigenvalue_ms")},
-                       "fp64": {k2: info64[k2] for k2 in ("inner_iterations", "degree_steps", "time_filter_ms",
+                       "fp64": {k2: info64[k2] for k2 in ("inner_iterations", "degree_steps", "fp64_degree_steps",
+                                                           "time_filter_ms",
                                                            "time_filter_steps_ms",
                                                            "time_ortho_ms", "time_eigenvalue_ms")} if info64 else None},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                      "peak_source": peak_src, "kernel": "rm_step_kernel (fused filter degree-step, CSR)",
                      "algorithmic_bytes_per_launch": alg_bytes / fsteps if fsteps else None,
-                     "launches": fsteps, "fp64_launches": f64steps,
-                     "bytes_per_launch_fp32": bytes_fp32_step, "bytes_per_launch_fp64": bytes_fp64_step},
+                     "launches": fsteps, "fp64_launches": f64steps, "correction_launches": csteps,
+                     "bytes_per_launch_fp32": bytes_fp32_step, "bytes_per_launch_correction": bytes_corr_step,
+                     "bytes_per_launch_fp64": bytes_fp64_step},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "eigenpairs/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},

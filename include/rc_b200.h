@@ -224,6 +224,11 @@ typedef struct rc_solve_params {
     int orth_mode;                 /* 0: Rayleigh-Ritz on the filtered block with the Cholesky factor of its
                                       scaled Gram matrix folded in, CholeskyQR2 when that matrix is
                                       ill-conditioned; 1: always CholeskyQR2 then Rayleigh-Ritz */
+    int mixed_refine;              /* MIXED, after the switch tolerance: 0 (default) the FP32 correction
+                                      filter (the recurrence applied to the residual block A V - V diag(lam)
+                                      of the Ritz vectors, whose FP32 rounding error shrinks with the
+                                      residual; real operators, subspace <= 96; FP64 filter otherwise or
+                                      when it stalls); 1 the FP64 filter */
 } rc_solve_params;
 
 typedef struct rc_solve_info {
@@ -255,6 +260,8 @@ typedef struct rc_solve_info {
     int64_t fused_rr_fallbacks;    /* of those, rejected for conditioning and redone after CholeskyQR2 */
     double time_filter_steps_ms;   /* part of time_filter_ms spent in the fused degree-step launches
                                       themselves (row-major filter, transposes excluded; phase_timing = 1) */
+    int64_t correction_iterations; /* MIXED: inner iterations that ran the FP32 correction filter */
+    int64_t correction_degree_steps; /* of degree_steps, those of the correction filter */
 } rc_solve_info;
 
 void rc_solve_params_default(rc_solve_params* p);

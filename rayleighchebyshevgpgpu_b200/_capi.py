@@ -59,6 +59,7 @@ class SolveParams(C.Structure):
         ("verbose", C.c_int),
         ("phase_timing", C.c_int),
         ("orth_mode", C.c_int),
+        ("mixed_refine", C.c_int),
     ]
 
 
@@ -91,6 +92,8 @@ class SolveInfo(C.Structure):
         ("fused_rr", c_i64),
         ("fused_rr_fallbacks", c_i64),
         ("time_filter_steps_ms", C.c_double),
+        ("correction_iterations", c_i64),
+        ("correction_degree_steps", c_i64),
     ]
 
     def as_dict(self) -> dict:

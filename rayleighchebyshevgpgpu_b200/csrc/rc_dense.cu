@@ -296,10 +296,12 @@ rc_status xt(rc_ctx* ctx, int dtype, const XtArgs& a) {
     if (a.n <= 0 || a.nc <= 0) return RC_OK;
     // real fast path: plain products and residual-only dual products
     const bool plain = a.alpha == 1.0 && a.beta == 0.0;
-    const bool dual_res_only = a.X2 != nullptr && a.Y2 == nullptr && a.lam != nullptr && a.res_count > 0;
+    const bool dual_res_only =
+        a.X2 != nullptr && a.Y2 == nullptr && a.lam != nullptr && (a.res_count > 0 || a.R32 != nullptr);
     if (plain && (a.X2 == nullptr || dual_res_only) && xt2_supported(dtype, a.k, a.nc))
         return xt2(ctx, a.n, a.k, a.nc, (const double*)a.X, a.ldx, (const double*)a.T, a.ldt, (double*)a.Y, a.ldy,
-                   (const double*)a.X2, a.ldx2, a.lam, dual_res_only ? a.res_count : 0, a.res);
+                   (const double*)a.X2, a.ldx2, a.lam, dual_res_only ? a.res_count : 0, a.res, a.R32, a.ldr);
+    if (a.R32) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "xt: the FP32 residual block needs a real block of <= 96 columns");
     return dtype == RC_COMPLEX128 ? xt_t<double2>(ctx, a) : xt_t<double>(ctx, a);
 }
 
@@ -426,14 +428,12 @@ rc_status chol_factor(rc_ctx* ctx, int dtype, int64_t s, int64_t nrows, const vo
     }
     if (dtype == RC_COMPLEX128) {
         if (dyn > 48 * 1024)
-            RC_CU(ctx, cudaFuncSetAttribute(chol_factor_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)dyn));
+            RC_CU(ctx, allow_max_smem(ctx, chol_factor_kernel<double2>));
         chol_factor_kernel<double2><<<1, 1024, dyn, ctx->stream>>>((int)s, nrows, (const double2*)G, (double2*)base,
                                                                   (double2*)Tout, dsc, flags, pivout, mode);
     } else {
         if (dyn > 48 * 1024)
-            RC_CU(ctx, cudaFuncSetAttribute(chol_factor_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)dyn));
+            RC_CU(ctx, allow_max_smem(ctx, chol_factor_kernel<double>));
         chol_factor_kernel<double><<<1, 1024, dyn, ctx->stream>>>((int)s, nrows, (const double*)G, (double*)base,
                                                                  (double*)Tout, dsc, flags, pivout, mode);
     }
@@ -631,12 +631,12 @@ rc_status small_eigh_work(rc_ctx* ctx, int dtype, int64_t s, void* A, void* Q, d
     const int sweeps = 60;
     if (dtype == RC_COMPLEX128) {
         if (dyn > 48 * 1024)
-            RC_CU(ctx, cudaFuncSetAttribute(jacobi_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+            RC_CU(ctx, allow_max_smem(ctx, jacobi_kernel<double2>));
         jacobi_kernel<double2><<<1, 1024, dyn, ctx->stream>>>((int)s, (const double2*)A, (double2*)Q, evals, info,
                                                               (double2*)work, fit ? 1 : 0, sweeps);
     } else {
         if (dyn > 48 * 1024)
-            RC_CU(ctx, cudaFuncSetAttribute(jacobi_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+            RC_CU(ctx, allow_max_smem(ctx, jacobi_kernel<double>));
         jacobi_kernel<double><<<1, 1024, dyn, ctx->stream>>>((int)s, (const double*)A, (double*)Q, evals, info,
                                                              (double*)work, fit ? 1 : 0, sweeps);
     }

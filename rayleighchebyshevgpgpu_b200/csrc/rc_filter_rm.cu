@@ -28,6 +28,43 @@ rm_step_kernel(Pol op, int64_t n, int nseg, int64_t ld, int groups, const TS* __
                                      pf_x);
 }
 
+// Degree step of the correction filter: y = alpha A x + beta x + gamma z + sig[c] src.
+template <class Pol, class TS, class TC, int W, class IX>
+__global__ void __launch_bounds__(kRmThreads, rm_min_blocks<TS>())
+rm_step_src_kernel(Pol op, int64_t n, int nseg, int64_t ld, int groups, const TS* __restrict__ x, const TS* z, TS* y,
+                   TC alpha, TC beta, TC gamma, int64_t pf_z, int64_t pf_x, const TS* __restrict__ src,
+                   const float* __restrict__ sig) {
+    rm_step_rows<Pol, TS, TC, W, IX, true>(op, n, nseg, ld, groups, (int64_t)blockIdx.x, x, z, y, alpha, beta, gamma,
+                                           pf_z, pf_x, src, sig);
+}
+
+// Scalar recurrence of the correction filter, one thread per column c:
+//   c_0 = 1, c_1 = a lam_c + b, c_k = (a lam_c + b) c_{k-1} - c_{k-2};
+//   sig[k*ld + c] = c_{k-1} for 2 <= k <= m (the source coefficient of step k),
+//   coef[c] = c_m / (m+1) (the weight of v_c in the result). Columns s..ld get zeros.
+__global__ void corr_coef_kernel(int64_t s, int64_t ld, int64_t m, double a, double b, const double* __restrict__ lam,
+                                 float* __restrict__ sig, double* __restrict__ coef) {
+    for (int64_t c = threadIdx.x; c < ld; c += blockDim.x) {
+        const double t = c < s ? a * lam[c] + b : 0.0;
+        double cm2 = 1.0, cm1 = t;  // c_0, c_1
+        for (int64_t k = 2; k <= m; ++k) {
+            sig[k * ld + c] = c < s ? (float)cm1 : 0.0f;
+            const double ck = t * cm1 - cm2;
+            cm2 = cm1;
+            cm1 = ck;
+        }
+        if (c < s) coef[c] = (m >= 1 ? cm1 : 1.0) / (double)(m + 1);
+    }
+}
+
+template <class TS>
+__global__ void __launch_bounds__(256)
+corr_to_cm_kernel(int64_t n, int64_t s, const TS* __restrict__ E, int64_t ld, double* __restrict__ Vc, int64_t ldv,
+                  const double* __restrict__ coef, double beta) {
+    __shared__ TS tile[32][33];
+    corr_to_cm_tile<TS>(n, s, E, ld, Vc, ldv, coef, beta, (int64_t)blockIdx.x * 32, (int64_t)blockIdx.y * 32, tile);
+}
+
 
 template <class TV, class TS>
 __global__ void __launch_bounds__(256)
@@ -95,6 +132,49 @@ static rc_status run_rm_filter(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, 
     return RC_OK;
 }
 
+// The correction filter (FP32 storage, real operators). V holds Ritz vectors v_c with Ritz values
+// lam_c, and R = A V - V diag(lam) (row-major FP32, leading dimension ld). With x_k = c_k v + a e_k
+// (c_k the scalar recurrence at lam_c) the recurrence of run_rm_filter becomes
+//   e_0 = 0, e_1 = R, e_k = a A e_{k-1} + b e_{k-1} - e_{k-2} + c_{k-1} R,
+// and the result x_m/(m+1) = coef_c v_c + a e_m/(m+1) is formed in FP64. e_k is small (of the size
+// of the residual), so its FP32 rounding perturbs the filtered block by FP32 rounding times the
+// residual instead of times the block: the subspace keeps converging past the FP32 floor of the
+// plain FP32 filter. e_2 -> A, e_3 -> B (e_1 = R is read as x_{k-2}), then e_k over e_{k-2}.
+template <class Pol, class TS, class TC, int W, class IX>
+static rc_status run_rm_corr(rc_ctx* ctx, const Pol& pol, int64_t n, double* V, int64_t ldv, int64_t s,
+                             int64_t degree, double a, double b, const TS* R, const float* sig, const double* coef,
+                             TS* A, TS* B, int64_t ld, int64_t band) {
+    const int64_t pf_z = ctx->pf_rows;
+    const int64_t pf_x = pf_z > 0 ? pf_z + band : 0;
+    constexpr int VEC = Pack16<TS>::V;
+    const TC ta = s_from<TC>(a, 0.0), tb = s_from<TC>(b, 0.0), tm1 = s_from<TC>(-1.0, 0.0);
+    if (ld % (VEC * W) != 0) return rc_fail(ctx, RC_ERR_INVALID, "correction filter: leading dimension not padded");
+    const int nseg = (int)(ld / (VEC * W));
+    if (nseg > kRmThreads) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "correction filter: block too wide");
+    const int rows_per_iter = kRmThreads / nseg;
+    constexpr bool kCsr = Pol::kIsCsr;
+    const int groups = ctx->rm_groups > 0 ? ctx->rm_groups : (kCsr ? 4 : 8);
+    const int64_t rows_per_cta = (int64_t)groups * rows_per_iter;
+    const unsigned grid_seg = (unsigned)((n + rows_per_cta - 1) / rows_per_cta);
+    step_mark(ctx);
+    for (int64_t k = 2; k <= degree; ++k) {
+        const TS* xk1 = k == 2 ? R : ((k - 1) % 2 == 0 ? A : B);   // e_{k-1}
+        TS* y = k % 2 == 0 ? A : B;                                  // e_k
+        const TS* z = k == 2 ? nullptr : (k == 3 ? R : y);           // e_{k-2}
+        rm_step_src_kernel<Pol, TS, TC, W, IX><<<grid_seg, kRmThreads, 0, ctx->stream>>>(
+            pol, n, nseg, ld, groups, xk1, z, y, ta, tb, k == 2 ? s_zero(TC()) : tm1, pf_z, pf_x, R, sig + k * ld);
+        ctx->launches++;
+    }
+    RC_CU(ctx, cudaGetLastError());
+    step_mark(ctx);
+    const TS* em = degree == 1 ? R : (degree % 2 == 0 ? A : B);
+    const dim3 tgrid((unsigned)((n + 31) / 32), (unsigned)((s + 31) / 32)), tblk(32, 8);
+    corr_to_cm_kernel<TS><<<tgrid, tblk, 0, ctx->stream>>>(n, s, em, ld, V, ldv, coef, a / (double)(degree + 1));
+    ctx->launches++;
+    RC_CU(ctx, cudaGetLastError());
+    return RC_OK;
+}
+
 // Offset type and slices per thread: 32-bit offsets when the block's last element offset fits;
 // two 16-byte slices per thread for CSR with FP64 storage and one otherwise (the faster choice
 // on 128^3 7-point operators with 96 columns), unless the context sets the count
@@ -139,6 +219,56 @@ static rc_status rm_filter_dispatch(rc_ctx* ctx, rc_op* op, void* V, int64_t ldv
     }
     StencilRows<TD, TC, 5> pol{op->nx, op->ny, op->nz, dg, op->offdiag, theta};
     return run_rm_select<StencilRows<TD, TC, 5>, TS, TC>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band);
+}
+
+template <class Pol>
+static rc_status rm_corr_select(rc_ctx* ctx, const Pol& pol, int64_t n, double* V, int64_t ldv, int64_t s,
+                                int64_t degree, double a, double b, const float* R, const float* sig,
+                                const double* coef, float* A, float* B, int64_t ld, int64_t band) {
+    if ((n + 1) * ld < ((int64_t)1 << 32))
+        return run_rm_corr<Pol, float, float, 1, uint32_t>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B,
+                                                           ld, band);
+    return run_rm_corr<Pol, float, float, 1, int64_t>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld,
+                                                      band);
+}
+
+bool rm_corr_supported(const rc_op* op, int64_t s) {
+    return op->dtype == RC_REAL64 && op->kind != 2 && s >= 1 && s <= 96 &&
+           (op->kind == 0 || op->skind == 5 || op->skind == 7 || op->skind == 27);
+}
+
+rc_status rm_filter_corr(rc_ctx* ctx, rc_op* op, double* V, int64_t ldv, int64_t s, int64_t degree, double a,
+                         double b, const double* lam_dev, const float* R, void* bufA, void* bufB) {
+    if (!rm_corr_supported(op, s)) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "correction filter: unsupported operator");
+    if (degree < 1) return RC_OK;
+    RC_TRY(ensure_fp32(ctx, op));
+    const int64_t ld = rm_leading_dim(RC_REAL64, P32, s);
+    void* tab = nullptr;
+    RC_TRY(rc_slot(ctx, S_CORR, (size_t)(degree + 1) * ld * sizeof(float) + (size_t)ld * sizeof(double) + 256, &tab));
+    float* sig = (float*)tab;
+    double* coef = (double*)((char*)tab + (((size_t)(degree + 1) * ld * sizeof(float) + 255) / 256) * 256);
+    corr_coef_kernel<<<1, 128, 0, ctx->stream>>>(s, ld, degree, a, b, lam_dev, sig, coef);
+    ctx->launches++;
+    RC_CU(ctx, cudaGetLastError());
+    const int64_t n = op->n;
+    const int64_t band = op->kind == 0 ? op->band : (op->skind == 5 ? op->nx : op->nx * op->ny);
+    float* A = (float*)bufA;
+    float* B = (float*)bufB;
+    if (op->kind == 0) {
+        CsrRows<float, float> pol{op->rowptr, op->colind, (const float*)op->vals32};
+        return rm_corr_select(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band);
+    }
+    const double theta = 0.0;
+    if (op->skind == 27) {
+        StencilRows<float, float, 27> pol{op->nx, op->ny, op->nz, op->diag32, op->offdiag, theta};
+        return rm_corr_select(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band);
+    }
+    if (op->skind == 7) {
+        StencilRows<float, float, 7> pol{op->nx, op->ny, op->nz, op->diag32, op->offdiag, theta};
+        return rm_corr_select(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band);
+    }
+    StencilRows<float, float, 5> pol{op->nx, op->ny, op->nz, op->diag32, op->offdiag, theta};
+    return rm_corr_select(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band);
 }
 
 // Row length padded to 32 bytes (two 16-byte slices); the padding columns are never read back.

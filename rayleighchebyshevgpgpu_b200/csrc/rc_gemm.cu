@@ -1,106 +1,163 @@
-// rc_gemm.cu -- FP64 tall-skinny GEMMs of the Rayleigh-Ritz step for real blocks with s <= 96.
+// rc_gemm.cu -- FP64 tall-skinny GEMMs of the Rayleigh-Ritz step for real blocks with s <= 96,
+// on the FP64 tensor pipe (mma.sync m8n8k4 .f64, which runs at the full FP64 rate on sm_100a and
+// needs a quarter of the shared-memory reads of a register-tiled DFMA loop).
 //
 //  gram2: C_y = X^T Y_y for up to two right-hand blocks (G = V^T V and H = V^T (A V) in one
-//         launch). Grid (row chunk, y): each CTA accumulates the whole s x s product of its row
-//         chunk, 256 threads with 6x6 (in general R x R, 16R >= s) register tiles; the next
-//         K-tile of X and Y is staged in registers while the current one is consumed from
-//         shared memory (padded rows: conflict-free stores and broadcast/contiguous reads).
-//         Per-chunk partials are summed by gram_reduce in a fixed order (deterministic).
-//  xt2:   Y = X T (n x k times k x nc, k, nc <= 96), persistent CTAs holding T in shared
-//         memory; the dual form also forms W T on the fly for the first res_count columns and
-//         reduces only ||(W T)_c - lam_c (X T)_c||^2 per column (W T itself is not stored).
+//         launch), both symmetric: only the 32x32 super-blocks on and above the diagonal are
+//         formed (the reference's CPU formVtAV also forms the upper triangle,
+//         RayleighChebyshevLM.h:1928-1969). One CTA per SM walks its chunk of rows in 32-row
+//         K-tiles, double-buffered in shared memory by cp.async; warp (y, bi, bj) accumulates
+//         the 32x32 super-block (bi, bj) of C_y in 16 mma tiles. Per-chunk partials are summed
+//         by gram2_reduce_kernel in a fixed order (deterministic).
+//  xt2:   Y = X T (n x k times k x nc, k, nc <= 96), persistent CTAs with T resident in shared
+//         memory and 32-row tiles of X (and W) double-buffered; warp (slab, half) forms 8 rows x
+//         48 columns. The dual form also forms W T for the columns that need it and reduces
+//         ||(W T)_c - lam_c (X T)_c||^2 for c < res_count; with R32 it writes the residual block
+//         R = W T - (X T) diag(lam) in row-major FP32 (the source term of the correction filter).
 // These replace cublasDgemm(OP_T, OP_N) and cublasDgemm(OP_N, OP_N) plus the residual kernel
 // of the reference (RayleighChebyshevLMCuda.h:2139-2161, :2200-2285).
+//
+// mma.m8n8k4 .f64 fragments (g = lane / 4, q = lane % 4): A (8x4, row) a = A[g][q];
+// B (4x8, col) b = B[q][g]; C (8x8) {c0, c1} = C[g][2q], C[g][2q+1].
 #include <algorithm>
 #include "rc_common.cuh"
 #include "rc_internal.h"
 
 namespace rcb {
 
-constexpr int G2_THREADS = 256;
-constexpr int G2_KT = 16;
-
-template <int R>
-__global__ void __launch_bounds__(G2_THREADS, (R >= 6 ? 1 : 2))
-gram2_kernel(int64_t n, int m, int nc, const double* __restrict__ X, int64_t ldx, const double* __restrict__ Y0,
-             int64_t ldy0, const double* __restrict__ Y1, int64_t ldy1, double* __restrict__ part, int64_t rows) {
-    constexpr int TB = 16 * R;
-    constexpr int S = TB + 1;  // padded smem row (conflict-free stores of consecutive rows)
-    constexpr int NL = (G2_KT * TB) / G2_THREADS;  // elements per thread per operand per K-tile
-    extern __shared__ __align__(16) double g2s[];
-    double* Xs = g2s;                    // [2][KT][S]
-    double* Ys = g2s + 2 * G2_KT * S;    // [2][KT][S]
-    const double* Y = blockIdx.y == 0 ? Y0 : Y1;
-    const int64_t ldy = blockIdx.y == 0 ? ldy0 : ldy1;
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    const int64_t r_begin = (int64_t)blockIdx.x * rows;
-    const int64_t r_end = min(n, r_begin + rows);
-    double acc[R][R];
-#pragma unroll
-    for (int i = 0; i < R; ++i)
-#pragma unroll
-        for (int j = 0; j < R; ++j) acc[i][j] = 0.0;
-    double rx[NL], ry[NL];
-    auto fetch = [&](int64_t r0) {
-#pragma unroll
-        for (int l = 0; l < NL; ++l) {
-            const int e = tid + l * G2_THREADS;
-            const int kk = e % G2_KT, c = e / G2_KT;
-            const int64_t r = r0 + kk;
-            const bool ok = r < r_end;
-            rx[l] = (ok && c < m) ? __ldg(X + r + (int64_t)c * ldx) : 0.0;
-            ry[l] = (ok && c < nc) ? __ldg(Y + r + (int64_t)c * ldy) : 0.0;
-        }
-    };
-    auto stash = [&](int buf) {
-        double* xs = Xs + buf * G2_KT * S;
-        double* ys = Ys + buf * G2_KT * S;
-#pragma unroll
-        for (int l = 0; l < NL; ++l) {
-            const int e = tid + l * G2_THREADS;
-            const int kk = e % G2_KT, c = e / G2_KT;
-            xs[kk * S + c] = rx[l];
-            ys[kk * S + c] = ry[l];
-        }
-    };
-    int buf = 0;
-    if (r_begin < r_end) {
-        fetch(r_begin);
-        stash(0);
-    }
-    __syncthreads();
-    for (int64_t r0 = r_begin; r0 < r_end; r0 += G2_KT) {
-        const bool more = r0 + G2_KT < r_end;
-        if (more) fetch(r0 + G2_KT);
-        const double* xs = Xs + buf * G2_KT * S;
-        const double* ys = Ys + buf * G2_KT * S;
-#pragma unroll
-        for (int kk = 0; kk < G2_KT; ++kk) {
-            double a[R], b[R];
-#pragma unroll
-            for (int i = 0; i < R; ++i) a[i] = xs[kk * S + tx + 16 * i];
-#pragma unroll
-            for (int j = 0; j < R; ++j) b[j] = ys[kk * S + ty + 16 * j];
-#pragma unroll
-            for (int i = 0; i < R; ++i)
-#pragma unroll
-                for (int j = 0; j < R; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-        }
-        if (more) stash(buf ^ 1);
-        __syncthreads();
-        buf ^= 1;
-    }
-    double* P = part + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * (size_t)m * nc;
-#pragma unroll
-    for (int i = 0; i < R; ++i)
-#pragma unroll
-        for (int j = 0; j < R; ++j) {
-            const int mi = tx + 16 * i, nj = ty + 16 * j;
-            if (mi < m && nj < nc) P[mi + (int64_t)nj * m] = acc[i][j];
-        }
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
 }
 
-// C_y[i,j] = sum over chunks of part[y][chunk][i,j]; mirrored to exact symmetry (upper kept).
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// 16-byte (two rows) or 8-byte (one row) asynchronous copy global -> shared; bytes beyond
+// src_bytes are zero-filled (src_bytes = 0 reads nothing).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+
+// Copy rows [r0, r0 + RT) of columns [0, ncols) of a column-major block into a shared tile laid
+// out column by column with `rp` doubles per column (rows past r_end read as zero).
+template <int RT, bool V16>
+__device__ __forceinline__ void load_cols_async(double* tile, int rp, const double* __restrict__ src, int64_t ld,
+                                                int ncols, int64_t r0, int64_t r_end, int tid, int nthreads) {
+    if (V16) {
+        constexpr int H = RT / 2;
+        for (int e = tid; e < ncols * H; e += nthreads) {
+            const int c = e / H, rr = 2 * (e - c * H);
+            const int64_t r = r0 + rr;
+            const int64_t left = r_end - r;
+            const int bytes = left >= 2 ? 16 : (left == 1 ? 8 : 0);
+            const double* gp = bytes ? src + r + (int64_t)c * ld : src;
+            cp_async16(tile + c * rp + rr, gp, bytes);
+        }
+    } else {
+        for (int e = tid; e < ncols * RT; e += nthreads) {
+            const int c = e / RT, rr = e - c * RT;
+            const int64_t r = r0 + rr;
+            const bool ok = r < r_end;
+            cp_async8(tile + c * rp + rr, ok ? src + r + (int64_t)c * ld : src, ok ? 8 : 0);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// gram2
+// ---------------------------------------------------------------------------------------
+constexpr int GM_KT = 32;          // rows per K-tile
+constexpr int GM_KP = GM_KT + 4;   // doubles per column in shared memory (= 4 mod 16: conflict-free fragments)
+
+template <int SB, int NY>
+constexpr int gm_threads() {
+    return 32 * NY * SB * (SB + 1) / 2;
+}
+
+template <int SB, int NY, bool V16>
+__global__ void __launch_bounds__(gm_threads<SB, NY>(), 1)
+gram_mma_kernel(int64_t n, int m, const double* __restrict__ X, int64_t ldx, const double* __restrict__ Y0,
+                int64_t ldy0, const double* __restrict__ Y1, int64_t ldy1, double* __restrict__ part, int64_t rows) {
+    constexpr int NT = gm_threads<SB, NY>();
+    constexpr int NP = SB * (SB + 1) / 2;
+    constexpr int SC = 32 * SB;                 // padded columns
+    constexpr int OPS = 1 + NY;                 // operands per stage
+    constexpr int STAGE = OPS * SC * GM_KP;     // doubles per stage
+    extern __shared__ __align__(16) double gms[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, q = lane & 3;
+    const int y = warp / NP;
+    int pidx = warp - y * NP, bi = 0;
+    while (pidx >= SB - bi) {  // (bi, bj) with bi <= bj, row by row over the upper triangle
+        pidx -= SB - bi;
+        ++bi;
+    }
+    const int bj = bi + pidx;
+    const int64_t r_begin = (int64_t)blockIdx.x * rows;
+    const int64_t r_end = min(n, r_begin + rows);
+    // zero the padding columns m..SC of every operand of both stages once (never copied into)
+    {
+        const int per = (SC - m) * GM_KP;
+        for (int e = tid; e < 2 * OPS * per; e += NT) {
+            const int st = e / per, f = e - st * per;
+            gms[st * SC * GM_KP + m * GM_KP + f] = 0.0;
+        }
+    }
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    const int64_t ntiles = r_end > r_begin ? (r_end - r_begin + GM_KT - 1) / GM_KT : 0;
+    auto issue = [&](int64_t t) {
+        double* st = gms + (t & 1) * STAGE;
+        const int64_t r0 = r_begin + t * GM_KT;
+        load_cols_async<GM_KT, V16>(st, GM_KP, X, ldx, m, r0, r_end, tid, NT);
+        load_cols_async<GM_KT, V16>(st + SC * GM_KP, GM_KP, Y0, ldy0, m, r0, r_end, tid, NT);
+        if (NY == 2) load_cols_async<GM_KT, V16>(st + 2 * SC * GM_KP, GM_KP, Y1, ldy1, m, r0, r_end, tid, NT);
+    };
+    if (ntiles > 0) issue(0);
+    cp_async_commit();
+    for (int64_t t = 0; t < ntiles; ++t) {
+        if (t + 1 < ntiles) issue(t + 1);
+        cp_async_commit();
+        cp_async_wait1();
+        __syncthreads();
+        const double* xs = gms + (t & 1) * STAGE + (bi * 32 + g) * GM_KP + q;
+        const double* ys = gms + (t & 1) * STAGE + (1 + y) * SC * GM_KP + (bj * 32 + g) * GM_KP + q;
+#pragma unroll
+        for (int k0 = 0; k0 < GM_KT; k0 += 4) {
+            double a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = xs[i * 8 * GM_KP + k0];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = ys[j * 8 * GM_KP + k0];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+        }
+        __syncthreads();
+    }
+    double* P = part + ((size_t)y * gridDim.x + blockIdx.x) * (size_t)m * m;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int row = bi * 32 + i * 8 + g, col = bj * 32 + j * 8 + 2 * q + h;
+                if (row < m && col < m) P[row + (int64_t)col * m] = acc[i][j][h];
+            }
+}
+
+// C_y[i,j] = sum over chunks of part[y][chunk][i,j] for i <= j; mirrored to exact symmetry.
 __global__ void gram2_reduce_kernel(int m, int64_t nchunks, int ny, const double* __restrict__ part, double* C0,
                                     double* C1) {
     const int64_t total = (int64_t)m * m;
@@ -121,138 +178,193 @@ __global__ void gram2_reduce_kernel(int m, int64_t nchunks, int ny, const double
 
 bool gram2_supported(int dtype, int64_t m) { return dtype == RC_REAL64 && m >= 1 && m <= 96; }
 
+template <int SB, int NY, bool V16>
+static rc_status gram_mma_launch(rc_ctx* ctx, int64_t n, int64_t m, const double* X, int64_t ldx, const double* Y0,
+                                 int64_t ldy0, const double* Y1, int64_t ldy1, double* part, int64_t nchunks,
+                                 int64_t rows) {
+    constexpr int NT = gm_threads<SB, NY>();
+    const size_t smem = (size_t)2 * (1 + NY) * 32 * SB * GM_KP * sizeof(double);
+    RC_CU(ctx, allow_max_smem(ctx, gram_mma_kernel<SB, NY, V16>));
+    gram_mma_kernel<SB, NY, V16><<<(unsigned)nchunks, NT, smem, ctx->stream>>>(n, (int)m, X, ldx, Y0, ldy0, Y1,
+                                                                               ldy1, part, rows);
+    return RC_OK;
+}
+
 // C0 = X^T Y0 and (if Y1) C1 = X^T Y1, square m x m symmetric results (upper computed, mirrored).
 rc_status gram2(rc_ctx* ctx, int64_t n, int64_t m, const double* X, int64_t ldx, const double* Y0, int64_t ldy0,
                 double* C0, const double* Y1, int64_t ldy1, double* C1) {
     const int ny = Y1 ? 2 : 1;
-    const int R = m <= 32 ? 2 : (m <= 48 ? 3 : (m <= 64 ? 4 : 6));
-    int64_t nchunks = (2 * ctx->sm_count + ny - 1) / ny;
+    const int sb = (int)((m + 31) / 32);
+    // one CTA per SM for the widest blocks; narrower blocks run several CTAs per SM
+    const int per_sm = sb == 3 ? 1 : (sb == 2 ? 2 : 4);
+    int64_t nchunks = (int64_t)ctx->sm_count * per_sm;
     int64_t rows = (n + nchunks - 1) / nchunks;
-    rows = ((rows + G2_KT - 1) / G2_KT) * G2_KT;
+    rows = ((rows + GM_KT - 1) / GM_KT) * GM_KT;
     nchunks = (n + rows - 1) / rows;
     void* part = nullptr;
     RC_TRY(rc_slot(ctx, S_PART, (size_t)ny * nchunks * m * m * sizeof(double), &part));
-    dim3 grid((unsigned)nchunks, ny);
-    const size_t smem = (size_t)4 * G2_KT * (16 * R + 1) * sizeof(double);
-#define RC_G2(RR)                                                                                             \
-    do {                                                                                                      \
-        if (smem > 48 * 1024)                                                                                 \
-            RC_CU(ctx, cudaFuncSetAttribute(gram2_kernel<RR>, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
-                                            (int)smem));                                                      \
-        gram2_kernel<RR><<<grid, G2_THREADS, smem, ctx->stream>>>(n, (int)m, (int)m, X, ldx, Y0, ldy0,       \
-                                                                  Y1 ? Y1 : Y0, Y1 ? ldy1 : ldy0,            \
-                                                                  (double*)part, rows);                       \
-    } while (0)
-    if (R == 2) RC_G2(2);
-    else if (R == 3) RC_G2(3);
-    else if (R == 4) RC_G2(4);
-    else RC_G2(6);
-#undef RC_G2
+    // 16-byte copies need 16-byte aligned columns
+    const bool v16 = ((uintptr_t)X % 16 == 0) && ((uintptr_t)Y0 % 16 == 0) && (ldx % 2 == 0) && (ldy0 % 2 == 0) &&
+                     (!Y1 || (((uintptr_t)Y1 % 16 == 0) && (ldy1 % 2 == 0)));
+    const double* y1 = Y1 ? Y1 : Y0;
+    const int64_t l1 = Y1 ? ldy1 : ldy0;
+    double* pp = (double*)part;
+#define RC_GM(SBV, NYV)                                                                                           \
+    (v16 ? gram_mma_launch<SBV, NYV, true>(ctx, n, m, X, ldx, Y0, ldy0, y1, l1, pp, nchunks, rows)                \
+         : gram_mma_launch<SBV, NYV, false>(ctx, n, m, X, ldx, Y0, ldy0, y1, l1, pp, nchunks, rows))
+    rc_status st;
+    if (ny == 2) st = sb == 1 ? RC_GM(1, 2) : (sb == 2 ? RC_GM(2, 2) : RC_GM(3, 2));
+    else st = sb == 1 ? RC_GM(1, 1) : (sb == 2 ? RC_GM(2, 1) : RC_GM(3, 1));
+#undef RC_GM
+    RC_TRY(st);
     ctx->launches++;
     RC_CU(ctx, cudaGetLastError());
     const int64_t total = (int64_t)ny * m * m;
-    const unsigned g = (unsigned)std::min<int64_t>((total + 255) / 256, 4 * 148);
-    gram2_reduce_kernel<<<g, 256, 0, ctx->stream>>>((int)m, nchunks, ny, (const double*)part, C0, C1);
+    const unsigned gr = (unsigned)std::min<int64_t>((total + 255) / 256, 4 * 148);
+    gram2_reduce_kernel<<<gr, 256, 0, ctx->stream>>>((int)m, nchunks, ny, (const double*)part, C0, C1);
     ctx->launches++;
     RC_CU(ctx, cudaGetLastError());
     return RC_OK;
 }
 
 // ---------------------------------------------------------------------------------------
-// xt2: Y = X T with T (k x nc) resident in shared memory; persistent CTAs over 64-row tiles.
-// thread (tx, ty): rows tx + 16 i (i < 4), columns ty + 16 j (j < R).
+// xt2
 // ---------------------------------------------------------------------------------------
-constexpr int X2_THREADS = 256;
-constexpr int X2_RM = 4;
-constexpr int X2_BR = 16 * X2_RM;
+constexpr int XM_RT = 32;         // rows per tile
+constexpr int XM_RP = XM_RT + 4;  // doubles per column of a shared X/W tile (= 4 mod 16)
+constexpr int XM_CT = 6;          // 8-column mma tiles per warp (48 columns)
 
-template <int R, bool DUAL>
-__global__ void __launch_bounds__(X2_THREADS, 1)
-xt2_kernel(int64_t n, int k, int nc, const double* __restrict__ X, int64_t ldx, const double* __restrict__ Tm,
-           int64_t ldt, double* __restrict__ Y, int64_t ldy, const double* __restrict__ W, int64_t ldw,
-           const double* __restrict__ lam, int res_count, double* __restrict__ rpart) {
-    constexpr int TB = 16 * R;
-    constexpr int S = TB + 1;
-    extern __shared__ __align__(16) double x2s[];
-    double* Ts = x2s;                       // [k][S]
-    double* Xs = Ts + (size_t)k * S;        // [k][BR]
-    double* Ws = Xs + (size_t)k * X2_BR;    // [k][BR] (DUAL)
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    for (int e = tid; e < k * TB; e += X2_THREADS) {
-        const int kk = e % k, c = e / k;
-        Ts[kk * S + c] = c < nc ? Tm[kk + (int64_t)c * ldt] : 0.0;
+// Doubles per column of the shared T (>= k rounded up to 4, = 4 mod 16).
+__host__ __device__ inline int xm_kpt(int k) {
+    int k4 = (k + 3) / 4 * 4;
+    while (k4 % 16 != 4) k4 += 4;
+    return k4;
+}
+
+// Warps: 4 row slabs (8 rows each) x NH column halves (48 columns each).
+template <int NH, bool DUAL, bool V16>
+__global__ void __launch_bounds__(128 * NH, 1)
+xt_mma_kernel(int64_t n, int k, int nc, const double* __restrict__ X, int64_t ldx, const double* __restrict__ Tm,
+              int64_t ldt, double* __restrict__ Y, int64_t ldy, const double* __restrict__ W, int64_t ldw,
+              const double* __restrict__ lam, int dual_cols, int res_count, double* __restrict__ rpart,
+              float* __restrict__ R32, int64_t ldr) {
+    constexpr int NT = 128 * NH;
+    constexpr int OPS = DUAL ? 2 : 1;
+    const int kpt = xm_kpt(k);
+    const int k4 = (k + 3) / 4 * 4;
+    extern __shared__ __align__(16) double xms[];
+    double* Ts = xms;                                  // [NH*48][kpt]
+    double* tiles = Ts + (size_t)NH * 48 * kpt;        // [2][OPS][k4][XM_RP]
+    const int stage = OPS * k4 * XM_RP;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, q = lane & 3;
+    const int slab = warp & 3, half = warp >> 2;
+    const int cbase = half * 48;
+    for (int e = tid; e < NH * 48 * kpt; e += NT) {
+        const int c = e / kpt, kk = e - c * kpt;
+        Ts[e] = (c < nc && kk < k) ? Tm[kk + (int64_t)c * ldt] : 0.0;
     }
-    double lamc[R];
-    double rs[R];
-#pragma unroll
-    for (int j = 0; j < R; ++j) {
-        const int c = ty + 16 * j;
-        lamc[j] = (DUAL && c < res_count) ? lam[c] : 0.0;
-        rs[j] = 0.0;
+    // zero the padding columns k..k4 of every operand of both stages once
+    {
+        const int per = (k4 - k) * XM_RP;
+        for (int e = tid; e < 2 * OPS * per; e += NT) {
+            const int st = e / per, f = e - st * per;
+            tiles[st * k4 * XM_RP + k * XM_RP + f] = 0.0;
+        }
     }
-    const int64_t ntiles = (n + X2_BR - 1) / X2_BR;
-    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int64_t r0 = t * X2_BR;
-        __syncthreads();
-        for (int e = tid; e < k * X2_BR; e += X2_THREADS) {
-            const int rr = e % X2_BR, kk = e / X2_BR;
-            const int64_t r = r0 + rr;
-            Xs[kk * X2_BR + rr] = r < n ? __ldg(X + r + (int64_t)kk * ldx) : 0.0;
-            if (DUAL) Ws[kk * X2_BR + rr] = r < n ? __ldg(W + r + (int64_t)kk * ldw) : 0.0;
+    // mma tiles of this warp whose columns need W T (warp-uniform)
+    const int dtiles = DUAL ? max(0, min(XM_CT, (dual_cols - cbase + 7) / 8)) : 0;
+    double lamc[XM_CT][2], rs[XM_CT][2];
+#pragma unroll
+    for (int j = 0; j < XM_CT; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int c = cbase + j * 8 + 2 * q + h;
+            lamc[j][h] = (DUAL && c < dual_cols) ? lam[c] : 0.0;
+            rs[j][h] = 0.0;
         }
+    const int64_t ntiles = (n + XM_RT - 1) / XM_RT;
+    auto issue = [&](int64_t t, int b) {
+        double* st = tiles + b * stage;
+        const int64_t r0 = t * XM_RT;
+        load_cols_async<XM_RT, V16>(st, XM_RP, X, ldx, k, r0, n, tid, NT);
+        if (DUAL) load_cols_async<XM_RT, V16>(st + k4 * XM_RP, XM_RP, W, ldw, k, r0, n, tid, NT);
+    };
+    int buf = 0;
+    int64_t t = blockIdx.x;
+    if (t < ntiles) issue(t, 0);
+    cp_async_commit();
+    for (; t < ntiles; t += gridDim.x) {
+        const int64_t tn = t + gridDim.x;
+        if (tn < ntiles) issue(tn, buf ^ 1);
+        cp_async_commit();
+        cp_async_wait1();
         __syncthreads();
-        double acc[X2_RM][R], acc2[DUAL ? X2_RM : 1][DUAL ? R : 1];
+        const double* xs = tiles + buf * stage + slab * 8 + g + q * XM_RP;
+        const double* ws = xs + k4 * XM_RP;
+        const double* ts = Ts + (cbase + g) * kpt + q;
+        double acc[XM_CT][2], acc2[XM_CT][2];
 #pragma unroll
-        for (int i = 0; i < X2_RM; ++i)
+        for (int j = 0; j < XM_CT; ++j) acc[j][0] = acc[j][1] = acc2[j][0] = acc2[j][1] = 0.0;
+#pragma unroll 2
+        for (int k0 = 0; k0 < k4; k0 += 4) {
+            const double a = xs[k0 * XM_RP];
+            double b[XM_CT];
 #pragma unroll
-            for (int j = 0; j < R; ++j) {
-                acc[i][j] = 0.0;
-                if (DUAL) acc2[i % (DUAL ? X2_RM : 1)][j % (DUAL ? R : 1)] = 0.0;
+            for (int j = 0; j < XM_CT; ++j) b[j] = ts[j * 8 * kpt + k0];
+#pragma unroll
+            for (int j = 0; j < XM_CT; ++j) dmma(acc[j][0], acc[j][1], a, b[j]);
+            if (DUAL && dtiles > 0) {
+                const double w = ws[k0 * XM_RP];
+#pragma unroll
+                for (int j = 0; j < XM_CT; ++j)
+                    if (j < dtiles) dmma(acc2[j][0], acc2[j][1], w, b[j]);
             }
-#pragma unroll 4
-        for (int kk = 0; kk < k; ++kk) {
-            double a[X2_RM], w[X2_RM], b[R];
-#pragma unroll
-            for (int i = 0; i < X2_RM; ++i) {
-                a[i] = Xs[kk * X2_BR + tx + 16 * i];
-                if (DUAL) w[i] = Ws[kk * X2_BR + tx + 16 * i];
-            }
-#pragma unroll
-            for (int j = 0; j < R; ++j) b[j] = Ts[kk * S + ty + 16 * j];
-#pragma unroll
-            for (int i = 0; i < X2_RM; ++i)
-#pragma unroll
-                for (int j = 0; j < R; ++j) {
-                    acc[i][j] = fma(a[i], b[j], acc[i][j]);
-                    if (DUAL) acc2[i % (DUAL ? X2_RM : 1)][j % (DUAL ? R : 1)] =
-                        fma(w[i], b[j], acc2[i % (DUAL ? X2_RM : 1)][j % (DUAL ? R : 1)]);
-                }
         }
+        const int64_t r = t * XM_RT + slab * 8 + g;
+        if (r < n) {
 #pragma unroll
-        for (int i = 0; i < X2_RM; ++i) {
-            const int64_t r = r0 + tx + 16 * i;
-            if (r >= n) continue;
-#pragma unroll
-            for (int j = 0; j < R; ++j) {
-                const int c = ty + 16 * j;
-                if (c < nc) {
-                    Y[r + (int64_t)c * ldy] = acc[i][j];
-                    if (DUAL && c < res_count) {
-                        const double d = acc2[i % (DUAL ? X2_RM : 1)][j % (DUAL ? R : 1)] - lamc[j] * acc[i][j];
-                        rs[j] = fma(d, d, rs[j]);
+            for (int j = 0; j < XM_CT; ++j) {
+                const int c = cbase + j * 8 + 2 * q;
+                if (c < nc) Y[r + (int64_t)c * ldy] = acc[j][0];
+                if (c + 1 < nc) Y[r + (int64_t)(c + 1) * ldy] = acc[j][1];
+                if (DUAL && j < dtiles) {
+                    const double d0 = acc2[j][0] - lamc[j][0] * acc[j][0];
+                    const double d1 = acc2[j][1] - lamc[j][1] * acc[j][1];
+                    if (c < res_count) rs[j][0] = fma(d0, d0, rs[j][0]);
+                    if (c + 1 < res_count) rs[j][1] = fma(d1, d1, rs[j][1]);
+                    if (R32) {
+                        if (c + 1 < nc) {
+                            *reinterpret_cast<float2*>(R32 + r * ldr + c) = make_float2((float)d0, (float)d1);
+                        } else if (c < nc) {
+                            R32[r * ldr + c] = (float)d0;
+                        }
                     }
                 }
             }
         }
+        __syncthreads();
+        buf ^= 1;
     }
-    if (DUAL) {
+    if (DUAL && res_count > 0) {
+        // per column: sum over g (lanes with the same q), then over the four row slabs in order
+        double* red = tiles;  // [4][NH*48]; the tiles are no longer read
 #pragma unroll
-        for (int j = 0; j < R; ++j) {
-            double v = rs[j];
+        for (int j = 0; j < XM_CT; ++j)
 #pragma unroll
-            for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            const int c = ty + 16 * j;
-            if (tx == 0 && c < res_count) rpart[(size_t)blockIdx.x * res_count + c] = v;
+            for (int h = 0; h < 2; ++h) {
+                double v = rs[j][h];
+                v += __shfl_xor_sync(0xffffffffu, v, 4);
+                v += __shfl_xor_sync(0xffffffffu, v, 8);
+                v += __shfl_xor_sync(0xffffffffu, v, 16);
+                if (g == 0) red[slab * NH * 48 + cbase + j * 8 + 2 * q + h] = v;
+            }
+        __syncthreads();
+        for (int c = tid; c < res_count; c += NT) {
+            double v = 0.0;
+#pragma unroll
+            for (int sl = 0; sl < 4; ++sl) v += red[sl * NH * 48 + c];
+            rpart[(size_t)blockIdx.x * res_count + c] = v;
         }
     }
 }
@@ -271,43 +383,57 @@ bool xt2_supported(int dtype, int64_t k, int64_t nc) {
     return dtype == RC_REAL64 && k >= 1 && k <= 96 && nc >= 1 && nc <= 96;
 }
 
-// Y = X T; with W: residual norms ||(W T)_c - lam_c Y_c|| for c < res_count into res (device).
+template <int NH, bool DUAL, bool V16>
+static rc_status xt_mma_launch(rc_ctx* ctx, unsigned grid, int64_t n, int64_t k, int64_t nc, const double* X,
+                               int64_t ldx, const double* T, int64_t ldt, double* Y, int64_t ldy, const double* W,
+                               int64_t ldw, const double* lam, int64_t dual_cols, int64_t res_count, double* rpart,
+                               float* R32, int64_t ldr) {
+    const int k4 = (int)((k + 3) / 4 * 4);
+    const size_t smem =
+        ((size_t)NH * 48 * xm_kpt((int)k) + (size_t)2 * (DUAL ? 2 : 1) * k4 * XM_RP) * sizeof(double);
+    RC_CU(ctx, allow_max_smem(ctx, xt_mma_kernel<NH, DUAL, V16>));
+    xt_mma_kernel<NH, DUAL, V16><<<grid, 128 * NH, smem, ctx->stream>>>(
+        n, (int)k, (int)nc, X, ldx, T, ldt, Y, ldy, W, ldw, lam, (int)dual_cols, (int)res_count, rpart, R32, ldr);
+    return RC_OK;
+}
+
+// Y = X T; with W: residual norms ||(W T)_c - lam_c Y_c|| for c < res_count into res (device),
+// and with R32 the residual block (all nc columns) in row-major FP32 with leading dimension ldr.
 rc_status xt2(rc_ctx* ctx, int64_t n, int64_t k, int64_t nc, const double* X, int64_t ldx, const double* T,
               int64_t ldt, double* Y, int64_t ldy, const double* W, int64_t ldw, const double* lam, int64_t res_count,
-              double* res) {
-    const int R = nc <= 32 ? 2 : (nc <= 48 ? 3 : (nc <= 64 ? 4 : 6));
-    const bool dual = W != nullptr && res_count > 0;
-    const size_t smem = ((size_t)k * (16 * R + 1) + (size_t)k * X2_BR * (dual ? 2 : 1)) * sizeof(double);
-    const int64_t ntiles = (n + X2_BR - 1) / X2_BR;
-    const unsigned grid = (unsigned)std::min<int64_t>(ntiles, ctx->sm_count);
+              double* res, float* R32, int64_t ldr) {
+    const bool dual = W != nullptr && lam != nullptr && (res_count > 0 || R32 != nullptr);
+    if (!dual) {
+        res_count = 0;
+        R32 = nullptr;
+    }
+    const int64_t dual_cols = dual ? (R32 ? nc : std::min(res_count, nc)) : 0;
+    if (R32 && (ldr % 2 != 0 || (uintptr_t)R32 % 8 != 0))
+        return rc_fail(ctx, RC_ERR_INVALID, "xt2: the residual block needs an even leading dimension");
+    const int nh = nc <= 48 ? 1 : 2;
+    const int64_t ntiles = (n + XM_RT - 1) / XM_RT;
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ntiles, ctx->sm_count));
     double* rpart = nullptr;
-    if (dual) {
+    if (res_count > 0) {
         void* p = nullptr;
         RC_TRY(rc_slot(ctx, S_RPART, (size_t)grid * res_count * sizeof(double), &p));
         rpart = (double*)p;
     }
-#define RC_X2(RR, DD)                                                                                          \
-    do {                                                                                                       \
-        RC_CU(ctx, cudaFuncSetAttribute(xt2_kernel<RR, DD>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
-                                        (int)smem));                                                           \
-        xt2_kernel<RR, DD><<<grid, X2_THREADS, smem, ctx->stream>>>(n, (int)k, (int)nc, X, ldx, T, ldt, Y, ldy, \
-                                                                    W, ldw, lam, (int)res_count, rpart);       \
-    } while (0)
-    if (dual) {
-        if (R == 2) RC_X2(2, true);
-        else if (R == 3) RC_X2(3, true);
-        else if (R == 4) RC_X2(4, true);
-        else RC_X2(6, true);
-    } else {
-        if (R == 2) RC_X2(2, false);
-        else if (R == 3) RC_X2(3, false);
-        else if (R == 4) RC_X2(4, false);
-        else RC_X2(6, false);
-    }
-#undef RC_X2
+    const bool v16 =
+        ((uintptr_t)X % 16 == 0) && (ldx % 2 == 0) && (!dual || (((uintptr_t)W % 16 == 0) && ldw % 2 == 0));
+#define RC_XM(NHV, DV)                                                                                            \
+    (v16 ? xt_mma_launch<NHV, DV, true>(ctx, grid, n, k, nc, X, ldx, T, ldt, Y, ldy, W, ldw, lam, dual_cols,      \
+                                        res_count, rpart, R32, ldr)                                               \
+         : xt_mma_launch<NHV, DV, false>(ctx, grid, n, k, nc, X, ldx, T, ldt, Y, ldy, W, ldw, lam, dual_cols,     \
+                                         res_count, rpart, R32, ldr))
+    rc_status st;
+    if (dual) st = nh == 1 ? RC_XM(1, true) : RC_XM(2, true);
+    else st = nh == 1 ? RC_XM(1, false) : RC_XM(2, false);
+#undef RC_XM
+    RC_TRY(st);
     ctx->launches++;
     RC_CU(ctx, cudaGetLastError());
-    if (dual) {
+    if (res_count > 0) {
         resid2_reduce_kernel<<<(unsigned)res_count, 256, 0, ctx->stream>>>(grid, (int)res_count, rpart, res);
         ctx->launches++;
         RC_CU(ctx, cudaGetLastError());

@@ -58,7 +58,7 @@ struct rc_ctx {
 
 enum Slot {
     S_V = 0, S_W, S_T1, S_T2, S_FOUND, S_PART, S_SMALL, S_LANCZOS, S_RPART, S_IO, S_CB, S_EIG, S_FA, S_FB,
-    S_COUNT
+    S_R32, S_CORR, S_COUNT
 };
 
 struct rc_op {
@@ -101,6 +101,18 @@ rc_status rc_fail(rc_ctx* ctx, rc_status st, const std::string& msg);
         if (s_ != RC_OK) return s_;    \
     } while (0)
 
+// Allow `kernel` the device's largest dynamic shared memory. The attribute is process-wide state
+// of the function: every caller sets the same value, so concurrent solves (request-server
+// workers) never shrink it under one another's launches.
+template <class K>
+cudaError_t allow_max_smem(const rc_ctx* ctx, K kernel) {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(ctx->smem_optin - fa.sharedSizeBytes));
+}
+
 // Scratch slot of at least `bytes` (contents not preserved on growth).
 rc_status rc_slot(rc_ctx* ctx, int slot, size_t bytes, void** out);
 // Free every scratch slot (stream-ordered when the context has a memory pool).
@@ -136,6 +148,15 @@ rc_status filter_apply(rc_ctx* ctx, rc_op* op, void* V, int64_t ld, int64_t s, i
 // single-solve path (rc_serve.cu).
 rc_status serve_filter(rc_ctx* ctx, rc_op* op, void* V, int64_t ld, int64_t s, int64_t degree, double a, double b,
                        int prec, void* bufA, void* bufB, size_t buf_bytes, bool* handled);
+// Correction filter (rc_filter_rm.cu), the MIXED precision refinement: V (FP64 column-major,
+// leading dimension ldv) holds Ritz vectors with Ritz values lam_dev (device) and R (row-major
+// FP32, leading dimension rm_leading_dim(RC_REAL64, P32, s)) their residual block A V - V diag(lam);
+// V <- P_m(A')V with FP32 storage of the (small) deviation from the scalar recurrence. bufA and
+// bufB: two row-major FP32 blocks of the same size as R.
+bool rm_corr_supported(const rc_op* op, int64_t s);
+rc_status rm_filter_corr(rc_ctx* ctx, rc_op* op, double* V, int64_t ldv, int64_t s, int64_t degree, double a,
+                         double b, const double* lam_dev, const float* R, void* bufA, void* bufB);
+int64_t rm_leading_dim(int dtype, int prec, int64_t s);
 // Build the FP32 (c64) copy of an operator's values/diagonal used by the MIXED filter.
 rc_status ensure_fp32(rc_ctx* ctx, rc_op* op);
 // Degree-step timing (ctx->step_timing): record an event on the context stream; step_flush
@@ -162,18 +183,22 @@ struct XtArgs {
     void* Y2 = nullptr; int64_t ldy2 = 0;
     const double* lam = nullptr; int64_t res_count = 0;
     double* res = nullptr;  // device output, res_count residual norms
+    // optional: the residual block X2 T - Y diag(lam) (all nc columns) in row-major FP32 with
+    // leading dimension ldr (real blocks with k, nc <= 96 only)
+    float* R32 = nullptr; int64_t ldr = 0;
 };
 rc_status xt(rc_ctx* ctx, int dtype, const XtArgs& a);
 
 // FP64 real fast paths (s <= 96), rc_gemm.cu. gram2: C0 = X^T Y0 (and C1 = X^T Y1 when Y1),
-// symmetric results. xt2: Y = X T, plus residual norms of W T against lam when W is given.
+// symmetric results. xt2: Y = X T, plus residual norms of W T against lam when W is given, and
+// the residual block W T - Y diag(lam) in row-major FP32 when R32 is given.
 bool gram2_supported(int dtype, int64_t m);
 rc_status gram2(rc_ctx* ctx, int64_t n, int64_t m, const double* X, int64_t ldx, const double* Y0, int64_t ldy0,
                 double* C0, const double* Y1, int64_t ldy1, double* C1);
 bool xt2_supported(int dtype, int64_t k, int64_t nc);
 rc_status xt2(rc_ctx* ctx, int64_t n, int64_t k, int64_t nc, const double* X, int64_t ldx, const double* T,
               int64_t ldt, double* Y, int64_t ldy, const double* W, int64_t ldw, const double* lam, int64_t res_count,
-              double* res);
+              double* res, float* R32 = nullptr, int64_t ldr = 0);
 
 // Cholesky factor of Gram G (s x s) with diagonal scaling, shift on breakdown;
 // writes Tout = D^-1 R^-1 (upper). flags (device int[4]): [0] shifted, [1] failed, [2] zero column.

@@ -64,10 +64,14 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
 
 // The rows of virtual CTA `cta` (the kernel below passes blockIdx.x; the batched kernel of
 // rc_batch.cu passes its own CTA numbering), so one arithmetic serves both launch forms.
-template <class Pol, class TS, class TC, int W, class IX>
+// SRC (the correction filter): y also gets sig[c] * src(i, c), where src is a row-major block
+// with the same leading dimension and sig holds one coefficient per column (ld entries).
+template <class Pol, class TS, class TC, int W, class IX, bool SRC = false>
 __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg, int64_t ld, int groups, int64_t cta,
                                              const TS* __restrict__ x, const TS* z, TS* y, TC alpha, TC beta,
-                                             TC gamma, int64_t pf_z, int64_t pf_x) {
+                                             TC gamma, int64_t pf_z, int64_t pf_x,
+                                             const TS* __restrict__ src = nullptr,
+                                             const float* __restrict__ sig = nullptr) {
     constexpr int V = Pack16<TS>::V;
     const int rows_per_iter = blockDim.x / nseg;
     const int rloc = threadIdx.x / nseg;
@@ -76,6 +80,13 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
     const IX wstride = (IX)nseg * (IX)V;
     const IX ldx = (IX)ld;
     const int64_t stride = rows_per_iter;
+    TC sg[SRC ? W * V : 1];
+    if (SRC) {
+#pragma unroll
+        for (int w = 0; w < W; ++w)
+#pragma unroll
+            for (int v = 0; v < V; ++v) sg[w * V + v] = s_from<TC>((double)__ldg(sig + off + w * wstride + v), 0.0);
+    }
     int64_t i = cta * groups * rows_per_iter + rloc;
     const int64_t i_end = min(n, (cta + 1) * groups * rows_per_iter);
     typename Pol::Pre p0, p1;
@@ -94,6 +105,7 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
             for (int w = 0; w < W; ++w) {
                 if ((((off + w * wstride) * (IX)sizeof(TS)) & 127) != 0) continue;  // one per 128-byte line
                 if (z && i + pf_z < n) prefetch_l2(z + (IX)(i + pf_z) * ldx + off + w * wstride);
+                if (SRC && i + pf_z < n) prefetch_l2(src + (IX)(i + pf_z) * ldx + off + w * wstride);
                 if (i + pf_x < n) prefetch_l2(x + (IX)(i + pf_x) * ldx + off + w * wstride);
             }
         }
@@ -114,7 +126,18 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
             const IX o = oi + w * wstride;
             const Pack16<TS> xi = ld16_ro(x + o);
             Pack16<TS> out;
-            if (z) {
+            if (SRC) {
+                const Pack16<TS> si = ld16_ro(src + o);
+                const Pack16<TS> zi = z ? ld16(z + o) : Pack16<TS>{};
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    TC r = s_mul(alpha, acc[w * V + v]);
+                    r = s_fma(beta, s_cvt<TC>(xi.v[v]), r);
+                    if (z) r = s_fma(gamma, s_cvt<TC>(zi.v[v]), r);
+                    r = s_fma(sg[w * V + v], s_cvt<TC>(si.v[v]), r);
+                    out.v[v] = s_cvt<TS>(r);
+                }
+            } else if (z) {
                 const Pack16<TS> zi = ld16(z + o);
 #pragma unroll
                 for (int v = 0; v < V; ++v) {
@@ -176,6 +199,29 @@ __device__ __forceinline__ void to_cm_tile(int64_t n, int64_t s, const TS* __res
     for (int j = 0; j < 4; ++j) {
         const int64_t c = c0 + ty + 8 * j, r = r0 + tx;
         if (r < n && c < s) Vc[r + c * ldv] = s_rscale((real_t<TV>)scale, s_cvt<TV>(tile[tx][ty + 8 * j]));
+    }
+}
+
+// Last step of the correction filter: V[i + c*ldv] = coef[c] * V[i + c*ldv] + beta * E[i*ld + c]
+// (x_m = c_m(lambda_c) v_c + a e_m, scaled by 1/(m+1)); one 32x32 tile, threads 32 x 8.
+template <class TS>
+__device__ __forceinline__ void corr_to_cm_tile(int64_t n, int64_t s, const TS* __restrict__ E, int64_t ld,
+                                                double* __restrict__ Vc, int64_t ldv, const double* __restrict__ coef,
+                                                double beta, int64_t r0, int64_t c0, TS (&tile)[32][33]) {
+    const int tx = threadIdx.x, ty = threadIdx.y;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int64_t r = r0 + ty + 8 * j, c = c0 + tx;
+        tile[ty + 8 * j][tx] = (r < n && c < s) ? E[r * ld + c] : s_zero(TS());
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int64_t c = c0 + ty + 8 * j, r = r0 + tx;
+        if (r < n && c < s) {
+            double* vp = Vc + r + c * ldv;
+            *vp = fma(coef[c], *vp, beta * (double)tile[tx][ty + 8 * j]);
+        }
     }
 }
 

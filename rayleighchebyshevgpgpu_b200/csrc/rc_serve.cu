@@ -148,11 +148,17 @@ int64_t solve_footprint(const rc_op* op, const rc_solve_params& p, int sm_count)
         if (rm > n * ss * esz) t += 2 * round_2m(rm);
     }
     t += round_2m(8 * sq * sq * esz + sq * 16 + 512);                 // small Rayleigh-Ritz matrices
-    t += round_2m((4 * (int64_t)sm_count + 2) * sq * sq * esz);       // Gram partial sums
+    t += round_2m((8 * (int64_t)sm_count + 2) * sq * sq * esz);       // Gram partial sums
     t += round_2m(((n + 63) / 64) * sq * 8);                         // residual partial sums
     t += round_2m(3 * n * esz + sq * sq * esz + 4096);                // Lanczos vectors / small QR
     t += round_2m(4 * sq * sq * esz + 1024) + round_2m(2 * (sq + 1) * (sq + 1) * esz + 4096);  // cholqr, Jacobi
     if (op->kind == 2) t += round_2m(n * ss * esz);                   // callback step scratch
+    if (p.precision == RC_PREC_MIXED && p.mixed_refine == 0 && rcb::rm_corr_supported(op, ss)) {
+        // correction filter: the FP32 residual block and the coefficient table
+        const int64_t ld32 = rcb::rm_leading_dim(op->dtype, P32, ss);
+        const int64_t dmax = p.poly_degree_max > 0 ? p.poly_degree_max : 200;
+        t += round_2m(n * ld32 * 4) + round_2m((dmax + 1) * ld32 * 4 + ld32 * 8 + 512);
+    }
     return t;
 }
 

@@ -16,7 +16,9 @@
 //   * after an outer pass only the stale tail columns are refreshed (the CPU LM refreshes the
 //     buffer range, RayleighChebyshevLM.h:1086-1092; the GPU reference the whole block, :1176-1179);
 //   * MIXED precision: the filter runs in FP32/c64 until the residuals reach mixed_switch_tol
-//     or stall, then in FP64 until the stop test passes; it never stops in the FP32 phase.
+//     or stall (it never stops in this phase), then as the FP32 correction filter on the residual
+//     block of the Ritz vectors (rc_filter_rm.cu), which converges like the FP64 filter; FP64
+//     filter when the correction filter is unsupported, switched off, or stalls.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -58,8 +60,9 @@ private:
     rc_status randomize_cols(void* X, int64_t c0, int64_t c1);
     rc_status deflate(void* X, int64_t s);
     rc_status ortho(int64_t s);
-    rc_status rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool read_back);
-    rc_status rr_fused(int64_t s, int64_t res_count, bool* ok);
+    rc_status rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool read_back, float* R32 = nullptr);
+    rc_status rr_fused(int64_t s, int64_t res_count, bool* ok, float* R32 = nullptr);
+    rc_status r32_block(int64_t s, float** out);
     rc_status lanczos(int which, double tol, double* lmin, double* lmax);
     void tic(int ph);
     void toc(int ph);
@@ -84,6 +87,10 @@ private:
     int64_t fused_ok_ = 0, fused_fallback_ = 0;
     double* hbuf_ = nullptr;
     int64_t ss_cap_ = 0;
+    // MIXED correction filter: the residual block of the current Ritz vectors (row-major FP32),
+    // valid while haveR_ (written by the last Rayleigh-Ritz step, consumed by the next filter)
+    bool haveR_ = false;
+    int64_t corr_iters_ = 0, corr_steps_ = 0;
 
     std::vector<double> eigValues_, eigVecResiduals_, VtAVeigValue_, subspaceResiduals_;
     int64_t foundSize_ = 0;
@@ -213,7 +220,14 @@ rc_status Solver::ortho(int64_t s) {
 
 // Rayleigh-Ritz on orthonormal X (n x s): AX = A X, H = X^H AX, H = Q L Q^H,
 // X <- X Q, AX <- AX Q, residuals of the first res_count columns; results read to the host.
-rc_status Solver::rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool read_back) {
+rc_status Solver::r32_block(int64_t s, float** out) {
+    void* p = nullptr;
+    RC_TRY(rc_slot(ctx_, S_R32, (size_t)n_ * rm_leading_dim(RC_REAL64, P32, s) * sizeof(float), &p));
+    *out = (float*)p;
+    return RC_OK;
+}
+
+rc_status Solver::rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool read_back, float* R32) {
     StepArgs st;
     st.s = s;
     st.x = X; st.xp = P64; st.ldx = n_;
@@ -230,6 +244,10 @@ rc_status Solver::rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool rea
     a.X2 = AX; a.ldx2 = n_;
     a.Y2 = nullptr;  // only the residual norms of (A X) Q are needed
     a.lam = dlam_; a.res_count = res_count; a.res = dres_;
+    if (R32) {
+        a.R32 = R32;
+        a.ldr = rm_leading_dim(RC_REAL64, P32, s);
+    }
     RC_TRY(xt(ctx_, dtype_, a));
     std::swap(X, T1_);
     if (read_back) {
@@ -252,7 +270,7 @@ rc_status Solver::rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool rea
 // problem. Accepted only when the scaled Gram matrix is well conditioned (smallest Cholesky pivot
 // >= 1e-3, no shift needed); otherwise *ok = false, V_ still holds V_f and the caller
 // orthonormalises and repeats the Rayleigh-Ritz step.
-rc_status Solver::rr_fused(int64_t s, int64_t res_count, bool* ok) {
+rc_status Solver::rr_fused(int64_t s, int64_t res_count, bool* ok, float* R32) {
     StepArgs st;
     st.s = s;
     st.x = V_; st.xp = P64; st.ldx = n_;
@@ -281,6 +299,10 @@ rc_status Solver::rr_fused(int64_t s, int64_t res_count, bool* ok) {
     a.X2 = W_; a.ldx2 = n_;
     a.Y2 = nullptr;  // only the residual norms of W Q are needed
     a.lam = dlam_; a.res_count = res_count; a.res = dres_;
+    if (R32) {
+        a.R32 = R32;
+        a.ldr = rm_leading_dim(RC_REAL64, P32, s);
+    }
     RC_TRY(xt(ctx_, dtype_, a));
     RC_CU(ctx_, cudaMemcpyAsync(hbuf_, dlam_, s * sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
     if (res_count > 0)
@@ -377,6 +399,8 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
     const int stopCondition = (P_.stop_condition == RC_STOP_DEFAULT) ? RC_STOP_COMBINATION : P_.stop_condition;
     const bool mixed = P_.precision == RC_PREC_MIXED && op_->kind != 2;
     const double switchTol = P_.mixed_switch_tol > 0 ? P_.mixed_switch_tol : 1e-6;
+    // MIXED phases: 0 plain FP32 filter, 1 FP32 correction filter, 2 FP64 filter
+    enum { PH_PLAIN32 = 0, PH_CORR32 = 1, PH_FP64 = 2 };
 
     bool completedBasisFlag = false;
     int exitFlag = 0;
@@ -390,6 +414,8 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
         ++outer_passes_;
         for (int64_t k = bufferSize; k < subspaceSize; ++k) oldEigs[k] = oldEigs[bufferSize];  // :1169-1172
         if (applyCountCumulative > 0) RC_TRY(randomize_cols(V_, subspaceSize - lastFoundCount, subspaceSize));
+        haveR_ = false;
+        const bool corrOk = mixed && P_.mixed_refine == 0 && rm_corr_supported(op_, subspaceSize);
 
         tic(PH_ORTHO);
         RC_TRY(ortho(subspaceSize));  // the reference orthogonalizes twice here (:1195-1196)
@@ -408,9 +434,10 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
         int64_t oscillationCount = 0;
         int64_t residualCheckCount = 0;
         // mixed-precision phase state
-        bool fp32Phase = mixed;
+        int phase = mixed ? PH_PLAIN32 : PH_FP64;
         double bestFp32Residual = 1e300;
         int stallCount = 0;
+        size_t corrStart = 0;  // residualHistory index where the correction phase began
 
         while ((stopCheckValue > subspaceTol) && (innerLoopCount < maxInnerLoopCount)) {
             if (ctx_->cancel && ctx_->cancel->load(std::memory_order_relaxed))
@@ -440,18 +467,49 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
             // ---- filter (:1305-1319)
             double fa = 0.0, fb = 0.0;
             cpoly_.coefficients(starDegree, starBound, shift, fa, fb);
-            const int prec = fp32Phase ? RC_PREC_MIXED : RC_PREC_FP64;
+            const int prec = phase == PH_FP64 ? RC_PREC_FP64 : RC_PREC_MIXED;
             tic(PH_FILTER);
             if (!completedBasisFlag) {
                 int64_t steps = 0;
-                // filter_apply takes (g1, g2) with a = g2*g1, b = g2
-                RC_TRY(filter_apply(ctx_, op_, V_, n_, subspaceSize, starDegree, filterRepetitionCount, fa, fb,
-                                    prec, T1_, T2_, (size_t)n_ * subspaceSize * esz_, &steps));
+                if (phase == PH_CORR32 && haveR_) {
+                    // the correction filter: V_ holds the Ritz vectors, dlam_ their values and the
+                    // R32 slot their residual block; its two FP32 work blocks fit in T1_
+                    float* R32 = nullptr;
+                    RC_TRY(r32_block(subspaceSize, &R32));
+                    const size_t rmb = (size_t)n_ * rm_leading_dim(RC_REAL64, P32, subspaceSize) * sizeof(float);
+                    const size_t blk = (size_t)n_ * subspaceSize * esz_;
+                    void* bufA = T1_;
+                    void* bufB = (char*)T1_ + ((rmb + 255) / 256) * 256;
+                    if (((rmb + 255) / 256) * 256 + rmb > blk) bufB = T2_;
+                    if (rmb > blk) {  // narrow blocks: the row padding makes an FP32 block larger
+                        RC_TRY(rc_slot(ctx_, S_FA, rmb, &bufA));
+                        RC_TRY(rc_slot(ctx_, S_FB, rmb, &bufB));
+                    }
+                    for (int64_t r = 0; r < filterRepetitionCount; ++r) {
+                        if (r > 0) {  // a repeated application has no residual block: plain FP32
+                            int64_t st2 = 0;
+                            RC_TRY(filter_apply(ctx_, op_, V_, n_, subspaceSize, starDegree, 1, fa, fb,
+                                                RC_PREC_MIXED, T1_, T2_, (size_t)n_ * subspaceSize * esz_, &st2));
+                            steps += st2;
+                            continue;
+                        }
+                        RC_TRY(rm_filter_corr(ctx_, op_, (double*)V_, n_, subspaceSize, starDegree, fa, fb, dlam_,
+                                              R32, bufA, bufB));
+                        steps += starDegree;
+                        corr_steps_ += starDegree;
+                    }
+                    ++corr_iters_;
+                } else {
+                    // filter_apply takes (g1, g2) with a = g2*g1, b = g2
+                    RC_TRY(filter_apply(ctx_, op_, V_, n_, subspaceSize, starDegree, filterRepetitionCount, fa,
+                                        fb, prec, T1_, T2_, (size_t)n_ * subspaceSize * esz_, &steps));
+                }
                 degree_steps_ += steps;
-                if (!fp32Phase) fp64_steps_ += steps;
+                if (phase == PH_FP64) fp64_steps_ += steps;
             }
+            haveR_ = false;
             toc(PH_FILTER);
-            if (fp32Phase) ++mixed_iters_;
+            if (phase != PH_FP64) ++mixed_iters_;
             applyCount += 1;
             count_opapply_ += starDegree * subspaceSize;
 
@@ -460,10 +518,16 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
             if (foundSize_ + subspaceSize < vectorDimension) residualCheckCount = subspaceIncrementSize;
             else residualCheckCount = subspaceSize;
             bool fused = false;
+            // the residual block for the next correction filter, once the residuals approach the
+            // switch tolerance
+            float* R32 = nullptr;
+            const double prevResidual = residualHistory.empty() ? 1e300 : residualHistory.back();
+            if (corrOk && phase != PH_FP64 && (phase == PH_CORR32 || prevResidual < 1e3 * switchTol))
+                RC_TRY(r32_block(subspaceSize, &R32));
             if (P_.orth_mode == 0) {
                 tic(PH_EIG);
                 RC_TRY(deflate(V_, subspaceSize));
-                RC_TRY(rr_fused(subspaceSize, residualCheckCount, &fused));
+                RC_TRY(rr_fused(subspaceSize, residualCheckCount, &fused, R32));
                 toc(PH_EIG);
             }
             if (!fused) {
@@ -471,9 +535,10 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
                 RC_TRY(ortho(subspaceSize));
                 toc(PH_ORTHO);
                 tic(PH_EIG);
-                RC_TRY(rr(V_, W_, subspaceSize, residualCheckCount, true));
+                RC_TRY(rr(V_, W_, subspaceSize, residualCheckCount, true, R32));
                 toc(PH_EIG);
             }
+            haveR_ = R32 != nullptr;
             flush();
             count_ortho_ += 1;
             count_opapply_ += subspaceSize + residualCheckCount;
@@ -523,7 +588,7 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
                 printf("%-5ld : Degree %-3ld  Residual Max: %-10.5g  Eig Diff Max: %-10.5g  Eig Conv Factor: %-10.5g "
                        "Max Gap %-10.5g %s\n",
                        (long)innerLoopCount, (long)starDegree, maxResidual, maxEigDiff, eigDiffRatio, maxGap,
-                       fp32Phase ? "[fp32 filter]" : "");
+                       phase == PH_PLAIN32 ? "[fp32 filter]" : (phase == PH_CORR32 ? "[fp32 correction]" : ""));
 
             // ---- stop test (:1520-1545)
             if (stopCondition == RC_STOP_RESIDUAL_ONLY) {
@@ -536,7 +601,8 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
             }
             if (subspaceIncrementSize == 0) stopCheckValue = 0.0;
             // oscillation stop for RESIDUAL_ONLY (:1551-1592)
-            if ((stopCondition == RC_STOP_RESIDUAL_ONLY) && (maxResidual < std::sqrt(subspaceTol)) && !fp32Phase) {
+            if ((stopCondition == RC_STOP_RESIDUAL_ONLY) && (maxResidual < std::sqrt(subspaceTol)) &&
+                phase != PH_PLAIN32) {
                 const int64_t rIndex = (int64_t)residualHistory.size() - 1;
                 if (rIndex > 3) {
                     const double a = (residualHistory[rIndex - 3] - 2.0 * residualHistory[rIndex - 2] +
@@ -549,9 +615,11 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
                     }
                 }
             }
-            // ---- mixed precision: leave the FP32 phase once the residual has reached the switch
-            // tolerance, has stalled, or the stop test would pass (never stop in FP32).
-            if (fp32Phase) {
+            // ---- mixed precision: leave the plain FP32 phase once the residual has reached the
+            // switch tolerance, has stalled, or the stop test would pass (never stop there); leave
+            // the correction phase for FP64 when it stops converging (no 0.7x reduction over eight
+            // iterations).
+            if (phase == PH_PLAIN32) {
                 bool sw = maxResidual <= switchTol || stopCheckValue <= subspaceTol;
                 if (maxResidual < 0.5 * bestFp32Residual) {
                     bestFp32Residual = maxResidual;
@@ -560,9 +628,13 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
                     sw = true;  // FP32 rounding floor reached
                 }
                 if (sw) {
-                    fp32Phase = false;
+                    phase = corrOk ? PH_CORR32 : PH_FP64;
+                    corrStart = residualHistory.size();
                     if (stopCheckValue <= subspaceTol) stopCheckValue = subspaceTol + 1.0;
                 }
+            } else if (phase == PH_CORR32) {
+                const size_t h = residualHistory.size();
+                if (h >= corrStart + 9 && maxResidual > 0.7 * residualHistory[h - 9]) phase = PH_FP64;
             }
             // ---- update the filter interval (:1602-1605)
             lambdaStar = VtAVeigValue_[subspaceSize - 1];
@@ -603,6 +675,7 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
                 printf("\nFound Count: %3ld Largest Eig Found: %-20.15g Lambda Bound: %-20.15g \n", (long)foundSize_,
                        eigValues_[foundSize_ - 1], lambdaMax);
         }
+        haveR_ = false;
         // shuffle the unconverged vectors to the head of the block (:1707-1716)
         if (!exitFlag && foundCount > 0) {
             RC_TRY(copy_cols(ctx_, dtype_, (char*)V_ + (size_t)foundCount * n_ * esz_, n_, T1_, n_, n_,
@@ -795,6 +868,8 @@ rc_status Solver::run(const void* v0, double* evals_out, void* evecs_out, double
         r.fused_rr = fused_ok_ + fused_fallback_;
         r.fused_rr_fallbacks = fused_fallback_;
         r.time_filter_steps_ms = ctx_->step_ms - step_ms0_;
+        r.correction_iterations = corr_iters_;
+        r.correction_degree_steps = corr_steps_;
         std::memcpy(info, &r, std::min(sz, sizeof(r)));
     }
     return RC_OK;

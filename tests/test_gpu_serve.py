@@ -31,6 +31,14 @@ def _mix():
     return reqs
 
 
+def _done(h, timeout_ms):
+    """Wait for a request; a request that did not finish raises with its own status and message."""
+    st = h.wait(timeout_ms)
+    if st != "done":
+        h.result()
+    assert st == "done", st
+
+
 def _params(P, prec, seed):
     p = R.make_params(P.k, P.tol, precision=prec, stop="RESIDUAL_ONLY")
     p.seed = seed
@@ -53,7 +61,7 @@ def test_served_results_equal_alone_in_mix_and_solo(ctx):
         alone = []
         for i, ((P, prec, _), op) in enumerate(zip(reqs, ops)):
             rq = srv.submit(op, _params(P, prec, 7 + i), v0=_start(P))
-            assert rq.wait(120000) == "done"
+            _done(rq, 120000)
             alone.append(rq.result())
         st_alone = srv.stats()
     # served in the mix: everything submitted at once
@@ -62,7 +70,7 @@ def test_served_results_equal_alone_in_mix_and_solo(ctx):
                    for i, ((P, prec, _), op) in enumerate(zip(reqs, ops))]
         mixed = []
         for h in handles:
-            assert h.wait(120000) == "done"
+            _done(h, 120000)
             mixed.append(h.result())
         st_mix = srv.stats()
     assert st_alone["max_jobs_in_batch"] == 1
@@ -115,13 +123,13 @@ def test_admission_keeps_footprint_under_budget(ctx):
     # budget: room for about two of these solves at once (each ~ 64000 * (4*24 + 16) * 8 B + slack)
     with R.Server(0, max_active=6) as probe:
         one = probe.submit(ops[0], _params(Ps[0], "mixed", 1))
-        assert one.wait(120000) == "done"
+        _done(one, 120000)
         need = one.info()["reserved_bytes"]
     budget = int(2.5 * (need + Ps[0].n * 8 * 2))
     with R.Server(0, max_active=6, budget_bytes=budget) as srv:
         hs = [srv.submit(op, _params(P, "mixed", 11 + i)) for i, (P, op) in enumerate(zip(Ps, ops))]
         for h in hs:
-            assert h.wait(180000) == "done"
+            _done(h, 180000)
         st = srv.stats()
         assert st["completed"] == 6
         assert st["bytes_peak"] <= budget
@@ -165,7 +173,7 @@ def test_cancel_queued_and_running(ctx):
         assert st["cancelled"] >= 1
         # the server keeps serving after cancellations
         again = srv.submit(ops, _params(small, "mixed", 2))
-        assert again.wait(120000) == "done"
+        _done(again, 120000)
         assert again.result().info["found"] == small.k
     opb.close()
     ops.close()
@@ -195,7 +203,7 @@ def test_callback_operator_is_served_unbatched(ctx):
     op = R.CallbackOperator(ctx, P.n, apply)
     with R.Server(0, max_active=2) as srv:
         h = srv.submit(op, _params(P, "fp64", 4), v0=_start(P))
-        assert h.wait(120000) == "done"
+        _done(h, 120000)
         res = h.result()
         st = srv.stats()
     assert calls["n"] > 10 and st["batched_jobs"] == 0

@@ -65,6 +65,35 @@ def test_complex_tight_binding_vs_lapack(ctx, precision):
         _check_pairs(A, res, 16, 1e-9, rtol=1e-9)
 
 
+@pytest.mark.parametrize("kind,dims,k", [(5, (80, 72), 32), (7, (18, 17, 16), 16), (27, (16, 15, 14), 16)])
+def test_mixed_correction_filter_matches_fp64(ctx, kind, dims, k):
+    """MIXED precision past the switch tolerance runs the FP32 correction filter (the recurrence on
+    the residual block of the Ritz vectors): it reaches tol 1e-10 with no FP64 degree step and the
+    FP64 path's eigenvalues; mixed_refine = 1 keeps the FP64 refinement filter."""
+    n = int(np.prod(dims))
+    diag = (4.0 if kind == 5 else (6.0 if kind == 7 else 1.0)) + np.random.default_rng(kind).uniform(0, 3, n)
+    Q = problems.Problem(f"corr{kind}", dims, kind, diag, -1.0 / 26.0 if kind == 27 else -1.0, k=k)
+    A = O.csr_matrix(*Q.csr())
+    dense = O.dense_lowest(A, k)
+    incr, buf = problems.block_sizes(k)
+    start = Q.start_block(incr + buf)
+    for form in ("csr", "stencil"):
+        op = R.operator_from_problem(ctx, Q, form)
+        f64 = _solve(ctx, op, Q, k, 1e-10, "fp64", start=start)
+        mix = _solve(ctx, op, Q, k, 1e-10, "mixed", start=start)
+        old = _solve(ctx, op, Q, k, 1e-10, "mixed", start=start, mixed_refine=1)
+        assert mix.info["correction_iterations"] > 0, mix.info
+        assert mix.info["fp64_degree_steps"] == 0, mix.info
+        assert mix.info["correction_degree_steps"] > 0
+        assert old.info["correction_iterations"] == 0 and old.info["fp64_degree_steps"] > 0
+        np.testing.assert_allclose(mix.evals, f64.evals, rtol=1e-10)
+        np.testing.assert_allclose(mix.evals, dense, rtol=1e-10, atol=1e-13)
+        X = mix.evecs.T
+        r = np.linalg.norm(A @ X - X * mix.evals, axis=0) / np.maximum(np.abs(mix.evals), 0.1)
+        assert r.max() <= 1.5e-10, r.max()
+        op.close()
+
+
 def test_multipass_deflation_incr_smaller_than_k(ctx):
     Q = problems.small_laplacian((24, 24), seed=5)
     A = O.csr_matrix(*Q.csr())
