@@ -275,9 +275,13 @@ def run_ours(args):
     # ---- accuracy: mixed vs FP64 (eigenvalues and largest subspace angle) ----
     eig_err = float(np.max(np.abs(res_mixed.evals - res64.evals) / np.abs(res64.evals))) if res64 else None
     with torch.no_grad():
-        M = mixed_vecs @ fp64_vecs.T  # k x k (rows are eigenvectors)
-        sv = torch.linalg.svdvals(M)
-        angle = float(torch.arccos(torch.clamp(sv.min(), -1.0, 1.0)).item())
+        # largest principal angle between the two k-dimensional eigenspaces: sin(theta_max) is the
+        # largest singular value of the part of the mixed basis outside the FP64 span (rows are
+        # orthonormal eigenvectors); this avoids the cancellation of arccos(sigma_min) near 1
+        D = mixed_vecs - (mixed_vecs @ fp64_vecs.T) @ fp64_vecs
+        sin_max = float(torch.sqrt(torch.clamp(torch.linalg.eigvalsh(D @ D.T).max(), min=0.0)).item())
+        angle = float(np.arcsin(min(1.0, sin_max)))
+        del D
     max_res_rel = float(np.max(res_mixed.residuals / np.maximum(np.abs(res_mixed.evals), 0.1)))
 
     # ---- end to end through the C ABI with host buffers (pinned), copies inside the timed region ----

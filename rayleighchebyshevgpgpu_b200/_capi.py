@@ -200,11 +200,12 @@ def lib() -> C.CDLL:
     """Load librcb200.so (raises if it has not been built)."""
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
+        path = os.environ.get("RCB200_LIB", LIB_PATH)  # an alternative build of the same library
+        if not os.path.exists(path):
             raise RuntimeError(
-                f"{LIB_PATH} is missing: build it with `python -m rayleighchebyshevgpgpu_b200.build`; "
+                f"{path} is missing: build it with `python -m rayleighchebyshevgpgpu_b200.build`; "
                 "this package has no CPU fallback")
-        L = C.CDLL(LIB_PATH)
+        L = C.CDLL(path)
         for name, (res, args) in SIGNATURES.items():
             f = getattr(L, name)
             f.restype = res

@@ -22,9 +22,8 @@
 
 namespace rcb {
 
-// Grids of the batched kernels: the step kernels' resident CTAs per SM (8 for FP32 storage, 6
-// for FP64, as the single-solve kernels) and the transposes'.
-constexpr int kBatchStepBlocksPerSm = 8;
+// Grids of the batched kernels: the step kernels' resident CTAs per SM (rm_min_blocks, as the
+// single-solve kernels) and the transposes'.
 constexpr int kBatchTileBlocksPerSm = 8;
 
 template <class TS, class TC, class Pol, int W>
@@ -234,7 +233,7 @@ BatchCounters batch_runner_counters(const BatchRunner* R) { return R->counters; 
 
 // The batch's launches on R->stream, reading table `tab` (device).
 static cudaError_t issue(BatchRunner* R, int slot, int64_t depth, bool has32, bool has64, int64_t* launches) {
-    const unsigned gs = (unsigned)(R->sm_count * kBatchStepBlocksPerSm);
+    const unsigned gs = (unsigned)(R->sm_count * rm_min_blocks<float>());
     const unsigned gt = (unsigned)(R->sm_count * kBatchTileBlocksPerSm);
     const dim3 tblk(32, 8);
     cudaError_t e = cudaMemcpyAsync(R->dev[slot], R->host[slot], sizeof(BatchTable), cudaMemcpyHostToDevice, R->stream);

@@ -321,9 +321,13 @@ chol_factor_kernel(int s, int64_t nrows, const T* __restrict__ G, T* Mg, T* Tout
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_bad;
     __shared__ double s_piv, s_minpiv;
+    // In shared memory the matrices have an odd leading dimension (s + 1), so that a warp reading
+    // along a row (consecutive columns) hits distinct banks.
+    const int lm = mode >= 1 ? s + 1 : s;
+    const int lx = mode == 2 ? s + 1 : s;
     T* M = mode >= 1 ? (T*)smem_raw : Mg;
-    T* X = mode == 2 ? M + (size_t)s * s : Tout;
-    double* dsc = mode == 2 ? (double*)(X + (size_t)s * s) : (mode == 1 ? (double*)(M + (size_t)s * s) : dscg);
+    T* X = mode == 2 ? M + (size_t)s * lm : Tout;
+    double* dsc = mode == 2 ? (double*)(X + (size_t)s * lx) : (mode == 1 ? (double*)(M + (size_t)s * lm) : dscg);
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int i = tid; i < s; i += nt) {
         const double gi = s_real(G[i + (int64_t)i * s]);
@@ -348,13 +352,13 @@ chol_factor_kernel(int s, int64_t nrows, const T* __restrict__ G, T* Mg, T* Tout
             if (!isfinite(s_real(g)) || !isfinite(s_imag(g))) g = s_zero(T());
             g = s_rscale(1.0 / (dsc[i] * dsc[j]), g);
             if (i == j) g = s_from<T>(s_real(g) + shift, 0.0);
-            M[e] = g;
+            M[i + (int64_t)j * lm] = g;
         }
         __syncthreads();
         // right-looking upper Cholesky: M[k,j] (j>=k) becomes R[k,j]
         for (int k = 0; k < s; ++k) {
             if (tid == 0) {
-                const double p = s_real(M[k + (int64_t)k * s]);
+                const double p = s_real(M[k + (int64_t)k * lm]);
                 if (!(p > 1e-13)) s_bad = 1;
                 s_minpiv = fmin(s_minpiv, p);
                 s_piv = sqrt(p > 1e-300 ? p : 1e-300);
@@ -362,16 +366,16 @@ chol_factor_kernel(int s, int64_t nrows, const T* __restrict__ G, T* Mg, T* Tout
             __syncthreads();
             if (s_bad && attempt == 0) break;
             const double rkk = s_piv;
-            for (int j = k + 1 + tid; j < s; j += nt) M[k + (int64_t)j * s] = s_rscale(1.0 / rkk, M[k + (int64_t)j * s]);
-            if (tid == 0) M[k + (int64_t)k * s] = s_from<T>(rkk, 0.0);
+            for (int j = k + 1 + tid; j < s; j += nt) M[k + (int64_t)j * lm] = s_rscale(1.0 / rkk, M[k + (int64_t)j * lm]);
+            if (tid == 0) M[k + (int64_t)k * lm] = s_from<T>(rkk, 0.0);
             __syncthreads();
             const int rem = s - k - 1;
             for (int64_t e = tid; e < (int64_t)rem * rem; e += nt) {
                 const int i = k + 1 + (int)(e % rem), j = k + 1 + (int)(e / rem);
                 if (i <= j) {
                     // M[i,j] -= conj(R[k,i]) R[k,j]
-                    const T rki = M[k + (int64_t)i * s], rkj = M[k + (int64_t)j * s];
-                    M[i + (int64_t)j * s] = s_sub(M[i + (int64_t)j * s], s_mul(s_conj(rki), rkj));
+                    const T rki = M[k + (int64_t)i * lm], rkj = M[k + (int64_t)j * lm];
+                    M[i + (int64_t)j * lm] = s_sub(M[i + (int64_t)j * lm], s_mul(s_conj(rki), rkj));
                 }
             }
             __syncthreads();
@@ -389,23 +393,30 @@ chol_factor_kernel(int s, int64_t nrows, const T* __restrict__ G, T* Mg, T* Tout
         }
     }
     __syncthreads();
-    // X = R^-1 (upper): for i = s-1 .. 0, X[i,j] = (delta_ij - sum_{l=i+1..j} R[i,l] X[l,j]) / R[i,i]
-    for (int64_t e = tid; e < (int64_t)s * s; e += nt) X[e] = s_zero(T());
+    // X = R^-1 (upper), right-looking back substitution on all columns at once: starting from
+    // X = I, for k = s-1 .. 0 row k is final after dividing by R[k,k], and its multiples
+    // R[l,k] X[k,:] are removed from the rows l < k.
+    for (int64_t e = tid; e < (int64_t)s * s; e += nt) {
+        const int i = (int)(e % s), j = (int)(e / s);
+        X[i + (int64_t)j * lx] = s_from<T>(i == j ? 1.0 : 0.0, 0.0);
+    }
     __syncthreads();
-    for (int i = s - 1; i >= 0; --i) {
-        const double inv = 1.0 / s_real(M[i + (int64_t)i * s]);
-        for (int j = i + tid; j < s; j += nt) {
-            T acc = s_from<T>(i == j ? 1.0 : 0.0, 0.0);
-            for (int l = i + 1; l <= j; ++l) acc = s_sub(acc, s_mul(M[i + (int64_t)l * s], X[l + (int64_t)j * s]));
-            X[i + (int64_t)j * s] = s_rscale(inv, acc);
+    for (int k = s - 1; k >= 0; --k) {
+        const double inv = 1.0 / s_real(M[k + (int64_t)k * lm]);
+        for (int j = k + tid; j < s; j += nt) X[k + (int64_t)j * lx] = s_rscale(inv, X[k + (int64_t)j * lx]);
+        __syncthreads();
+        const int cols = s - k;
+        for (int64_t e = tid; e < (int64_t)k * cols; e += nt) {
+            const int l = (int)(e % k), j = k + (int)(e / k);
+            X[l + (int64_t)j * lx] = s_sub(X[l + (int64_t)j * lx], s_mul(M[l + (int64_t)k * lm], X[k + (int64_t)j * lx]));
         }
         __syncthreads();
     }
     if (tid == 0 && pivout) pivout[0] = s_minpiv;
     // Tout = D^-1 X
     for (int64_t e = tid; e < (int64_t)s * s; e += nt) {
-        const int i = (int)(e % s);
-        Tout[e] = s_rscale(1.0 / dsc[i], X[e]);
+        const int i = (int)(e % s), j = (int)(e / s);
+        Tout[e] = s_rscale(1.0 / dsc[i], X[i + (int64_t)j * lx]);
     }
 }
 
@@ -416,7 +427,7 @@ rc_status chol_factor(rc_ctx* ctx, int dtype, int64_t s, int64_t nrows, const vo
     RC_TRY(rc_slot(ctx, S_LANCZOS, (size_t)s * s * esz + (size_t)s * 8 + 256, &base));
     double* dsc = (double*)((char*)base + (size_t)s * s * esz);
     const size_t budget = ctx->smem_optin > 4096 ? ctx->smem_optin - 4096 : 0;
-    const size_t mat = (size_t)s * s * esz;
+    const size_t mat = (size_t)s * (s + 1) * esz;  // with the padded leading dimension
     int mode = 0;
     size_t dyn = 0;
     if (2 * mat + (size_t)s * 8 <= budget) {
@@ -497,6 +508,7 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
     }
     __shared__ double s_fro;
     __shared__ int s_rot;
+    __shared__ unsigned long long s_maxsn;  // largest |sin| of the sweep's rotations (bits of a positive double)
     __shared__ double red[32];
     __syncthreads();
     double f = 0.0;
@@ -510,7 +522,10 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
     const int nblk = npair * npair;
     int sweep = 0;
     for (; sweep < max_sweeps; ++sweep) {
-        if (tid == 0) s_rot = 0;
+        if (tid == 0) {
+            s_rot = 0;
+            s_maxsn = 0ull;
+        }
         __syncthreads();
         for (int r = 0; r < M; ++r) {
             for (int i = tid; i < npair; i += nt) {
@@ -529,6 +544,7 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
                         c = 1.0 / sqrt(1.0 + t * t);
                         sn = t * c;
                         s_rot = 1;
+                        atomicMax(&s_maxsn, (unsigned long long)__double_as_longlong(fabs(sn)));
                     }
                 }
                 rc[i] = c;
@@ -538,9 +554,11 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
                 qq[i] = q;
             }
             __syncthreads();
-            // A <- G^H A G on 2x2 blocks (row pair bi, column pair bj)
+            // A <- G^H A G on 2x2 blocks (row pair bi, column pair bj); A stays Hermitian, so
+            // only the blocks with bi <= bj are formed and each is mirrored into (bj, bi)
             for (int e = tid; e < nblk; e += nt) {
                 const int bi = e % npair, bj = e / npair;
+                if (bi > bj) continue;
                 const double si = rsn[bi], sj = rsn[bj];
                 if (si == 0.0 && sj == 0.0) continue;
                 const int pi = pp[bi], qi = qq[bi], pj = pp[bj], qj = qq[bj];
@@ -570,6 +588,12 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
                 A[qi + pj * ld] = n_qp;
                 A[pi + qj * ld] = n_pq;
                 A[qi + qj * ld] = n_qq;
+                if (bi != bj) {
+                    A[pj + pi * ld] = s_conj(n_pp);
+                    A[pj + qi * ld] = s_conj(n_qp);
+                    A[qj + pi * ld] = s_conj(n_pq);
+                    A[qj + qi * ld] = s_conj(n_qq);
+                }
             }
             // Q <- Q G_j (columns p_j, q_j of rows 0..s-1)
             for (int e = tid; e < npair * s; e += nt) {
@@ -586,8 +610,14 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
             __syncthreads();
         }
         const int rot = s_rot;
+        const double maxsn = __longlong_as_double((long long)s_maxsn);
         __syncthreads();
-        if (!rot) break;
+        // no rotation, or only rotations so small (|sin| < 1e-9) that the off-diagonal entries
+        // they leave (of order sin^2) are below the rotation threshold of another sweep
+        if (!rot || maxsn < 1e-9) {
+            if (rot) ++sweep;
+            break;
+        }
     }
     // ascending order (rank sort, ties by index) over the s real indices
     for (int i = tid; i < s; i += nt) {

@@ -197,7 +197,8 @@ static rc_status rm_filter_dispatch(rc_ctx* ctx, rc_op* op, void* V, int64_t ldv
     const int64_t n = op->n;
     const int64_t band = op->kind == 0 ? op->band : (op->skind == 5 ? op->nx : op->nx * op->ny);
     if (op->kind == 0) {
-        CsrRows<TS, TC> pol{op->rowptr, op->colind, (const TS*)(sizeof(real_t<TS>) == 8 ? op->vals64 : op->vals32)};
+        const TS* vals = (const TS*)(sizeof(real_t<TS>) == 8 ? op->vals64 : op->vals32);
+        CsrRows<TS, TC> pol{op->rowptr, op->colind, vals};
         return run_rm_select<CsrRows<TS, TC>, TS, TC>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band);
     }
     using TD = real_t<TS>;

@@ -42,7 +42,7 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src, int src_by
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::); }
 
 // Copy rows [r0, r0 + RT) of columns [0, ncols) of a column-major block into a shared tile laid
 // out column by column with `rp` doubles per column (rows past r_end read as zero).
@@ -122,13 +122,15 @@ gram_mma_kernel(int64_t n, int m, const double* __restrict__ X, int64_t ldx, con
         load_cols_async<GM_KT, V16>(st + SC * GM_KP, GM_KP, Y0, ldy0, m, r0, r_end, tid, NT);
         if (NY == 2) load_cols_async<GM_KT, V16>(st + 2 * SC * GM_KP, GM_KP, Y1, ldy1, m, r0, r_end, tid, NT);
     };
+    // two stages, one barrier per K-tile: after the barrier every warp has finished tile t-1, so
+    // the copies of tile t+1 go into its stage while tile t is multiplied
     if (ntiles > 0) issue(0);
     cp_async_commit();
     for (int64_t t = 0; t < ntiles; ++t) {
+        cp_async_wait0();
+        __syncthreads();
         if (t + 1 < ntiles) issue(t + 1);
         cp_async_commit();
-        cp_async_wait1();
-        __syncthreads();
         const double* xs = gms + (t & 1) * STAGE + (bi * 32 + g) * GM_KP + q;
         const double* ys = gms + (t & 1) * STAGE + (1 + y) * SC * GM_KP + (bj * 32 + g) * GM_KP + q;
 #pragma unroll
@@ -143,7 +145,6 @@ gram_mma_kernel(int64_t n, int m, const double* __restrict__ X, int64_t ldx, con
 #pragma unroll
                 for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
         }
-        __syncthreads();
     }
     double* P = part + ((size_t)y * gridDim.x + blockIdx.x) * (size_t)m * m;
 #pragma unroll
@@ -290,16 +291,17 @@ xt_mma_kernel(int64_t n, int k, int nc, const double* __restrict__ X, int64_t ld
         load_cols_async<XM_RT, V16>(st, XM_RP, X, ldx, k, r0, n, tid, NT);
         if (DUAL) load_cols_async<XM_RT, V16>(st + k4 * XM_RP, XM_RP, W, ldw, k, r0, n, tid, NT);
     };
+    // two stages, one barrier per tile (as in gram_mma_kernel)
     int buf = 0;
     int64_t t = blockIdx.x;
     if (t < ntiles) issue(t, 0);
     cp_async_commit();
     for (; t < ntiles; t += gridDim.x) {
+        cp_async_wait0();
+        __syncthreads();
         const int64_t tn = t + gridDim.x;
         if (tn < ntiles) issue(tn, buf ^ 1);
         cp_async_commit();
-        cp_async_wait1();
-        __syncthreads();
         const double* xs = tiles + buf * stage + slab * 8 + g + q * XM_RP;
         const double* ws = xs + k4 * XM_RP;
         const double* ts = Ts + (cbase + g) * kpt + q;
@@ -343,10 +345,10 @@ xt_mma_kernel(int64_t n, int k, int nc, const double* __restrict__ X, int64_t ld
                 }
             }
         }
-        __syncthreads();
         buf ^= 1;
     }
     if (DUAL && res_count > 0) {
+        __syncthreads();  // the last tile's reads are done before its stage is reused below
         // per column: sum over g (lanes with the same q), then over the four row slabs in order
         double* red = tiles;  // [4][NH*48]; the tiles are no longer read
 #pragma unroll
