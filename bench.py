@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-sample-degree", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-count", type=int, default=64,
+                    help="requests of the configuration-4 serving stream run after the timed solves (0: skip)")
     return ap.parse_args()
 
 
@@ -395,6 +397,19 @@ def run_ours(args):
         "gpu_launches": int(launches),
         "clocks": clk,
     }
+    # ---- serving (configuration 4, the first --serve-count requests of the stream), N = 1 only ----
+    if world == 1 and args.serve_count > 0:
+        from rayleighchebyshevgpgpu_b200 import serve_bench
+        try:
+            sv = serve_bench.run(count=args.serve_count)
+            line["serving"] = {k: sv[k] for k in ("requests", "completed", "eigenpairs_per_s", "requests_per_s",
+                                                  "latency_ms_p50", "latency_ms_p99", "capacity_eigenpairs_per_s",
+                                                  "arrival_rate_per_s", "max_active", "max_jobs_in_batch",
+                                                  "hbm_peak_reserved_bytes")}
+            line["serving"]["workload"] = (f"configuration-4 stream, first {args.serve_count} of 256 requests, "
+                                           "Poisson arrivals at 0.8 x measured capacity, mixed precision")
+        except Exception as e:  # reported, never required for the headline
+            line["serving"] = {"unavailable": str(e)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     op.close()

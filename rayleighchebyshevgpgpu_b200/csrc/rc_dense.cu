@@ -320,7 +320,7 @@ chol_factor_kernel(int s, int64_t nrows, const T* __restrict__ G, T* Mg, T* Tout
                    int mode) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_bad;
-    __shared__ double s_piv, s_minpiv;
+    __shared__ double s_minpiv;
     // In shared memory the matrices have an odd leading dimension (s + 1), so that a warp reading
     // along a row (consecutive columns) hits distinct banks.
     const int lm = mode >= 1 ? s + 1 : s;
@@ -355,31 +355,28 @@ chol_factor_kernel(int s, int64_t nrows, const T* __restrict__ G, T* Mg, T* Tout
             M[i + (int64_t)j * lm] = g;
         }
         __syncthreads();
-        // right-looking upper Cholesky: M[k,j] (j>=k) becomes R[k,j]
+        // right-looking upper Cholesky with one barrier per step: row k is final once step k-1
+        // is done, so every thread reads the pivot p_k itself and updates the trailing matrix with
+        // the unscaled row, M[i,j] -= conj(M[k,i]) M[k,j] / p_k; the rows are scaled by sqrt(p_k)
+        // after the loop.
+        bool bad = false;
         for (int k = 0; k < s; ++k) {
-            if (tid == 0) {
-                const double p = s_real(M[k + (int64_t)k * lm]);
-                if (!(p > 1e-13)) s_bad = 1;
-                s_minpiv = fmin(s_minpiv, p);
-                s_piv = sqrt(p > 1e-300 ? p : 1e-300);
-            }
-            __syncthreads();
-            if (s_bad && attempt == 0) break;
-            const double rkk = s_piv;
-            for (int j = k + 1 + tid; j < s; j += nt) M[k + (int64_t)j * lm] = s_rscale(1.0 / rkk, M[k + (int64_t)j * lm]);
-            if (tid == 0) M[k + (int64_t)k * lm] = s_from<T>(rkk, 0.0);
-            __syncthreads();
+            const double p = s_real(M[k + (int64_t)k * lm]);
+            if (!(p > 1e-13)) bad = true;
+            if (tid == 0) s_minpiv = fmin(s_minpiv, p);
+            if (bad && attempt == 0) break;
+            const double pinv = 1.0 / (p > 1e-300 ? p : 1e-300);
             const int rem = s - k - 1;
             for (int64_t e = tid; e < (int64_t)rem * rem; e += nt) {
                 const int i = k + 1 + (int)(e % rem), j = k + 1 + (int)(e / rem);
                 if (i <= j) {
-                    // M[i,j] -= conj(R[k,i]) R[k,j]
-                    const T rki = M[k + (int64_t)i * lm], rkj = M[k + (int64_t)j * lm];
-                    M[i + (int64_t)j * lm] = s_sub(M[i + (int64_t)j * lm], s_mul(s_conj(rki), rkj));
+                    const T mki = M[k + (int64_t)i * lm], mkj = M[k + (int64_t)j * lm];
+                    M[i + (int64_t)j * lm] = s_sub(M[i + (int64_t)j * lm], s_rscale(pinv, s_mul(s_conj(mki), mkj)));
                 }
             }
             __syncthreads();
         }
+        if (tid == 0 && bad) s_bad = 1;
         __syncthreads();
         if (!s_bad) break;
         if (attempt == 0) {
@@ -393,30 +390,42 @@ chol_factor_kernel(int s, int64_t nrows, const T* __restrict__ G, T* Mg, T* Tout
         }
     }
     __syncthreads();
-    // X = R^-1 (upper), right-looking back substitution on all columns at once: starting from
-    // X = I, for k = s-1 .. 0 row k is final after dividing by R[k,k], and its multiples
-    // R[l,k] X[k,:] are removed from the rows l < k.
+    // R[k,j] = M[k,j] / sqrt(p_k) (j > k), R[k,k] = sqrt(p_k); the pivots go through X first
+    for (int k = tid; k < s; k += nt) {
+        const double p = s_real(M[k + (int64_t)k * lm]);
+        X[k] = s_from<T>(sqrt(p > 1e-300 ? p : 1e-300), 0.0);
+    }
+    __syncthreads();
+    for (int64_t e = tid; e < (int64_t)s * s; e += nt) {
+        const int i = (int)(e % s), j = (int)(e / s);
+        const double rkk = s_real(X[i]);
+        if (j > i) M[i + (int64_t)j * lm] = s_rscale(1.0 / rkk, M[i + (int64_t)j * lm]);
+        else if (j == i) M[i + (int64_t)i * lm] = s_from<T>(rkk, 0.0);
+    }
+    __syncthreads();
+    // X = R^-1 (upper), right-looking back substitution on all columns at once with one barrier
+    // per step: Y starts as I; at step k (s-1 .. 0) row k of Y is final, and R[l,k] Y[k,:]/R[k,k]
+    // is removed from the rows l < k. X[k,:] = Y[k,:]/R[k,k] is applied in the last pass.
     for (int64_t e = tid; e < (int64_t)s * s; e += nt) {
         const int i = (int)(e % s), j = (int)(e / s);
         X[i + (int64_t)j * lx] = s_from<T>(i == j ? 1.0 : 0.0, 0.0);
     }
     __syncthreads();
-    for (int k = s - 1; k >= 0; --k) {
+    for (int k = s - 1; k >= 1; --k) {
         const double inv = 1.0 / s_real(M[k + (int64_t)k * lm]);
-        for (int j = k + tid; j < s; j += nt) X[k + (int64_t)j * lx] = s_rscale(inv, X[k + (int64_t)j * lx]);
-        __syncthreads();
         const int cols = s - k;
         for (int64_t e = tid; e < (int64_t)k * cols; e += nt) {
             const int l = (int)(e % k), j = k + (int)(e / k);
-            X[l + (int64_t)j * lx] = s_sub(X[l + (int64_t)j * lx], s_mul(M[l + (int64_t)k * lm], X[k + (int64_t)j * lx]));
+            X[l + (int64_t)j * lx] =
+                s_sub(X[l + (int64_t)j * lx], s_mul(M[l + (int64_t)k * lm], s_rscale(inv, X[k + (int64_t)j * lx])));
         }
         __syncthreads();
     }
     if (tid == 0 && pivout) pivout[0] = s_minpiv;
-    // Tout = D^-1 X
+    // Tout = D^-1 X = D^-1 diag(R)^-1 Y
     for (int64_t e = tid; e < (int64_t)s * s; e += nt) {
         const int i = (int)(e % s), j = (int)(e / s);
-        Tout[e] = s_rscale(1.0 / dsc[i], X[i + (int64_t)j * lx]);
+        Tout[e] = s_rscale(1.0 / (dsc[i] * s_real(M[i + (int64_t)i * lm])), X[i + (int64_t)j * lx]);
     }
 }
 

@@ -30,7 +30,7 @@ rm_step_kernel(Pol op, int64_t n, int nseg, int64_t ld, int groups, const TS* __
 
 // Degree step of the correction filter: y = alpha A x + beta x + gamma z + sig[c] src.
 template <class Pol, class TS, class TC, int W, class IX>
-__global__ void __launch_bounds__(kRmThreads, rm_min_blocks<TS>())
+__global__ void __launch_bounds__(kRmThreads, rm_src_min_blocks())
 rm_step_src_kernel(Pol op, int64_t n, int nseg, int64_t ld, int groups, const TS* __restrict__ x, const TS* z, TS* y,
                    TC alpha, TC beta, TC gamma, int64_t pf_z, int64_t pf_x, const TS* __restrict__ src,
                    const float* __restrict__ sig) {

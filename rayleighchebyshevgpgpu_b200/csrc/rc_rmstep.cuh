@@ -38,13 +38,17 @@ __device__ __forceinline__ void st16(TS* p, const Pack16<TS>& v) {
 }
 
 constexpr int kRmThreads = 256;
-// Resident CTAs per SM the register budget must allow: 6 (40 registers) for both storage
-// precisions. Measured on 128^3 7-point CSR operators with 96 columns: for FP32 storage, 6 is 6 %
-// faster than 8 (32 registers, which spill in the correction step) and than 4; for FP64, 6 is
-// faster than 4 and 3.
+// Resident CTAs per SM the register budget must allow: 8 (32 registers) for FP32 storage, 6 (40
+// registers) for FP64 storage and for the correction step (rm_src_min_blocks), which spills at 32.
+// Measured on 128^3 7-point CSR operators with 96 columns: the FP32 step takes 0.52 ms at 8 and
+// 0.60 ms at 6; the correction step 0.75 ms at 8 and 0.66 ms at 6; the FP64 step is fastest at 6.
 #ifndef RC_RM_MIN_BLOCKS_F32
-#define RC_RM_MIN_BLOCKS_F32 6
+#define RC_RM_MIN_BLOCKS_F32 8
 #endif
+#ifndef RC_RM_MIN_BLOCKS_SRC
+#define RC_RM_MIN_BLOCKS_SRC 6
+#endif
+constexpr int rm_src_min_blocks() { return RC_RM_MIN_BLOCKS_SRC; }
 #ifndef RC_RM_MIN_BLOCKS_F64
 #define RC_RM_MIN_BLOCKS_F64 6
 #endif
