@@ -128,6 +128,8 @@ rc_status rc_ctx_create(int device, rc_ctx** out) {
         c->smem_optin = prop.sharedMemPerBlockOptin;
     }
     c->slots.resize(S_COUNT);
+    if (const char* v = std::getenv("RCB200_CM_CPT")) c->cm_cpt = std::max(0, std::atoi(v));
+    if (const char* v = std::getenv("RCB200_CM_ORDER")) c->cm_order = std::atoi(v) == 1 ? 1 : 0;
     if (const char* v = std::getenv("RCB200_CSR_KERNEL")) {
         if (!std::strcmp(v, "loop")) c->csr_variant = 1;
         else if (!std::strcmp(v, "reg")) c->csr_variant = 2;

@@ -300,8 +300,10 @@ rc_status xt(rc_ctx* ctx, int dtype, const XtArgs& a) {
         a.X2 != nullptr && a.Y2 == nullptr && a.lam != nullptr && (a.res_count > 0 || a.R32 != nullptr);
     if (plain && (a.X2 == nullptr || dual_res_only) && xt2_supported(dtype, a.k, a.nc))
         return xt2(ctx, a.n, a.k, a.nc, (const double*)a.X, a.ldx, (const double*)a.T, a.ldt, (double*)a.Y, a.ldy,
-                   (const double*)a.X2, a.ldx2, a.lam, dual_res_only ? a.res_count : 0, a.res, a.R32, a.ldr);
-    if (a.R32) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "xt: the FP32 residual block needs a real block of <= 96 columns");
+                   (const double*)a.X2, a.ldx2, a.lam, dual_res_only ? a.res_count : 0, a.res, a.R32, a.ldr, a.Yrm,
+                   a.ldyr);
+    if (a.R32 || a.Yrm)
+        return rc_fail(ctx, RC_ERR_UNSUPPORTED, "xt: row-major outputs need a real block of <= 96 columns");
     return dtype == RC_COMPLEX128 ? xt_t<double2>(ctx, a) : xt_t<double>(ctx, a);
 }
 
@@ -322,13 +324,15 @@ chol_factor_kernel(int s, int64_t nrows, const T* __restrict__ G, T* Mg, T* Tout
     __shared__ int s_bad;
     __shared__ double s_minpiv;
     // In shared memory the matrices have an odd leading dimension (s + 1), so that a warp reading
-    // along a row (consecutive columns) hits distinct banks.
+    // along a row (consecutive columns) hits distinct banks. The block is 32 x (blockDim/32):
+    // lane tx walks rows, warp ty walks columns, so no index needs a division.
     const int lm = mode >= 1 ? s + 1 : s;
     const int lx = mode == 2 ? s + 1 : s;
     T* M = mode >= 1 ? (T*)smem_raw : Mg;
     T* X = mode == 2 ? M + (size_t)s * lm : Tout;
     double* dsc = mode == 2 ? (double*)(X + (size_t)s * lx) : (mode == 1 ? (double*)(M + (size_t)s * lm) : dscg);
     const int tid = threadIdx.x, nt = blockDim.x;
+    const int tx = tid & 31, ty = tid >> 5, nwy = nt >> 5;
     for (int i = tid; i < s; i += nt) {
         const double gi = s_real(G[i + (int64_t)i * s]);
         double d = (gi > 0.0 && isfinite(gi)) ? sqrt(gi) : 0.0;
@@ -346,19 +350,19 @@ chol_factor_kernel(int s, int64_t nrows, const T* __restrict__ G, T* Mg, T* Tout
     for (int attempt = 0; attempt < 2; ++attempt) {
         const double shift = attempt == 0 ? 0.0 : sigma;
         if (tid == 0) s_minpiv = 1e300;
-        for (int64_t e = tid; e < (int64_t)s * s; e += nt) {
-            const int i = (int)(e % s), j = (int)(e / s);
-            T g = G[e];
-            if (!isfinite(s_real(g)) || !isfinite(s_imag(g))) g = s_zero(T());
-            g = s_rscale(1.0 / (dsc[i] * dsc[j]), g);
-            if (i == j) g = s_from<T>(s_real(g) + shift, 0.0);
-            M[i + (int64_t)j * lm] = g;
-        }
+        for (int j = ty; j < s; j += nwy)
+            for (int i = tx; i < s; i += 32) {
+                T g = G[i + (int64_t)j * s];
+                if (!isfinite(s_real(g)) || !isfinite(s_imag(g))) g = s_zero(T());
+                g = s_rscale(1.0 / (dsc[i] * dsc[j]), g);
+                if (i == j) g = s_from<T>(s_real(g) + shift, 0.0);
+                M[i + (int64_t)j * lm] = g;
+            }
         __syncthreads();
         // right-looking upper Cholesky with one barrier per step: row k is final once step k-1
         // is done, so every thread reads the pivot p_k itself and updates the trailing matrix with
-        // the unscaled row, M[i,j] -= conj(M[k,i]) M[k,j] / p_k; the rows are scaled by sqrt(p_k)
-        // after the loop.
+        // the unscaled row, M[i,j] -= conj(M[k,i]) M[k,j] / p_k (k < i <= j); the rows are scaled
+        // by sqrt(p_k) after the loop.
         bool bad = false;
         for (int k = 0; k < s; ++k) {
             const double p = s_real(M[k + (int64_t)k * lm]);
@@ -366,13 +370,10 @@ chol_factor_kernel(int s, int64_t nrows, const T* __restrict__ G, T* Mg, T* Tout
             if (tid == 0) s_minpiv = fmin(s_minpiv, p);
             if (bad && attempt == 0) break;
             const double pinv = 1.0 / (p > 1e-300 ? p : 1e-300);
-            const int rem = s - k - 1;
-            for (int64_t e = tid; e < (int64_t)rem * rem; e += nt) {
-                const int i = k + 1 + (int)(e % rem), j = k + 1 + (int)(e / rem);
-                if (i <= j) {
-                    const T mki = M[k + (int64_t)i * lm], mkj = M[k + (int64_t)j * lm];
-                    M[i + (int64_t)j * lm] = s_sub(M[i + (int64_t)j * lm], s_rscale(pinv, s_mul(s_conj(mki), mkj)));
-                }
+            for (int j = k + 1 + ty; j < s; j += nwy) {
+                const T mkj = s_rscale(pinv, M[k + (int64_t)j * lm]);
+                for (int i = k + 1 + tx; i <= j; i += 32)
+                    M[i + (int64_t)j * lm] = s_sub(M[i + (int64_t)j * lm], s_mul(s_conj(M[k + (int64_t)i * lm]), mkj));
             }
             __syncthreads();
         }
@@ -396,37 +397,33 @@ chol_factor_kernel(int s, int64_t nrows, const T* __restrict__ G, T* Mg, T* Tout
         X[k] = s_from<T>(sqrt(p > 1e-300 ? p : 1e-300), 0.0);
     }
     __syncthreads();
-    for (int64_t e = tid; e < (int64_t)s * s; e += nt) {
-        const int i = (int)(e % s), j = (int)(e / s);
-        const double rkk = s_real(X[i]);
-        if (j > i) M[i + (int64_t)j * lm] = s_rscale(1.0 / rkk, M[i + (int64_t)j * lm]);
-        else if (j == i) M[i + (int64_t)i * lm] = s_from<T>(rkk, 0.0);
-    }
+    for (int j = ty; j < s; j += nwy)
+        for (int i = tx; i <= j; i += 32) {
+            const double rkk = s_real(X[i]);
+            if (j > i) M[i + (int64_t)j * lm] = s_rscale(1.0 / rkk, M[i + (int64_t)j * lm]);
+            else M[i + (int64_t)i * lm] = s_from<T>(rkk, 0.0);
+        }
     __syncthreads();
     // X = R^-1 (upper), right-looking back substitution on all columns at once with one barrier
-    // per step: Y starts as I; at step k (s-1 .. 0) row k of Y is final, and R[l,k] Y[k,:]/R[k,k]
+    // per step: Y starts as I; at step k (s-1 .. 1) row k of Y is final, and R[l,k] Y[k,:]/R[k,k]
     // is removed from the rows l < k. X[k,:] = Y[k,:]/R[k,k] is applied in the last pass.
-    for (int64_t e = tid; e < (int64_t)s * s; e += nt) {
-        const int i = (int)(e % s), j = (int)(e / s);
-        X[i + (int64_t)j * lx] = s_from<T>(i == j ? 1.0 : 0.0, 0.0);
-    }
+    for (int j = ty; j < s; j += nwy)
+        for (int i = tx; i < s; i += 32) X[i + (int64_t)j * lx] = s_from<T>(i == j ? 1.0 : 0.0, 0.0);
     __syncthreads();
     for (int k = s - 1; k >= 1; --k) {
         const double inv = 1.0 / s_real(M[k + (int64_t)k * lm]);
-        const int cols = s - k;
-        for (int64_t e = tid; e < (int64_t)k * cols; e += nt) {
-            const int l = (int)(e % k), j = k + (int)(e / k);
-            X[l + (int64_t)j * lx] =
-                s_sub(X[l + (int64_t)j * lx], s_mul(M[l + (int64_t)k * lm], s_rscale(inv, X[k + (int64_t)j * lx])));
+        for (int j = k + ty; j < s; j += nwy) {
+            const T ykj = s_rscale(inv, X[k + (int64_t)j * lx]);
+            for (int l = tx; l < k; l += 32)
+                X[l + (int64_t)j * lx] = s_sub(X[l + (int64_t)j * lx], s_mul(M[l + (int64_t)k * lm], ykj));
         }
         __syncthreads();
     }
     if (tid == 0 && pivout) pivout[0] = s_minpiv;
     // Tout = D^-1 X = D^-1 diag(R)^-1 Y
-    for (int64_t e = tid; e < (int64_t)s * s; e += nt) {
-        const int i = (int)(e % s), j = (int)(e / s);
-        Tout[e] = s_rscale(1.0 / (dsc[i] * s_real(M[i + (int64_t)i * lm])), X[i + (int64_t)j * lx]);
-    }
+    for (int j = ty; j < s; j += nwy)
+        for (int i = tx; i < s; i += 32)
+            Tout[i + (int64_t)j * s] = s_rscale(1.0 / (dsc[i] * s_real(M[i + (int64_t)i * lm])), X[i + (int64_t)j * lx]);
 }
 
 rc_status chol_factor(rc_ctx* ctx, int dtype, int64_t s, int64_t nrows, const void* G, void* Tout, int* flags,
@@ -510,6 +507,7 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
     }
     Q = A + (size_t)sp * ld;
     const int tid = threadIdx.x, nt = blockDim.x;
+    const int tx = tid & 31, ty = tid >> 5, nwy = nt >> 5;  // lanes walk rows, warps walk columns
     for (int e = tid; e < sp * sp; e += nt) {
         const int i = e % sp, j = e / sp;
         A[i + j * ld] = (i < s && j < s) ? Ain[i + (int64_t)j * s] : s_zero(T());
@@ -528,7 +526,6 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
     const double abs_tol = 1e-17 * s_fro;
     const double rel_tol = 1e-15;
     const int M = sp - 1;
-    const int nblk = npair * npair;
     int sweep = 0;
     for (; sweep < max_sweeps; ++sweep) {
         if (tid == 0) {
@@ -537,12 +534,27 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
         }
         __syncthreads();
         for (int r = 0; r < M; ++r) {
+            unsigned long long snbits = 0ull;  // this thread's largest |sin| (bits of a positive double)
             for (int i = tid; i < npair; i += nt) {
                 int p, q;
                 rr_pair<T>(r, i, M, sp, p, q);
                 double c = 1.0, sn = 0.0;
                 T u = s_from<T>(1.0, 0.0);
-                if (q < s) {
+                if (q < s && !IsComplex<T>::value) {
+                    // real: u = sign(apq), and the angle from one square root and one division,
+                    // t = sign(d) 2|apq| / (|d| + sqrt(d^2 + 4 apq^2)) with d = aqq - app
+                    const double apq = s_real(A[p + q * ld]);
+                    const double app = s_real(A[p + p * ld]), aqq = s_real(A[q + q * ld]);
+                    const double mag = fabs(apq);
+                    if (mag > abs_tol && mag * mag > rel_tol * rel_tol * fabs(app * aqq)) {
+                        u = s_from<T>(apq >= 0.0 ? 1.0 : -1.0, 0.0);
+                        const double d = aqq - app;
+                        const double t = copysign(2.0 * mag, d) / (fabs(d) + sqrt(d * d + 4.0 * mag * mag));
+                        c = rsqrt(1.0 + t * t);
+                        sn = t * c;
+                        snbits = max(snbits, (unsigned long long)__double_as_longlong(fabs(sn)));
+                    }
+                } else if (q < s) {
                     const T apq = A[p + q * ld];
                     const double app = s_real(A[p + p * ld]), aqq = s_real(A[q + q * ld]);
                     const double mag = sqrt(s_abs2(apq));
@@ -552,8 +564,7 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
                         const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
                         c = 1.0 / sqrt(1.0 + t * t);
                         sn = t * c;
-                        s_rot = 1;
-                        atomicMax(&s_maxsn, (unsigned long long)__double_as_longlong(fabs(sn)));
+                        snbits = max(snbits, (unsigned long long)__double_as_longlong(fabs(sn)));
                     }
                 }
                 rc[i] = c;
@@ -562,12 +573,20 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
                 pp[i] = p;
                 qq[i] = q;
             }
+            // one shared-memory atomic per warp that computed angles (a rotation has sin != 0)
+            if (tid < ((npair + 31) & ~31)) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) snbits = max(snbits, __shfl_xor_sync(0xffffffffu, snbits, o));
+                if ((tid & 31) == 0 && snbits) {
+                    atomicMax(&s_maxsn, snbits);
+                    s_rot = 1;
+                }
+            }
             __syncthreads();
             // A <- G^H A G on 2x2 blocks (row pair bi, column pair bj); A stays Hermitian, so
             // only the blocks with bi <= bj are formed and each is mirrored into (bj, bi)
-            for (int e = tid; e < nblk; e += nt) {
-                const int bi = e % npair, bj = e / npair;
-                if (bi > bj) continue;
+            for (int bj = ty; bj < npair; bj += nwy)
+            for (int bi = tx; bi <= bj; bi += 32) {
                 const double si = rsn[bi], sj = rsn[bj];
                 if (si == 0.0 && sj == 0.0) continue;
                 const int pi = pp[bi], qi = qq[bi], pj = pp[bj], qj = qq[bj];
@@ -605,8 +624,8 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
                 }
             }
             // Q <- Q G_j (columns p_j, q_j of rows 0..s-1)
-            for (int e = tid; e < npair * s; e += nt) {
-                const int row = e % s, bj = e / s;
+            for (int bj = ty; bj < npair; bj += nwy)
+            for (int row = tx; row < s; row += 32) {
                 const double sj = rsn[bj];
                 if (sj == 0.0) continue;
                 const int pj = pp[bj], qj = qq[bj];

@@ -13,6 +13,7 @@
 //   to_cm:     x_m/(m+1) row-major -> X column-major (FP64)
 // Storage/compute: FP32 (c64) in MIXED precision, FP64 (c128) otherwise.
 #include <cstring>
+#include <type_traits>
 #include "rc_common.cuh"
 #include "rc_internal.h"
 #include "rc_rowops.cuh"
@@ -36,6 +37,43 @@ rm_step_src_kernel(Pol op, int64_t n, int nseg, int64_t ld, int groups, const TS
                    const float* __restrict__ sig) {
     rm_step_rows<Pol, TS, TC, W, IX, true>(op, n, nseg, ld, groups, (int64_t)blockIdx.x, x, z, y, alpha, beta, gamma,
                                            pf_z, pf_x, src, sig);
+}
+
+// The 27-point steps with the box sum reused along x (rm_step_rows27).
+// 4 resident CTAs per SM: the three cross-section sums need more than the 40 registers of the
+// per-row steps.
+template <class TD, class TS, class TC, int W, class IX, bool SRC>
+__global__ void __launch_bounds__(kRmThreads, 4)
+rm_step27_kernel(StencilRows<TD, TC, 27> op, int64_t n, int nseg, int64_t ld, const TS* __restrict__ x, const TS* z,
+                 TS* y, TC alpha, TC beta, TC gamma, int64_t pf_z, int64_t pf_x, const TS* __restrict__ src,
+                 const float* __restrict__ sig) {
+    rm_step_rows27<TD, TS, TC, W, IX, SRC>(op, n, nseg, ld, kRun27, (int64_t)blockIdx.x, x, z, y, alpha, beta, gamma,
+                                           pf_z, pf_x, src, sig);
+}
+
+template <class Pol, class TS, class TC, int W, class IX, bool SRC>
+static void launch_step(rc_ctx* ctx, const Pol& pol, int64_t n, int nseg, int64_t ld, int groups, const TS* x,
+                        const TS* z, TS* y, TC a, TC b, TC g, int64_t pf_z, int64_t pf_x, const TS* src,
+                        const float* sig) {
+    const int rows_per_iter = kRmThreads / nseg;
+    if constexpr (IsStencil27<Pol>::value) {
+        using TD = typename IsStencil27<Pol>::diag_t;
+        const int64_t rows_per_cta = (int64_t)kRun27 * rows_per_iter;
+        const unsigned grid = (unsigned)((n + rows_per_cta - 1) / rows_per_cta);
+        rm_step27_kernel<TD, TS, TC, W, IX, SRC><<<grid, kRmThreads, 0, ctx->stream>>>(pol, n, nseg, ld, x, z, y, a, b,
+                                                                                       g, pf_z, pf_x, src, sig);
+    } else {
+        const int64_t rows_per_cta = (int64_t)groups * rows_per_iter;
+        const unsigned grid = (unsigned)((n + rows_per_cta - 1) / rows_per_cta);
+        if (SRC)
+            rm_step_src_kernel<Pol, TS, TC, W, IX><<<grid, kRmThreads, 0, ctx->stream>>>(pol, n, nseg, ld, groups, x,
+                                                                                         z, y, a, b, g, pf_z, pf_x,
+                                                                                         src, sig);
+        else
+            rm_step_kernel<Pol, TS, TC, W, IX><<<grid, kRmThreads, 0, ctx->stream>>>(pol, n, nseg, ld, groups, x, z, y,
+                                                                                     a, b, g, pf_z, pf_x);
+    }
+    ctx->launches++;
 }
 
 // Scalar recurrence of the correction filter, one thread per column c:
@@ -98,14 +136,11 @@ static rc_status run_rm_filter(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, 
     if (ld % (VEC * W) != 0) return rc_fail(ctx, RC_ERR_INVALID, "row-major filter: leading dimension not padded");
     const int nseg = (int)(ld / (VEC * W));
     if (nseg > kRmThreads) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "row-major filter: block too wide");
-    const int rows_per_iter = kRmThreads / nseg;
     // consecutive row groups per CTA (measured on 128^3 7-point operators, 96 columns):
     // CSR 4 (FP32) / 2 (FP64), stencil 8 (FP32) / 4 (FP64)
     constexpr bool kCsr = Pol::kIsCsr;
     constexpr bool kF32 = sizeof(real_t<TS>) == 4;
     const int groups = ctx->rm_groups > 0 ? ctx->rm_groups : (kCsr ? (kF32 ? 4 : 2) : (kF32 ? 8 : 4));
-    const int64_t rows_per_cta = (int64_t)groups * rows_per_iter;
-    const unsigned grid_seg = (unsigned)((n + rows_per_cta - 1) / rows_per_cta);
     if ((s + 31) / 32 > 65535) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "row-major filter: too many columns");
     const dim3 tgrid((unsigned)((n + 31) / 32), (unsigned)((s + 31) / 32)), tblk(32, 8);
     TS* A = (TS*)bufA;
@@ -119,9 +154,8 @@ static rc_status run_rm_filter(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, 
         TS* y = k % 2 ? B : A;                // x_k overwrites x_{k-2}
         // k = 1 has no x_{k-2} (gamma = 0): z is not read
         const TS* z = k >= 2 ? y : nullptr;
-        rm_step_kernel<Pol, TS, TC, W, IX><<<grid_seg, kRmThreads, 0, ctx->stream>>>(
-            pol, n, nseg, ld, groups, xk1, z, y, ta, tb, k >= 2 ? tm1 : s_zero(TC()), pf_z, pf_x);
-        ctx->launches++;
+        launch_step<Pol, TS, TC, W, IX, false>(ctx, pol, n, nseg, ld, groups, xk1, z, y, ta, tb,
+                                               k >= 2 ? tm1 : s_zero(TC()), pf_z, pf_x, nullptr, nullptr);
     }
     RC_CU(ctx, cudaGetLastError());
     step_mark(ctx);
@@ -151,19 +185,15 @@ static rc_status run_rm_corr(rc_ctx* ctx, const Pol& pol, int64_t n, double* V, 
     if (ld % (VEC * W) != 0) return rc_fail(ctx, RC_ERR_INVALID, "correction filter: leading dimension not padded");
     const int nseg = (int)(ld / (VEC * W));
     if (nseg > kRmThreads) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "correction filter: block too wide");
-    const int rows_per_iter = kRmThreads / nseg;
     constexpr bool kCsr = Pol::kIsCsr;
     const int groups = ctx->rm_groups > 0 ? ctx->rm_groups : (kCsr ? 4 : 8);
-    const int64_t rows_per_cta = (int64_t)groups * rows_per_iter;
-    const unsigned grid_seg = (unsigned)((n + rows_per_cta - 1) / rows_per_cta);
     step_mark(ctx);
     for (int64_t k = 2; k <= degree; ++k) {
         const TS* xk1 = k == 2 ? R : ((k - 1) % 2 == 0 ? A : B);   // e_{k-1}
         TS* y = k % 2 == 0 ? A : B;                                  // e_k
         const TS* z = k == 2 ? nullptr : (k == 3 ? R : y);           // e_{k-2}
-        rm_step_src_kernel<Pol, TS, TC, W, IX><<<grid_seg, kRmThreads, 0, ctx->stream>>>(
-            pol, n, nseg, ld, groups, xk1, z, y, ta, tb, k == 2 ? s_zero(TC()) : tm1, pf_z, pf_x, R, sig + k * ld);
-        ctx->launches++;
+        launch_step<Pol, TS, TC, W, IX, true>(ctx, pol, n, nseg, ld, groups, xk1, z, y, ta, tb,
+                                              k == 2 ? s_zero(TC()) : tm1, pf_z, pf_x, R, sig + k * ld);
     }
     RC_CU(ctx, cudaGetLastError());
     step_mark(ctx);

@@ -10,8 +10,9 @@
 //         the 32x32 super-block (bi, bj) of C_y in 16 mma tiles. Per-chunk partials are summed
 //         by gram2_reduce_kernel in a fixed order (deterministic).
 //  xt2:   Y = X T (n x k times k x nc, k, nc <= 96), persistent CTAs with T resident in shared
-//         memory and 32-row tiles of X (and W) double-buffered; warp (slab, half) forms 8 rows x
-//         48 columns. The dual form also forms W T for the columns that need it and reduces
+//         memory. Plain form: 64-row tiles of X double-buffered, warp (slab, half) forms 16 rows x
+//         48 columns. Dual form (32-row tiles of X and W, 8-row warp slabs) also forms W T for the
+//         columns that need it and reduces
 //         ||(W T)_c - lam_c (X T)_c||^2 for c < res_count; with R32 it writes the residual block
 //         R = W T - (X T) diag(lam) in row-major FP32 (the source term of the correction filter).
 // These replace cublasDgemm(OP_T, OP_N) and cublasDgemm(OP_N, OP_N) plus the residual kernel
@@ -371,6 +372,90 @@ xt_mma_kernel(int64_t n, int k, int nc, const double* __restrict__ X, int64_t ld
     }
 }
 
+// Plain product Y = X T (no dual): 64-row tiles, warp (slab, half) forms 16 rows x 48 columns
+// (two mma row tiles share each B fragment: 8 shared-memory reads per 12 mma).
+constexpr int XP_RT = 64;
+constexpr int XP_RP = XP_RT + 4;  // = 4 mod 16
+
+template <int NH, bool V16>
+__global__ void __launch_bounds__(128 * NH, 1)
+xt_mma_plain_kernel(int64_t n, int k, int nc, const double* __restrict__ X, int64_t ldx,
+                    const double* __restrict__ Tm, int64_t ldt, double* __restrict__ Y, int64_t ldy,
+                    double* __restrict__ Yrm, int64_t ldyr) {
+    constexpr int NT = 128 * NH;
+    const int kpt = xm_kpt(k);
+    const int k4 = (k + 3) / 4 * 4;
+    extern __shared__ __align__(16) double xps[];
+    double* Ts = xps;                            // [NH*48][kpt]
+    double* tiles = Ts + (size_t)NH * 48 * kpt;  // [2][k4][XP_RP]
+    const int stage = k4 * XP_RP;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, q = lane & 3;
+    const int slab = warp & 3, half = warp >> 2;
+    const int cbase = half * 48;
+    for (int e = tid; e < NH * 48 * kpt; e += NT) {
+        const int c = e / kpt, kk = e - c * kpt;
+        Ts[e] = (c < nc && kk < k) ? Tm[kk + (int64_t)c * ldt] : 0.0;
+    }
+    {
+        const int per = (k4 - k) * XP_RP;
+        for (int e = tid; e < 2 * per; e += NT) {
+            const int st = e / per, f = e - st * per;
+            tiles[st * stage + k * XP_RP + f] = 0.0;
+        }
+    }
+    const int64_t ntiles = (n + XP_RT - 1) / XP_RT;
+    int buf = 0;
+    int64_t t = blockIdx.x;
+    if (t < ntiles) load_cols_async<XP_RT, V16>(tiles, XP_RP, X, ldx, k, t * XP_RT, n, tid, NT);
+    cp_async_commit();
+    for (; t < ntiles; t += gridDim.x) {
+        cp_async_wait0();
+        __syncthreads();
+        const int64_t tn = t + gridDim.x;
+        if (tn < ntiles) load_cols_async<XP_RT, V16>(tiles + (buf ^ 1) * stage, XP_RP, X, ldx, k, tn * XP_RT, n, tid, NT);
+        cp_async_commit();
+        const double* xs = tiles + buf * stage + slab * 16 + g + q * XP_RP;
+        const double* ts = Ts + (cbase + g) * kpt + q;
+        double acc[2][XM_CT][2];
+#pragma unroll
+        for (int m = 0; m < 2; ++m)
+#pragma unroll
+            for (int j = 0; j < XM_CT; ++j) acc[m][j][0] = acc[m][j][1] = 0.0;
+#pragma unroll 2
+        for (int k0 = 0; k0 < k4; k0 += 4) {
+            const double a0 = xs[k0 * XP_RP], a1 = xs[k0 * XP_RP + 8];
+            double b[XM_CT];
+#pragma unroll
+            for (int j = 0; j < XM_CT; ++j) b[j] = ts[j * 8 * kpt + k0];
+#pragma unroll
+            for (int j = 0; j < XM_CT; ++j) {
+                dmma(acc[0][j][0], acc[0][j][1], a0, b[j]);
+                dmma(acc[1][j][0], acc[1][j][1], a1, b[j]);
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+            const int64_t r = t * XP_RT + slab * 16 + m * 8 + g;
+            if (r < n) {
+#pragma unroll
+                for (int j = 0; j < XM_CT; ++j) {
+                    const int c = cbase + j * 8 + 2 * q;
+                    if (c < nc) Y[r + (int64_t)c * ldy] = acc[m][j][0];
+                    if (c + 1 < nc) Y[r + (int64_t)(c + 1) * ldy] = acc[m][j][1];
+                    if (Yrm) {  // row-major copy (even leading dimension: 16-byte pairs)
+                        if (c + 1 < nc)
+                            *reinterpret_cast<double2*>(Yrm + r * ldyr + c) = make_double2(acc[m][j][0], acc[m][j][1]);
+                        else if (c < nc)
+                            Yrm[r * ldyr + c] = acc[m][j][0];
+                    }
+                }
+            }
+        }
+        buf ^= 1;
+    }
+}
+
 __global__ void resid2_reduce_kernel(int64_t nblocks, int res_count, const double* __restrict__ rpart,
                                      double* __restrict__ res) {
     const int c = blockIdx.x;
@@ -403,7 +488,7 @@ static rc_status xt_mma_launch(rc_ctx* ctx, unsigned grid, int64_t n, int64_t k,
 // and with R32 the residual block (all nc columns) in row-major FP32 with leading dimension ldr.
 rc_status xt2(rc_ctx* ctx, int64_t n, int64_t k, int64_t nc, const double* X, int64_t ldx, const double* T,
               int64_t ldt, double* Y, int64_t ldy, const double* W, int64_t ldw, const double* lam, int64_t res_count,
-              double* res, float* R32, int64_t ldr) {
+              double* res, float* R32, int64_t ldr, double* Yrm, int64_t ldyr) {
     const bool dual = W != nullptr && lam != nullptr && (res_count > 0 || R32 != nullptr);
     if (!dual) {
         res_count = 0;
@@ -423,14 +508,35 @@ rc_status xt2(rc_ctx* ctx, int64_t n, int64_t k, int64_t nc, const double* X, in
     }
     const bool v16 =
         ((uintptr_t)X % 16 == 0) && (ldx % 2 == 0) && (!dual || (((uintptr_t)W % 16 == 0) && ldw % 2 == 0));
+    if (Yrm && (dual || ldyr % 2 != 0 || (uintptr_t)Yrm % 16 != 0))
+        return rc_fail(ctx, RC_ERR_INVALID, "xt2: the row-major copy needs the plain product and an even leading dimension");
+    if (!dual) {
+        const int64_t pt = (n + XP_RT - 1) / XP_RT;
+        const unsigned pg = (unsigned)std::max<int64_t>(1, std::min<int64_t>(pt, ctx->sm_count));
+        const size_t psm = ((size_t)nh * 48 * xm_kpt((int)k) + (size_t)2 * ((k + 3) / 4 * 4) * XP_RP) * sizeof(double);
+#define RC_XP(NHV, VV)                                                                                            \
+    do {                                                                                                          \
+        RC_CU(ctx, allow_max_smem(ctx, xt_mma_plain_kernel<NHV, VV>));                                            \
+        xt_mma_plain_kernel<NHV, VV><<<pg, 128 * NHV, psm, ctx->stream>>>(n, (int)k, (int)nc, X, ldx, T, ldt, Y, ldy, \
+                                                                          Yrm, ldyr);                            \
+    } while (0)
+        if (nh == 1) {
+            if (v16) RC_XP(1, true); else RC_XP(1, false);
+        } else {
+            if (v16) RC_XP(2, true); else RC_XP(2, false);
+        }
+#undef RC_XP
+        ctx->launches++;
+        RC_CU(ctx, cudaGetLastError());
+        return RC_OK;
+    }
 #define RC_XM(NHV, DV)                                                                                            \
     (v16 ? xt_mma_launch<NHV, DV, true>(ctx, grid, n, k, nc, X, ldx, T, ldt, Y, ldy, W, ldw, lam, dual_cols,      \
                                         res_count, rpart, R32, ldr)                                               \
          : xt_mma_launch<NHV, DV, false>(ctx, grid, n, k, nc, X, ldx, T, ldt, Y, ldy, W, ldw, lam, dual_cols,     \
                                          res_count, rpart, R32, ldr))
     rc_status st;
-    if (dual) st = nh == 1 ? RC_XM(1, true) : RC_XM(2, true);
-    else st = nh == 1 ? RC_XM(1, false) : RC_XM(2, false);
+    st = nh == 1 ? RC_XM(1, true) : RC_XM(2, true);
 #undef RC_XM
     RC_TRY(st);
     ctx->launches++;

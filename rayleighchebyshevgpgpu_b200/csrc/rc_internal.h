@@ -34,6 +34,11 @@ struct rc_ctx {
     // CSR step kernel: 0 auto (register-cached rows when every row has <= 8 entries),
     // 1 row loop, 2 register-cached rows. Read from RCB200_CSR_KERNEL at context creation.
     int csr_variant = 0;
+    // Column-major operator steps and residual blocks (W = A V, R = A Y - Y diag(lam)): columns per
+    // chunk (0 = all) and chunk order (0: chunk index slowest, one sweep down the rows per chunk;
+    // 1: chunk index fastest). RCB200_CM_CPT, RCB200_CM_ORDER.
+    int cm_cpt = 0;
+    int cm_order = 0;
     // L2 prefetch distance (rows) of the row-major filter steps; 0 = off. RCB200_PF_ROWS.
     int64_t pf_rows = 0;
     // 16-byte slices per thread in the row-major filter steps: 0 = by storage precision (two
@@ -58,7 +63,7 @@ struct rc_ctx {
 
 enum Slot {
     S_V = 0, S_W, S_T1, S_T2, S_FOUND, S_PART, S_SMALL, S_LANCZOS, S_RPART, S_IO, S_CB, S_EIG, S_FA, S_FB,
-    S_R32, S_CORR, S_COUNT
+    S_R32, S_CORR, S_YRM, S_COUNT
 };
 
 struct rc_op {
@@ -186,6 +191,8 @@ struct XtArgs {
     // optional: the residual block X2 T - Y diag(lam) (all nc columns) in row-major FP32 with
     // leading dimension ldr (real blocks with k, nc <= 96 only)
     float* R32 = nullptr; int64_t ldr = 0;
+    // optional: a row-major FP64 copy of Y (plain products, real blocks with k, nc <= 96)
+    double* Yrm = nullptr; int64_t ldyr = 0;
 };
 rc_status xt(rc_ctx* ctx, int dtype, const XtArgs& a);
 
@@ -198,7 +205,15 @@ rc_status gram2(rc_ctx* ctx, int64_t n, int64_t m, const double* X, int64_t ldx,
 bool xt2_supported(int dtype, int64_t k, int64_t nc);
 rc_status xt2(rc_ctx* ctx, int64_t n, int64_t k, int64_t nc, const double* X, int64_t ldx, const double* T,
               int64_t ldt, double* Y, int64_t ldy, const double* W, int64_t ldw, const double* lam, int64_t res_count,
-              double* res, float* R32 = nullptr, int64_t ldr = 0);
+              double* res, float* R32 = nullptr, int64_t ldr = 0, double* Yrm = nullptr, int64_t ldyr = 0);
+
+// Residual block of Ritz vectors on native real operators (rc_resid.cu): R = A Y - Y diag(lam)
+// from the row-major FP64 copy Yrm of Y (leading dimension rm_leading_dim(RC_REAL64, P64, s)),
+// its column norms ||R_c|| for c < res_count into res (device), and with R32 the row-major FP32
+// copy of R (leading dimension rm_leading_dim(RC_REAL64, P32, s)). One pass over Yrm.
+bool resid_supported(const rc_op* op, int64_t s);
+rc_status resid_block(rc_ctx* ctx, const rc_op* op, const double* Yrm, int64_t ld, int64_t s, const double* lam,
+                      int64_t res_count, double* res, float* R32, int64_t ldr);
 
 // Cholesky factor of Gram G (s x s) with diagonal scaling, shift on breakdown;
 // writes Tout = D^-1 R^-1 (upper). flags (device int[4]): [0] shifted, [1] failed, [2] zero column.

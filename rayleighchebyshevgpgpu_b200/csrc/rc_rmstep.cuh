@@ -173,6 +173,123 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
     }
 }
 
+// The 27-point stencil (every neighbour weight offd) with the box sum reused along x:
+//   (A x)_i = (diag_i - offd) x_i + offd S_i,  S_i = Q(i-1) + Q(i) + Q(i+1),
+// where Q(j) is the sum of x over the 3x3 cross-section (y, z neighbours, Dirichlet) of row j.
+// Each thread walks `run` consecutive rows, so Q(i+1) is the only new cross-section per row:
+// 9 gathers per row instead of 27 (the per-row form is bound by L1 throughput). Thread (r, seg)
+// of a CTA takes rows cta*rows_per_iter*run + r*run .. + run, the CTA a contiguous range.
+// The sums are formed in a different order than rm_step_rows (a rounding-level difference).
+template <class TD, class TS, class TC, int W, class IX, bool SRC>
+__device__ __forceinline__ void rm_step_rows27(const StencilRows<TD, TC, 27>& op, int64_t n, int nseg, int64_t ld,
+                                               int run, int64_t cta, const TS* __restrict__ x, const TS* z, TS* y,
+                                               TC alpha, TC beta, TC gamma, int64_t pf_z, int64_t pf_x,
+                                               const TS* __restrict__ src, const float* __restrict__ sig) {
+    constexpr int V = Pack16<TS>::V;
+    const int rows_per_iter = blockDim.x / nseg;
+    const int rloc = threadIdx.x / nseg;
+    if (rloc >= rows_per_iter) return;
+    const IX off = (IX)(threadIdx.x - rloc * nseg) * (IX)V;
+    const IX wstride = (IX)nseg * (IX)V;
+    const IX ldx = (IX)ld;
+    TC sg[SRC ? W * V : 1];
+    if (SRC) {
+#pragma unroll
+        for (int w = 0; w < W; ++w)
+#pragma unroll
+            for (int v = 0; v < V; ++v) sg[w * V + v] = s_from<TC>((double)__ldg(sig + off + w * wstride + v), 0.0);
+    }
+    const int64_t nx = op.nx, ny = op.ny, nz = op.nz, sy = nx, sz = nx * ny;
+    const TC woff = s_from<TC>(op.offd, 0.0);
+    const int64_t i0 = (cta * rows_per_iter + rloc) * (int64_t)run;
+    const int64_t i1 = min(n, i0 + run);
+    // cross-section sum of row j (same y, z as row i) for this thread's slices
+    auto cross = [&](int64_t j, bool vym, bool vyp, bool vzm, bool vzp, TC (&q)[W * V]) {
+#pragma unroll
+        for (int v = 0; v < W * V; ++v) q[v] = s_zero(TC());
+#pragma unroll
+        for (int dz = -1; dz <= 1; ++dz) {
+            const bool vz = dz < 0 ? vzm : (dz > 0 ? vzp : true);
+#pragma unroll
+            for (int dy = -1; dy <= 1; ++dy) {
+                const bool vy = dy < 0 ? vym : (dy > 0 ? vyp : true);
+                if (vz && vy) {
+                    const TS* xj = x + ((IX)(j + dy * sy + dz * sz) * ldx + off);
+#pragma unroll
+                    for (int w = 0; w < W; ++w) {
+                        const Pack16<TS> pk = ld16_ro(xj + w * wstride);
+#pragma unroll
+                        for (int v = 0; v < V; ++v) q[w * V + v] = s_add(q[w * V + v], s_cvt<TC>(pk.v[v]));
+                    }
+                }
+            }
+        }
+    };
+    TC qm[W * V], q0[W * V], qp[W * V];
+    for (int64_t i = i0; i < i1; ++i) {
+        const int64_t ix = i % nx, t = i / nx, iy = t % ny, iz = t / ny;
+        const bool vym = iy > 0, vyp = iy + 1 < ny, vzm = iz > 0, vzp = iz + 1 < nz;
+        if (i == i0 || ix == 0) {  // (re)start the window at the run's first row or a new x-line
+            if (ix > 0) cross(i - 1, vym, vyp, vzm, vzp, qm);
+            else
+#pragma unroll
+                for (int v = 0; v < W * V; ++v) qm[v] = s_zero(TC());
+            cross(i, vym, vyp, vzm, vzp, q0);
+        }
+        if (ix + 1 < nx) cross(i + 1, vym, vyp, vzm, vzp, qp);
+        else
+#pragma unroll
+            for (int v = 0; v < W * V; ++v) qp[v] = s_zero(TC());
+        const IX oi = (IX)i * ldx + off;
+        if (pf_z > 0 && i + pf_z < n) {
+#pragma unroll
+            for (int w = 0; w < W; ++w) {
+                if ((((off + w * wstride) * (IX)sizeof(TS)) & 127) != 0) continue;
+                if (z) prefetch_l2(z + (IX)(i + pf_z) * ldx + off + w * wstride);
+                if (SRC) prefetch_l2(src + (IX)(i + pf_z) * ldx + off + w * wstride);
+                if (i + pf_x < n) prefetch_l2(x + (IX)(i + pf_x) * ldx + off + w * wstride);
+            }
+        }
+        const TC dmw = s_sub(s_from<TC>((double)op.diag[i], 0.0), woff);
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            const IX o = oi + w * wstride;
+            const Pack16<TS> xi = ld16_ro(x + o);
+            Pack16<TS> zi{}, si{};
+            if (z) zi = ld16(z + o);
+            if (SRC) si = ld16_ro(src + o);
+            Pack16<TS> out;
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                const int e = w * V + v;
+                const TC xv = s_cvt<TC>(xi.v[v]);
+                const TC ax = s_fma(woff, s_add(s_add(qm[e], q0[e]), qp[e]), s_mul(dmw, xv));
+                TC r = s_mul(alpha, ax);
+                r = s_fma(beta, xv, r);
+                if (z) r = s_fma(gamma, s_cvt<TC>(zi.v[v]), r);
+                if (SRC) r = s_fma(sg[e], s_cvt<TC>(si.v[v]), r);
+                out.v[v] = s_cvt<TS>(r);
+            }
+            st16(y + o, out);
+        }
+#pragma unroll
+        for (int v = 0; v < W * V; ++v) {
+            qm[v] = q0[v];
+            q0[v] = qp[v];
+        }
+    }
+}
+
+template <class P> struct IsStencil27 {
+    static constexpr bool value = false;
+    using diag_t = float;
+};
+template <class TD, class TC> struct IsStencil27<StencilRows<TD, TC, 27>> {
+    static constexpr bool value = true;
+    using diag_t = TD;
+};
+constexpr int kRun27 = 16;  // consecutive rows per thread in rm_step_rows27
+
 // Layout change between the caller's column-major FP64 block and the row-major scratch, through
 // 32x32 shared-memory tiles (coalesced on both sides), converting precision and scaling.
 //   to_rm:  R[i*ld + c] = (TS) V[i + c*ldv]

@@ -153,6 +153,8 @@ int64_t solve_footprint(const rc_op* op, const rc_solve_params& p, int sm_count)
     t += round_2m(3 * n * esz + sq * sq * esz + 4096);                // Lanczos vectors / small QR
     t += round_2m(4 * sq * sq * esz + 1024) + round_2m(2 * (sq + 1) * (sq + 1) * esz + 4096);  // cholqr, Jacobi
     if (op->kind == 2) t += round_2m(n * ss * esz);                   // callback step scratch
+    if (rcb::resid_supported(op, ss))                                 // row-major copy of the Ritz vectors
+        t += round_2m(n * rcb::rm_leading_dim(op->dtype, P64, ss) * 8);
     if (p.precision == RC_PREC_MIXED && p.mixed_refine == 0 && rcb::rm_corr_supported(op, ss)) {
         // correction filter: the FP32 residual block and the coefficient table
         const int64_t ld32 = rcb::rm_leading_dim(op->dtype, P32, ss);

@@ -63,6 +63,7 @@ private:
     rc_status rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool read_back, float* R32 = nullptr);
     rc_status rr_fused(int64_t s, int64_t res_count, bool* ok, float* R32 = nullptr);
     rc_status r32_block(int64_t s, float** out);
+    rc_status ritz_and_residuals(XtArgs a, int64_t s, int64_t res_count, float* R32);
     rc_status lanczos(int which, double tol, double* lmin, double* lmax);
     void tic(int ph);
     void toc(int ph);
@@ -220,6 +221,37 @@ rc_status Solver::ortho(int64_t s) {
 
 // Rayleigh-Ritz on orthonormal X (n x s): AX = A X, H = X^H AX, H = Q L Q^H,
 // X <- X Q, AX <- AX Q, residuals of the first res_count columns; results read to the host.
+// Ritz vectors Y = X Q (a.Y) and the residuals of their first res_count columns (dres_), plus
+// the FP32 residual block when R32 is given. Native real operators with s <= 96: Y by the GEMM,
+// which also writes a row-major copy, then R = A Y - Y diag(lam) in one pass over that copy
+// (rc_resid.cu). Otherwise (complex or callback operators, wider blocks): the dual GEMM (A X) Q
+// with the residual norms reduced on the fly.
+rc_status Solver::ritz_and_residuals(XtArgs a, int64_t s, int64_t res_count, float* R32) {
+    if (resid_supported(op_, s) && xt2_supported(dtype_, a.k, a.nc)) {
+        const int64_t ldrm = rm_leading_dim(RC_REAL64, P64, s);
+        void* yrm = nullptr;
+        RC_TRY(rc_slot(ctx_, S_YRM, (size_t)n_ * ldrm * sizeof(double), &yrm));
+        a.X2 = nullptr;
+        a.Y2 = nullptr;
+        a.lam = nullptr;
+        a.res_count = 0;
+        a.Yrm = (double*)yrm;
+        a.ldyr = ldrm;
+        RC_TRY(xt(ctx_, dtype_, a));
+        return resid_block(ctx_, op_, (const double*)yrm, ldrm, s, dlam_, res_count, dres_, R32,
+                           R32 ? rm_leading_dim(RC_REAL64, P32, s) : 0);
+    }
+    a.Y2 = nullptr;  // only the residual norms of (A X) Q are needed
+    a.lam = dlam_;
+    a.res_count = res_count;
+    a.res = dres_;
+    if (R32) {
+        a.R32 = R32;
+        a.ldr = rm_leading_dim(RC_REAL64, P32, s);
+    }
+    return xt(ctx_, dtype_, a);
+}
+
 rc_status Solver::r32_block(int64_t s, float** out) {
     void* p = nullptr;
     RC_TRY(rc_slot(ctx_, S_R32, (size_t)n_ * rm_leading_dim(RC_REAL64, P32, s) * sizeof(float), &p));
@@ -242,13 +274,7 @@ rc_status Solver::rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool rea
     a.T = Q_; a.ldt = s;
     a.Y = T1_; a.ldy = n_;
     a.X2 = AX; a.ldx2 = n_;
-    a.Y2 = nullptr;  // only the residual norms of (A X) Q are needed
-    a.lam = dlam_; a.res_count = res_count; a.res = dres_;
-    if (R32) {
-        a.R32 = R32;
-        a.ldr = rm_leading_dim(RC_REAL64, P32, s);
-    }
-    RC_TRY(xt(ctx_, dtype_, a));
+    RC_TRY(ritz_and_residuals(a, s, res_count, R32));
     std::swap(X, T1_);
     if (read_back) {
         RC_CU(ctx_, cudaMemcpyAsync(hbuf_, dlam_, s * sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
@@ -297,13 +323,7 @@ rc_status Solver::rr_fused(int64_t s, int64_t res_count, bool* ok, float* R32) {
     a.T = Q_; a.ldt = s;
     a.Y = T1_; a.ldy = n_;
     a.X2 = W_; a.ldx2 = n_;
-    a.Y2 = nullptr;  // only the residual norms of W Q are needed
-    a.lam = dlam_; a.res_count = res_count; a.res = dres_;
-    if (R32) {
-        a.R32 = R32;
-        a.ldr = rm_leading_dim(RC_REAL64, P32, s);
-    }
-    RC_TRY(xt(ctx_, dtype_, a));
+    RC_TRY(ritz_and_residuals(a, s, res_count, R32));
     RC_CU(ctx_, cudaMemcpyAsync(hbuf_, dlam_, s * sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
     if (res_count > 0)
         RC_CU(ctx_, cudaMemcpyAsync(hbuf_ + s, dres_, res_count * sizeof(double), cudaMemcpyDeviceToHost,
