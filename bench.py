@@ -386,7 +386,7 @@ def run_ours(args):
                                                            "time_ortho_ms", "time_eigenvalue_ms")} if info64 else None},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "peak_source": peak_src, "kernel": "rm_step_kernel (fused filter degree-step, CSR)",
+                     "peak_source": peak_src, "kernel": "rm_step_kernel + rm_step_src_kernel (fused filter degree-steps, CSR)",
                      "algorithmic_bytes_per_launch": alg_bytes / fsteps if fsteps else None,
                      "launches": fsteps, "fp64_launches": f64steps, "correction_launches": csteps,
                      "bytes_per_launch_fp32": bytes_fp32_step, "bytes_per_launch_correction": bytes_corr_step,

@@ -5,7 +5,9 @@
 // call exit(), cudaErrchk.h:8-51).
 #include <cstdio>
 #include <cstdlib>
+#include <cmath>
 #include <cstring>
+#include <vector>
 #include <new>
 #include <string>
 #include "rc_common.cuh"
@@ -97,6 +99,8 @@ static void op_release(rc_op* op) {
     if (op->vals32) cudaFree(op->vals32);
     if (op->diag64) cudaFree(op->diag64);
     if (op->diag32) cudaFree(op->diag32);
+    if (op->phase64) cudaFree(op->phase64);
+    if (op->phase32) cudaFree(op->phase32);
     delete op;
 }
 
@@ -264,6 +268,19 @@ rc_status rc_op_stencil_create(rc_ctx* ctx, int dtype, int kind, int64_t nx, int
     op->offdiag = offdiag;
     op->flux = dtype == RC_COMPLEX128 ? flux : 0.0;
     rc_status st = dev_copy(ctx, (void**)&op->diag64, diag, (size_t)op->n * 8, op);
+    if (st == RC_OK && dtype == RC_COMPLEX128) {
+        std::vector<double> p64((size_t)2 * nx);
+        std::vector<float> p32((size_t)2 * nx);
+        const double theta = 2.0 * 3.14159265358979323846 * op->flux;
+        for (int64_t x = 0; x < nx; ++x) {
+            p64[2 * x] = std::cos(theta * (double)x);
+            p64[2 * x + 1] = std::sin(theta * (double)x);
+            p32[2 * x] = (float)p64[2 * x];
+            p32[2 * x + 1] = (float)p64[2 * x + 1];
+        }
+        st = dev_copy(ctx, &op->phase64, p64.data(), p64.size() * sizeof(double), op);
+        if (st == RC_OK) st = dev_copy(ctx, &op->phase32, p32.data(), p32.size() * sizeof(float), op);
+    }
     if (st != RC_OK) {
         rc_op_destroy(op);
         return st;

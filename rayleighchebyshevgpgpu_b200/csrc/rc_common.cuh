@@ -63,6 +63,8 @@ RC_HD float2 s_rscale(float r, float2 a) { return make_float2(r * a.x, r * a.y);
 
 RC_HD double s_conj(double a) { return a; }
 RC_HD double2 s_conj(double2 a) { return make_double2(a.x, -a.y); }
+RC_HD float s_conj(float a) { return a; }
+RC_HD float2 s_conj(float2 a) { return make_float2(a.x, -a.y); }
 RC_HD double s_abs2(double a) { return a * a; }
 RC_HD float s_abs2(float a) { return a * a; }
 RC_HD double s_abs2(double2 a) { return a.x * a.x + a.y * a.y; }

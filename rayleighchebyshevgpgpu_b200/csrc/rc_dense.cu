@@ -485,6 +485,11 @@ __device__ __forceinline__ void rr_pair(int r, int i, int M, int sp, int& p, int
     }
 }
 
+// Threads of the one-CTA Jacobi (a multiple of 32, at most 1024).
+#ifndef RC_JACOBI_THREADS
+#define RC_JACOBI_THREADS 1024
+#endif
+
 template <class T>
 __global__ void __launch_bounds__(1024)
 jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __restrict__ evals, int* info,
@@ -690,12 +695,12 @@ rc_status small_eigh_work(rc_ctx* ctx, int dtype, int64_t s, void* A, void* Q, d
     if (dtype == RC_COMPLEX128) {
         if (dyn > 48 * 1024)
             RC_CU(ctx, allow_max_smem(ctx, jacobi_kernel<double2>));
-        jacobi_kernel<double2><<<1, 1024, dyn, ctx->stream>>>((int)s, (const double2*)A, (double2*)Q, evals, info,
+        jacobi_kernel<double2><<<1, RC_JACOBI_THREADS, dyn, ctx->stream>>>((int)s, (const double2*)A, (double2*)Q, evals, info,
                                                               (double2*)work, fit ? 1 : 0, sweeps);
     } else {
         if (dyn > 48 * 1024)
             RC_CU(ctx, allow_max_smem(ctx, jacobi_kernel<double>));
-        jacobi_kernel<double><<<1, 1024, dyn, ctx->stream>>>((int)s, (const double*)A, (double*)Q, evals, info,
+        jacobi_kernel<double><<<1, RC_JACOBI_THREADS, dyn, ctx->stream>>>((int)s, (const double*)A, (double*)Q, evals, info,
                                                              (double*)work, fit ? 1 : 0, sweeps);
     }
     ctx->launches++;

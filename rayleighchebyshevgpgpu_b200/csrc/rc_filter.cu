@@ -18,6 +18,7 @@
 // coalesced 128-byte (FP32) or 256-byte (FP64) segment.
 #include <cstdio>
 #include <string>
+#include <type_traits>
 #include "rc_common.cuh"
 #include "rc_internal.h"
 
@@ -32,6 +33,16 @@ template <> struct Stor<P64, true> { using type = double2; };
 template <> struct Stor<P32, true> { using type = float2; };
 
 constexpr int kStepThreads = 256;
+// Resident CTAs per SM the register budget of the real FP64 register-cached CSR step must allow: 4 (64
+// registers). W = A V on 128^3 x 96 FP64 takes 1.17 ms at 4, 1.64 ms at 3 and 1.45 ms unbounded.
+// The other scalar types (wider column chunks, complex) would spill at 64 and stay unbounded.
+#ifndef RC_CM_MIN_BLOCKS
+#define RC_CM_MIN_BLOCKS 4
+#endif
+template <class TC>
+constexpr int cm_min_blocks() {
+    return std::is_same<TC, double>::value ? RC_CM_MIN_BLOCKS : 1;
+}
 
 // ---------------------------------------------------------------------------------------
 // CSR step
@@ -79,7 +90,7 @@ csr_step_kernel(int64_t n, int64_t s, const int32_t* __restrict__ rowptr, const 
 // registers (padded with (i, 0)), so the MAXR x CB gathers of a column chunk are independent
 // loads the hardware keeps in flight together.
 template <class TA, class TX, class TZ, class TY, class TC, int CB, int MAXR>
-__global__ void __launch_bounds__(kStepThreads)
+__global__ void __launch_bounds__(kStepThreads, cm_min_blocks<TC>())
 csr_step_reg_kernel(int64_t n, int64_t s, const int32_t* __restrict__ rowptr, const int32_t* __restrict__ colind,
                     const TA* __restrict__ vals, const TX* __restrict__ x, int64_t ldx, const TZ* z, int64_t ldz,
                     TY* y, int64_t ldy, TC alpha, TC beta, TC gamma, real_t<TC> scale) {

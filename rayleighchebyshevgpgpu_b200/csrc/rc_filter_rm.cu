@@ -245,10 +245,12 @@ static rc_status rm_filter_dispatch(rc_ctx* ctx, rc_op* op, void* V, int64_t ldv
     }
     if (op->skind == 7) {
         StencilRows<TD, TC, 7> pol{op->nx, op->ny, op->nz, dg, op->offdiag, theta};
+        pol.ph = (const TC*)(sizeof(TD) == 8 ? op->phase64 : op->phase32);
         return run_rm_select<StencilRows<TD, TC, 7>, TS, TC>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld,
                                                              band);
     }
     StencilRows<TD, TC, 5> pol{op->nx, op->ny, op->nz, dg, op->offdiag, theta};
+    pol.ph = (const TC*)(sizeof(TD) == 8 ? op->phase64 : op->phase32);
     return run_rm_select<StencilRows<TD, TC, 5>, TS, TC>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band);
 }
 

@@ -86,6 +86,10 @@ struct rc_op {
     float* diag32 = nullptr;
     double offdiag = 0.0;
     double flux = 0.0;
+    // complex stencils: the Peierls phase exp(i 2 pi flux x) for x = 0..nx-1, as double2 and
+    // float2, so the kernels look it up instead of evaluating sincos per row
+    void* phase64 = nullptr;
+    void* phase32 = nullptr;
     // callback
     rc_block_apply_fn fn = nullptr;
     void* user = nullptr;

@@ -59,6 +59,7 @@ struct StencilRows {
     const TD* __restrict__ diag;
     double offd;
     double theta;
+    const TC* ph = nullptr;  // complex: phase table exp(i theta x), x < nx (else evaluated per row)
     template <class F>
     __device__ __forceinline__ void row(int64_t i, F&& f) const {
         const int64_t ix = i % nx;
@@ -85,15 +86,17 @@ struct StencilRows {
             }
         } else {
             if (KIND == 7 && iz > 0) f(i - sz, w);
+            TC p = s_zero(TC());
+            if (IsComplex<TC>::value) p = ph ? ph[ix] : unit_phase<TC>(theta * (double)ix, false);
             if (IsComplex<TC>::value) {
-                if (iy > 0) f(i - sy, s_mul(w, unit_phase<TC>(theta * (double)ix, false)));
+                if (iy > 0) f(i - sy, s_mul(w, p));
             } else {
                 if (iy > 0) f(i - sy, w);
             }
             if (ix > 0) f(i - 1, w);
             if (ix + 1 < nx) f(i + 1, w);
             if (IsComplex<TC>::value) {
-                if (iy + 1 < ny) f(i + sy, s_mul(w, unit_phase<TC>(theta * (double)ix, true)));
+                if (iy + 1 < ny) f(i + sy, s_mul(w, s_conj(p)));
             } else {
                 if (iy + 1 < ny) f(i + sy, w);
             }
