@@ -134,6 +134,61 @@ class CsrOperator(Operator):
         return self
 
 
+    @classmethod
+    def from_matrix_market(cls, ctx: Context, path: str) -> "CsrOperator":
+        """Create from a Matrix Market coordinate file (read_matrix_market)."""
+        rowptr, colind, vals = read_matrix_market(path)
+        return cls(ctx, rowptr, colind, vals)
+
+
+def read_matrix_market(path: str):
+    """CSR arrays (rowptr int32, colind int32, vals float64 or complex128) of a square Matrix Market
+    'coordinate' file with real, integer or complex entries and general, symmetric or hermitian
+    storage. Symmetric and hermitian files store one triangle; the other is filled in (the
+    conjugate for hermitian). Duplicate entries are summed; each row's columns come out sorted."""
+    with open(path) as f:
+        header = f.readline().split()
+        if len(header) < 5 or header[0] != "%%MatrixMarket" or header[1].lower() != "matrix":
+            raise ValueError(f"{path}: not a Matrix Market matrix file")
+        fmt, field, symm = header[2].lower(), header[3].lower(), header[4].lower()
+        if fmt != "coordinate":
+            raise ValueError(f"{path}: only the coordinate format is supported")
+        if field not in ("real", "integer", "complex", "double"):
+            raise ValueError(f"{path}: unsupported field {field}")
+        if symm not in ("general", "symmetric", "hermitian"):
+            raise ValueError(f"{path}: unsupported symmetry {symm}")
+        line = f.readline()
+        while line.startswith("%") or not line.strip():
+            line = f.readline()
+        nr, nc, nnz = (int(t) for t in line.split()[:3])
+        if nr != nc:
+            raise ValueError(f"{path}: the operator must be square ({nr} x {nc})")
+        data = np.loadtxt(f, ndmin=2, max_rows=nnz) if nnz > 0 else np.zeros((0, 4))
+    if data.shape[0] != nnz:
+        raise ValueError(f"{path}: expected {nnz} entries, read {data.shape[0]}")
+    i = data[:, 0].astype(np.int64) - 1
+    j = data[:, 1].astype(np.int64) - 1
+    complex_ = field == "complex"
+    v = data[:, 2] + 1j * data[:, 3] if complex_ else data[:, 2].astype(np.float64)
+    if symm != "general":
+        off = i != j
+        vt = np.conj(v[off]) if symm == "hermitian" else v[off]
+        i, j, v = np.concatenate([i, j[off]]), np.concatenate([j, i[off]]), np.concatenate([v, vt])
+    order = np.lexsort((j, i))
+    i, j, v = i[order], j[order], v[order]
+    if i.size:  # sum duplicates
+        key = i * nr + j
+        first = np.concatenate([[True], key[1:] != key[:-1]])
+        groups = np.cumsum(first) - 1
+        v = np.bincount(groups, weights=v.real, minlength=groups[-1] + 1) + (
+            1j * np.bincount(groups, weights=v.imag, minlength=groups[-1] + 1) if complex_ else 0.0)
+        i, j = i[first], j[first]
+    rowptr = np.zeros(nr + 1, dtype=np.int64)
+    np.add.at(rowptr, i + 1, 1)
+    rowptr = np.cumsum(rowptr).astype(np.int32)
+    return rowptr, j.astype(np.int32), (v.astype(np.complex128) if complex_ else v.astype(np.float64))
+
+
 class StencilOperator(Operator):
     """Matrix-free 5/7/27-point stencil with a diagonal array (Dirichlet boundaries)."""
 

@@ -183,3 +183,33 @@ def test_problem_generators_hermitian_and_sizes():
     # nnz of the 7-point 128^3 operator of configuration 2: n*7 - 6*128^2
     assert 128 ** 3 * 7 - 6 * 128 ** 2 == 14581760
     assert problems.block_sizes(64) == (64, 32) and problems.block_sizes(16) == (16, 8)
+
+
+def test_matrix_market_reader_symmetric_hermitian_general(tmp_path):
+    """Operator ingestion: Matrix Market coordinate files become the CSR arrays of rc_op_csr_create."""
+    from rayleighchebyshevgpgpu_b200.runtime import read_matrix_market
+    rng = np.random.default_rng(0)
+    n = 7
+    B = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    for field, symm, M in (("real", "symmetric", (B + B.T).real),
+                           ("complex", "hermitian", B + B.conj().T),
+                           ("real", "general", (B + B.T).real)):
+        M = M * (np.abs(M) > 0.8)  # sparse pattern
+        np.fill_diagonal(M, np.diag(M) + 5.0)
+        entries = [(r, c, M[r, c]) for r in range(n) for c in range(n)
+                   if M[r, c] != 0 and (symm == "general" or r >= c)]
+        path = tmp_path / f"{symm}.mtx"
+        with open(path, "w") as f:
+            f.write(f"%%MatrixMarket matrix coordinate {field} {symm}\n% test\n{n} {n} {len(entries)}\n")
+            for r, c, v in entries:
+                if field == "complex":
+                    f.write(f"{r + 1} {c + 1} {float(v.real)!r} {float(v.imag)!r}\n")
+                else:
+                    f.write(f"{r + 1} {c + 1} {float(v.real)!r}\n")
+        rp, ci, vals = read_matrix_market(str(path))
+        D = np.zeros((n, n), dtype=vals.dtype)
+        for r in range(n):
+            for k in range(rp[r], rp[r + 1]):
+                D[r, ci[k]] = vals[k]
+            assert np.all(np.diff(ci[rp[r]:rp[r + 1]]) > 0)
+        np.testing.assert_array_equal(D, M if field == "complex" else M.real)

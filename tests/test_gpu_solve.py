@@ -94,22 +94,25 @@ def test_mixed_correction_filter_matches_fp64(ctx, kind, dims, k):
         op.close()
 
 
-def test_multipass_deflation_incr_smaller_than_k(ctx):
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_multipass_deflation_incr_smaller_than_k(ctx, precision):
     Q = problems.small_laplacian((24, 24), seed=5)
     A = O.csr_matrix(*Q.csr())
     op = R.operator_from_problem(ctx, Q, "csr")
-    res = _solve(ctx, op, Q, 12, 1e-10, incr=4, buffer=8)
+    res = _solve(ctx, op, Q, 12, 1e-10, precision, incr=4, buffer=8)
     assert res.info["outer_passes"] >= 3
     _check_pairs(A, res, 12, 1e-10)
 
 
-def test_interval_mode_finds_all_below_lambda_max(ctx):
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_interval_mode_finds_all_below_lambda_max(ctx, precision):
     Q = problems.small_laplacian((20, 20), seed=6)
     A = O.csr_matrix(*Q.csr())
     dense = np.linalg.eigvalsh(A.toarray())
     lam = 0.5 * (dense[9] + dense[10])  # exactly 10 eigenvalues below
     op = R.operator_from_problem(ctx, Q, "csr")
-    p = R.make_params(4, 1e-10, incr=4, buffer=8, stop="RESIDUAL_ONLY", mode=2, lambda_max=lam)
+    p = R.make_params(4, 1e-10, incr=4, buffer=8, precision=precision, stop="RESIDUAL_ONLY", mode=2,
+                      lambda_max=lam)
     p.eig_count = Q.n
     res = R.solve(ctx, op, p, host=True)
     np.testing.assert_allclose(np.sort(res.evals), dense[:10], rtol=1e-9)
