@@ -313,7 +313,8 @@ def run_ours(args):
     # ---- roofline of the dominant kernel: the fused filter degree-step (rm_step_kernel) ----
     # Algorithmic bytes of one degree-step over the n x s block: the matrix once (values + column
     # indices + row pointers) and three block passes (read x_{k-1}, read x_{k-2}, write x_k); the
-    # correction filter's step (rm_step_src_kernel) also reads the residual block: four passes.
+    # correction filter's step (rm_step_src_kernel) also reads the residual block: four passes of
+    # its storage type (bfloat16 or FP32, info.correction_element_bytes).
     # The step time is the CUDA-event time of the degree-step launches inside the timed solves
     # (info.time_filter_steps_ms, transposes excluded). Degree-1 filters (column-major path, at
     # most a few per solve) are counted in degree_steps but not timed, a < 0.1 % overstatement.
@@ -321,7 +322,8 @@ def run_ours(args):
     b_a32 = nnz * (4 + 4) + (P.n + 1) * 4
     b_a64 = nnz * (8 + 4) + (P.n + 1) * 4
     bytes_fp32_step = b_a32 + 3 * P.n * s * 4
-    bytes_corr_step = b_a32 + 4 * P.n * s * 4
+    ceb = int(infos[-1].get("correction_element_bytes", 4) or 4)
+    bytes_corr_step = b_a32 + 4 * P.n * s * ceb
     bytes_fp64_step = b_a64 + 3 * P.n * s * 8
     fsteps = sum(i["degree_steps"] for i in infos)
     f64steps = sum(i["fp64_degree_steps"] for i in infos)
@@ -342,8 +344,8 @@ def run_ours(args):
     per_row = profile_dram_bytes_per_row()
     if per_row and fsteps:
         # without a capture of the correction step, its rows count as FP32 rows plus one more
-        # FP32 block row (the residual block)
-        corr_row = per_row.get("corr", per_row["fp32"] + s * 4)
+        # block row (the residual block)
+        corr_row = per_row.get("corr", per_row["fp32"] + s * ceb)
         traffic = P.n * (p32steps * per_row["fp32"] + csteps * corr_row + f64steps * per_row["fp64"]) / fsteps
     # ---- CPU baseline (rank 0, N = 1) ----
     cpu = None

@@ -262,6 +262,8 @@ typedef struct rc_solve_info {
                                       themselves (row-major filter, transposes excluded; phase_timing = 1) */
     int64_t correction_iterations; /* MIXED: inner iterations that ran the FP32 correction filter */
     int64_t correction_degree_steps; /* of degree_steps, those of the correction filter */
+    int64_t correction_element_bytes; /* bytes per stored element of the correction filter's residual
+                                         and recurrence blocks: 2 (bfloat16) or 4 (FP32) */
 } rc_solve_info;
 
 void rc_solve_params_default(rc_solve_params* p);

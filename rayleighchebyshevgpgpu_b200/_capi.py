@@ -94,6 +94,7 @@ class SolveInfo(C.Structure):
         ("time_filter_steps_ms", C.c_double),
         ("correction_iterations", c_i64),
         ("correction_degree_steps", c_i64),
+        ("correction_element_bytes", c_i64),
     ]
 
     def as_dict(self) -> dict:

@@ -29,46 +29,47 @@ rm_step_kernel(Pol op, int64_t n, int nseg, int64_t ld, int groups, const TS* __
                                      pf_x);
 }
 
-// Degree step of the correction filter: y = alpha A x + beta x + gamma z + sig[c] src.
-template <class Pol, class TS, class TC, int W, class IX>
-__global__ void __launch_bounds__(kRmThreads, rm_src_min_blocks())
-rm_step_src_kernel(Pol op, int64_t n, int nseg, int64_t ld, int groups, const TS* __restrict__ x, const TS* z, TS* y,
-                   TC alpha, TC beta, TC gamma, int64_t pf_z, int64_t pf_x, const TS* __restrict__ src,
+// Degree step of the correction filter: y = alpha A x + beta x + gamma z + sig[c] src, with x, z,
+// y and src stored as TM (FP32, or bfloat16 with FP32 arithmetic).
+template <class Pol, class TS, class TC, int W, class IX, class TM>
+__global__ void __launch_bounds__(kRmThreads, rm_src_min_blocks<TM>())
+rm_step_src_kernel(Pol op, int64_t n, int nseg, int64_t ld, int groups, const TM* __restrict__ x, const TM* z, TM* y,
+                   TC alpha, TC beta, TC gamma, int64_t pf_z, int64_t pf_x, const TM* __restrict__ src,
                    const float* __restrict__ sig) {
-    rm_step_rows<Pol, TS, TC, W, IX, true>(op, n, nseg, ld, groups, (int64_t)blockIdx.x, x, z, y, alpha, beta, gamma,
-                                           pf_z, pf_x, src, sig);
+    rm_step_rows<Pol, TS, TC, W, IX, true, TM>(op, n, nseg, ld, groups, (int64_t)blockIdx.x, x, z, y, alpha, beta,
+                                               gamma, pf_z, pf_x, src, sig);
 }
 
 // The 27-point steps with the box sum reused along x (rm_step_rows27).
 // 4 resident CTAs per SM: the three cross-section sums need more than the 40 registers of the
 // per-row steps.
-template <class TD, class TS, class TC, int W, class IX, bool SRC>
-__global__ void __launch_bounds__(kRmThreads, 4)
-rm_step27_kernel(StencilRows<TD, TC, 27> op, int64_t n, int nseg, int64_t ld, const TS* __restrict__ x, const TS* z,
-                 TS* y, TC alpha, TC beta, TC gamma, int64_t pf_z, int64_t pf_x, const TS* __restrict__ src,
+template <class TD, class TS, class TC, int W, class IX, bool SRC, class TM>
+__global__ void __launch_bounds__(kRmThreads, sizeof(TM) == 2 ? 3 : 4)
+rm_step27_kernel(StencilRows<TD, TC, 27> op, int64_t n, int nseg, int64_t ld, const TM* __restrict__ x, const TM* z,
+                 TM* y, TC alpha, TC beta, TC gamma, int64_t pf_z, int64_t pf_x, const TM* __restrict__ src,
                  const float* __restrict__ sig) {
-    rm_step_rows27<TD, TS, TC, W, IX, SRC>(op, n, nseg, ld, kRun27, (int64_t)blockIdx.x, x, z, y, alpha, beta, gamma,
-                                           pf_z, pf_x, src, sig);
+    rm_step_rows27<TD, TS, TC, W, IX, SRC, TM>(op, n, nseg, ld, kRun27, (int64_t)blockIdx.x, x, z, y, alpha, beta,
+                                               gamma, pf_z, pf_x, src, sig);
 }
 
-template <class Pol, class TS, class TC, int W, class IX, bool SRC>
-static void launch_step(rc_ctx* ctx, const Pol& pol, int64_t n, int nseg, int64_t ld, int groups, const TS* x,
-                        const TS* z, TS* y, TC a, TC b, TC g, int64_t pf_z, int64_t pf_x, const TS* src,
+template <class Pol, class TS, class TC, int W, class IX, bool SRC, class TM = TS>
+static void launch_step(rc_ctx* ctx, const Pol& pol, int64_t n, int nseg, int64_t ld, int groups, const TM* x,
+                        const TM* z, TM* y, TC a, TC b, TC g, int64_t pf_z, int64_t pf_x, const TM* src,
                         const float* sig) {
     const int rows_per_iter = kRmThreads / nseg;
     if constexpr (IsStencil27<Pol>::value) {
         using TD = typename IsStencil27<Pol>::diag_t;
         const int64_t rows_per_cta = (int64_t)kRun27 * rows_per_iter;
         const unsigned grid = (unsigned)((n + rows_per_cta - 1) / rows_per_cta);
-        rm_step27_kernel<TD, TS, TC, W, IX, SRC><<<grid, kRmThreads, 0, ctx->stream>>>(pol, n, nseg, ld, x, z, y, a, b,
-                                                                                       g, pf_z, pf_x, src, sig);
+        rm_step27_kernel<TD, TS, TC, W, IX, SRC, TM><<<grid, kRmThreads, 0, ctx->stream>>>(pol, n, nseg, ld, x, z, y, a,
+                                                                                           b, g, pf_z, pf_x, src, sig);
     } else {
         const int64_t rows_per_cta = (int64_t)groups * rows_per_iter;
         const unsigned grid = (unsigned)((n + rows_per_cta - 1) / rows_per_cta);
-        if (SRC)
-            rm_step_src_kernel<Pol, TS, TC, W, IX><<<grid, kRmThreads, 0, ctx->stream>>>(pol, n, nseg, ld, groups, x,
-                                                                                         z, y, a, b, g, pf_z, pf_x,
-                                                                                         src, sig);
+        if constexpr (SRC)
+            rm_step_src_kernel<Pol, TS, TC, W, IX, TM><<<grid, kRmThreads, 0, ctx->stream>>>(pol, n, nseg, ld, groups,
+                                                                                             x, z, y, a, b, g, pf_z,
+                                                                                             pf_x, src, sig);
         else
             rm_step_kernel<Pol, TS, TC, W, IX><<<grid, kRmThreads, 0, ctx->stream>>>(pol, n, nseg, ld, groups, x, z, y,
                                                                                      a, b, g, pf_z, pf_x);
@@ -95,12 +96,12 @@ __global__ void corr_coef_kernel(int64_t s, int64_t ld, int64_t m, double a, dou
     }
 }
 
-template <class TS>
+template <class TM>
 __global__ void __launch_bounds__(256)
-corr_to_cm_kernel(int64_t n, int64_t s, const TS* __restrict__ E, int64_t ld, double* __restrict__ Vc, int64_t ldv,
+corr_to_cm_kernel(int64_t n, int64_t s, const TM* __restrict__ E, int64_t ld, double* __restrict__ Vc, int64_t ldv,
                   const double* __restrict__ coef, double beta) {
-    __shared__ TS tile[32][33];
-    corr_to_cm_tile<TS>(n, s, E, ld, Vc, ldv, coef, beta, (int64_t)blockIdx.x * 32, (int64_t)blockIdx.y * 32, tile);
+    __shared__ float tile[32][33];
+    corr_to_cm_tile<TM>(n, s, E, ld, Vc, ldv, coef, beta, (int64_t)blockIdx.x * 32, (int64_t)blockIdx.y * 32, tile);
 }
 
 
@@ -155,7 +156,7 @@ static rc_status run_rm_filter(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, 
         // k = 1 has no x_{k-2} (gamma = 0): z is not read
         const TS* z = k >= 2 ? y : nullptr;
         launch_step<Pol, TS, TC, W, IX, false>(ctx, pol, n, nseg, ld, groups, xk1, z, y, ta, tb,
-                                               k >= 2 ? tm1 : s_zero(TC()), pf_z, pf_x, nullptr, nullptr);
+                                               k >= 2 ? tm1 : s_zero(TC()), pf_z, pf_x, (const TS*)nullptr, nullptr);
     }
     RC_CU(ctx, cudaGetLastError());
     step_mark(ctx);
@@ -174,13 +175,13 @@ static rc_status run_rm_filter(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, 
 // of the residual), so its FP32 rounding perturbs the filtered block by FP32 rounding times the
 // residual instead of times the block: the subspace keeps converging past the FP32 floor of the
 // plain FP32 filter. e_2 -> A, e_3 -> B (e_1 = R is read as x_{k-2}), then e_k over e_{k-2}.
-template <class Pol, class TS, class TC, int W, class IX>
+template <class Pol, class TS, class TC, int W, class IX, class TM>
 static rc_status run_rm_corr(rc_ctx* ctx, const Pol& pol, int64_t n, double* V, int64_t ldv, int64_t s,
-                             int64_t degree, double a, double b, const TS* R, const float* sig, const double* coef,
-                             TS* A, TS* B, int64_t ld, int64_t band) {
+                             int64_t degree, double a, double b, const TM* R, const float* sig, const double* coef,
+                             TM* A, TM* B, int64_t ld, int64_t band) {
     const int64_t pf_z = ctx->pf_rows;
     const int64_t pf_x = pf_z > 0 ? pf_z + band : 0;
-    constexpr int VEC = Pack16<TS>::V;
+    constexpr int VEC = Slice<TS, TM>::V;  // 8 values per 16-byte slice for bfloat16 blocks
     const TC ta = s_from<TC>(a, 0.0), tb = s_from<TC>(b, 0.0), tm1 = s_from<TC>(-1.0, 0.0);
     if (ld % (VEC * W) != 0) return rc_fail(ctx, RC_ERR_INVALID, "correction filter: leading dimension not padded");
     const int nseg = (int)(ld / (VEC * W));
@@ -189,17 +190,17 @@ static rc_status run_rm_corr(rc_ctx* ctx, const Pol& pol, int64_t n, double* V, 
     const int groups = ctx->rm_groups > 0 ? ctx->rm_groups : (kCsr ? 4 : 8);
     step_mark(ctx);
     for (int64_t k = 2; k <= degree; ++k) {
-        const TS* xk1 = k == 2 ? R : ((k - 1) % 2 == 0 ? A : B);   // e_{k-1}
-        TS* y = k % 2 == 0 ? A : B;                                  // e_k
-        const TS* z = k == 2 ? nullptr : (k == 3 ? R : y);           // e_{k-2}
-        launch_step<Pol, TS, TC, W, IX, true>(ctx, pol, n, nseg, ld, groups, xk1, z, y, ta, tb,
-                                              k == 2 ? s_zero(TC()) : tm1, pf_z, pf_x, R, sig + k * ld);
+        const TM* xk1 = k == 2 ? R : ((k - 1) % 2 == 0 ? A : B);   // e_{k-1}
+        TM* y = k % 2 == 0 ? A : B;                                  // e_k
+        const TM* z = k == 2 ? nullptr : (k == 3 ? R : y);           // e_{k-2}
+        launch_step<Pol, TS, TC, W, IX, true, TM>(ctx, pol, n, nseg, ld, groups, xk1, z, y, ta, tb,
+                                                  k == 2 ? s_zero(TC()) : tm1, pf_z, pf_x, R, sig + k * ld);
     }
     RC_CU(ctx, cudaGetLastError());
     step_mark(ctx);
-    const TS* em = degree == 1 ? R : (degree % 2 == 0 ? A : B);
+    const TM* em = degree == 1 ? R : (degree % 2 == 0 ? A : B);
     const dim3 tgrid((unsigned)((n + 31) / 32), (unsigned)((s + 31) / 32)), tblk(32, 8);
-    corr_to_cm_kernel<TS><<<tgrid, tblk, 0, ctx->stream>>>(n, s, em, ld, V, ldv, coef, a / (double)(degree + 1));
+    corr_to_cm_kernel<TM><<<tgrid, tblk, 0, ctx->stream>>>(n, s, em, ld, V, ldv, coef, a / (double)(degree + 1));
     ctx->launches++;
     RC_CU(ctx, cudaGetLastError());
     return RC_OK;
@@ -256,13 +257,13 @@ static rc_status rm_filter_dispatch(rc_ctx* ctx, rc_op* op, void* V, int64_t ldv
 
 template <class Pol>
 static rc_status rm_corr_select(rc_ctx* ctx, const Pol& pol, int64_t n, double* V, int64_t ldv, int64_t s,
-                                int64_t degree, double a, double b, const float* R, const float* sig,
-                                const double* coef, float* A, float* B, int64_t ld, int64_t band) {
+                                int64_t degree, double a, double b, const rc_corr_t* R, const float* sig,
+                                const double* coef, rc_corr_t* A, rc_corr_t* B, int64_t ld, int64_t band) {
     if ((n + 1) * ld < ((int64_t)1 << 32))
-        return run_rm_corr<Pol, float, float, 1, uint32_t>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B,
-                                                           ld, band);
-    return run_rm_corr<Pol, float, float, 1, int64_t>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld,
-                                                      band);
+        return run_rm_corr<Pol, float, float, 1, uint32_t, rc_corr_t>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig,
+                                                                      coef, A, B, ld, band);
+    return run_rm_corr<Pol, float, float, 1, int64_t, rc_corr_t>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef,
+                                                                 A, B, ld, band);
 }
 
 bool rm_corr_supported(const rc_op* op, int64_t s) {
@@ -271,7 +272,7 @@ bool rm_corr_supported(const rc_op* op, int64_t s) {
 }
 
 rc_status rm_filter_corr(rc_ctx* ctx, rc_op* op, double* V, int64_t ldv, int64_t s, int64_t degree, double a,
-                         double b, const double* lam_dev, const float* R, void* bufA, void* bufB) {
+                         double b, const double* lam_dev, const rc_corr_t* R, void* bufA, void* bufB) {
     if (!rm_corr_supported(op, s)) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "correction filter: unsupported operator");
     if (degree < 1) return RC_OK;
     RC_TRY(ensure_fp32(ctx, op));
@@ -285,8 +286,8 @@ rc_status rm_filter_corr(rc_ctx* ctx, rc_op* op, double* V, int64_t ldv, int64_t
     RC_CU(ctx, cudaGetLastError());
     const int64_t n = op->n;
     const int64_t band = op->kind == 0 ? op->band : (op->skind == 5 ? op->nx : op->nx * op->ny);
-    float* A = (float*)bufA;
-    float* B = (float*)bufB;
+    rc_corr_t* A = (rc_corr_t*)bufA;
+    rc_corr_t* B = (rc_corr_t*)bufB;
     if (op->kind == 0) {
         CsrRows<float, float> pol{op->rowptr, op->colind, (const float*)op->vals32};
         return rm_corr_select(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band);

@@ -1,5 +1,6 @@
 // rc_internal.h -- context/operator structs and kernel launchers shared by the library sources.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <atomic>
@@ -9,6 +10,18 @@
 
 // Storage/compute precision of a block: FP64 (double / c128) or FP32 (float / c64).
 enum { P64 = 0, P32 = 1 };
+
+// Storage of the residual block read by the correction filter: bfloat16 (default) or FP32
+// (RC_CORR_BF16=0). The block only feeds the correction e_k, which is of the size of the residual,
+// so its 8-bit mantissa perturbs the filtered vectors by 2^-9 of a residual-sized term.
+#ifndef RC_CORR_BF16
+#define RC_CORR_BF16 1
+#endif
+#if RC_CORR_BF16
+typedef __nv_bfloat16 rc_corr_t;
+#else
+typedef float rc_corr_t;
+#endif
 
 struct DevBuf {
     void* ptr = nullptr;
@@ -159,12 +172,12 @@ rc_status serve_filter(rc_ctx* ctx, rc_op* op, void* V, int64_t ld, int64_t s, i
                        int prec, void* bufA, void* bufB, size_t buf_bytes, bool* handled);
 // Correction filter (rc_filter_rm.cu), the MIXED precision refinement: V (FP64 column-major,
 // leading dimension ldv) holds Ritz vectors with Ritz values lam_dev (device) and R (row-major
-// FP32, leading dimension rm_leading_dim(RC_REAL64, P32, s)) their residual block A V - V diag(lam);
+// rc_corr_t, leading dimension rm_leading_dim(RC_REAL64, P32, s)) their residual block A V - V diag(lam);
 // V <- P_m(A')V with FP32 storage of the (small) deviation from the scalar recurrence. bufA and
 // bufB: two row-major FP32 blocks of the same size as R.
 bool rm_corr_supported(const rc_op* op, int64_t s);
 rc_status rm_filter_corr(rc_ctx* ctx, rc_op* op, double* V, int64_t ldv, int64_t s, int64_t degree, double a,
-                         double b, const double* lam_dev, const float* R, void* bufA, void* bufB);
+                         double b, const double* lam_dev, const rc_corr_t* R, void* bufA, void* bufB);
 int64_t rm_leading_dim(int dtype, int prec, int64_t s);
 // Build the FP32 (c64) copy of an operator's values/diagonal used by the MIXED filter.
 rc_status ensure_fp32(rc_ctx* ctx, rc_op* op);
@@ -217,7 +230,7 @@ rc_status xt2(rc_ctx* ctx, int64_t n, int64_t k, int64_t nc, const double* X, in
 // copy of R (leading dimension rm_leading_dim(RC_REAL64, P32, s)). One pass over Yrm.
 bool resid_supported(const rc_op* op, int64_t s);
 rc_status resid_block(rc_ctx* ctx, const rc_op* op, const double* Yrm, int64_t ld, int64_t s, const double* lam,
-                      int64_t res_count, double* res, float* R32, int64_t ldr);
+                      int64_t res_count, double* res, rc_corr_t* R32, int64_t ldr);
 
 // Cholesky factor of Gram G (s x s) with diagonal scaling, shift on breakdown;
 // writes Tout = D^-1 R^-1 (upper). flags (device int[4]): [0] shifted, [1] failed, [2] zero column.

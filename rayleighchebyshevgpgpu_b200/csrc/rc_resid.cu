@@ -22,7 +22,7 @@ namespace rcb {
 template <class Pol, int W, class IX>
 __global__ void __launch_bounds__(kRmThreads, 4)
 resid_rm_kernel(Pol op, int64_t n, int64_t s, int nseg, int64_t ld, int groups, const double* __restrict__ Y,
-                const double* __restrict__ lam, int res_count, double* __restrict__ part, float* __restrict__ R32,
+                const double* __restrict__ lam, int res_count, double* __restrict__ part, rc_corr_t* __restrict__ R32,
                 int64_t ldr) {
     constexpr int V = Pack16<double>::V;  // 2 columns per 16-byte slice
     extern __shared__ double red[];        // [rows_per_iter][ld]
@@ -82,7 +82,11 @@ resid_rm_kernel(Pol op, int64_t n, int64_t s, int nseg, int64_t ld, int groups, 
                 }
                 if (R32) {
                     const int64_t c0 = (int64_t)(off + w * wstride);
+#if RC_CORR_BF16
+                    *reinterpret_cast<__nv_bfloat162*>(R32 + i * ldr + c0) = __floats2bfloat162_rn(rv[0], rv[1]);
+#else
                     *reinterpret_cast<float2*>(R32 + i * ldr + c0) = make_float2(rv[0], rv[1]);
+#endif
                 }
             }
             p0 = p1;
@@ -122,7 +126,7 @@ bool resid_supported(const rc_op* op, int64_t s) {
 
 template <class Pol, int W, class IX>
 static rc_status resid_launch(rc_ctx* ctx, const Pol& pol, int64_t n, int64_t s, const double* Y, int64_t ld,
-                              const double* lam, int64_t res_count, double* res, float* R32, int64_t ldr) {
+                              const double* lam, int64_t res_count, double* res, rc_corr_t* R32, int64_t ldr) {
     constexpr int V = Pack16<double>::V;
     if (ld % (V * W) != 0) return rc_fail(ctx, RC_ERR_INVALID, "residual block: leading dimension not padded");
     const int nseg = (int)(ld / (V * W));
@@ -152,14 +156,14 @@ static rc_status resid_launch(rc_ctx* ctx, const Pol& pol, int64_t n, int64_t s,
 
 template <class Pol, int W>
 static rc_status resid_ix(rc_ctx* ctx, const Pol& pol, int64_t n, int64_t s, const double* Y, int64_t ld,
-                          const double* lam, int64_t res_count, double* res, float* R32, int64_t ldr) {
+                          const double* lam, int64_t res_count, double* res, rc_corr_t* R32, int64_t ldr) {
     if ((n + 1) * std::max(ld, ldr) < ((int64_t)1 << 32))
         return resid_launch<Pol, W, uint32_t>(ctx, pol, n, s, Y, ld, lam, res_count, res, R32, ldr);
     return resid_launch<Pol, W, int64_t>(ctx, pol, n, s, Y, ld, lam, res_count, res, R32, ldr);
 }
 
 rc_status resid_block(rc_ctx* ctx, const rc_op* op, const double* Yrm, int64_t ld, int64_t s, const double* lam,
-                      int64_t res_count, double* res, float* R32, int64_t ldr) {
+                      int64_t res_count, double* res, rc_corr_t* R32, int64_t ldr) {
     if (!resid_supported(op, s)) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "residual block: unsupported operator");
     if (res_count < 0 || res_count > s || ld != rm_leading_dim(RC_REAL64, P64, s) ||
         (R32 && ldr != rm_leading_dim(RC_REAL64, P32, s)))

@@ -4,7 +4,9 @@
 // that serve several solves in one launch (rc_batch.cu), so both launch forms compute the same
 // values in the same order.
 #pragma once
+#include <cuda_bf16.h>
 #include <cstring>
+#include <type_traits>
 #include "rc_common.cuh"
 #include "rc_rowops.cuh"
 
@@ -37,6 +39,65 @@ __device__ __forceinline__ void st16(TS* p, const Pack16<TS>& v) {
     *reinterpret_cast<uint4*>(p) = u;
 }
 
+// A 16-byte slice of a block stored as TM, unpacked to the storage type TS of the step arithmetic:
+// TM == TS (16/sizeof(TS) values), or TM bfloat16 with TS float (8 values; the correction
+// filter's bfloat16 blocks), rounded to nearest even on store.
+template <class TS, class TM = TS>
+struct Slice {
+    static constexpr int V = 16 / sizeof(TM);
+    TS v[V];
+};
+__device__ __forceinline__ float bf_lo(uint32_t u) { return __uint_as_float(u << 16); }
+__device__ __forceinline__ float bf_hi(uint32_t u) { return __uint_as_float(u & 0xffff0000u); }
+__device__ __forceinline__ uint32_t bf2_pack(float lo, float hi) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+    uint32_t u;
+    memcpy(&u, &h, 4);
+    return u;
+}
+template <class TS, class TM>
+__device__ __forceinline__ Slice<TS, TM> slice_from(const uint4& u) {
+    Slice<TS, TM> r;
+    if constexpr (std::is_same<TM, TS>::value) {
+        memcpy(&r, &u, 16);
+    } else {
+        static_assert(std::is_same<TS, float>::value && std::is_same<TM, __nv_bfloat16>::value,
+                      "bfloat16 blocks feed FP32 steps");
+        r.v[0] = bf_lo(u.x);
+        r.v[1] = bf_hi(u.x);
+        r.v[2] = bf_lo(u.y);
+        r.v[3] = bf_hi(u.y);
+        r.v[4] = bf_lo(u.z);
+        r.v[5] = bf_hi(u.z);
+        r.v[6] = bf_lo(u.w);
+        r.v[7] = bf_hi(u.w);
+    }
+    return r;
+}
+template <class TS, class TM>
+__device__ __forceinline__ Slice<TS, TM> ldv_ro(const TM* p) {
+    return slice_from<TS, TM>(__ldg(reinterpret_cast<const uint4*>(p)));
+}
+template <class TS, class TM>
+__device__ __forceinline__ Slice<TS, TM> ldv(const TM* p) {
+    return slice_from<TS, TM>(*reinterpret_cast<const uint4*>(p));
+}
+template <class TS, class TM>
+__device__ __forceinline__ void stv(TM* p, const Slice<TS, TM>& v) {
+    uint4 u;
+    if constexpr (std::is_same<TM, TS>::value) {
+        memcpy(&u, &v, 16);
+    } else {
+        u.x = bf2_pack(v.v[0], v.v[1]);
+        u.y = bf2_pack(v.v[2], v.v[3]);
+        u.z = bf2_pack(v.v[4], v.v[5]);
+        u.w = bf2_pack(v.v[6], v.v[7]);
+    }
+    *reinterpret_cast<uint4*>(p) = u;
+}
+__device__ __forceinline__ float elem_f(float v) { return v; }
+__device__ __forceinline__ float elem_f(__nv_bfloat16 v) { return __bfloat162float(v); }
+
 constexpr int kRmThreads = 256;
 // Resident CTAs per SM the register budget must allow: 8 (32 registers) for FP32 storage, 6 (40
 // registers) for FP64 storage and for the correction step (rm_src_min_blocks), which spills at 32.
@@ -48,7 +109,14 @@ constexpr int kRmThreads = 256;
 #ifndef RC_RM_MIN_BLOCKS_SRC
 #define RC_RM_MIN_BLOCKS_SRC 6
 #endif
-constexpr int rm_src_min_blocks() { return RC_RM_MIN_BLOCKS_SRC; }
+#ifndef RC_RM_MIN_BLOCKS_SRC_BF16
+#define RC_RM_MIN_BLOCKS_SRC_BF16 4
+#endif
+// bfloat16 blocks: 8 columns per thread need the 64 registers of 4 resident CTAs per SM
+template <class TM>
+constexpr int rm_src_min_blocks() {
+    return sizeof(TM) == 2 ? RC_RM_MIN_BLOCKS_SRC_BF16 : RC_RM_MIN_BLOCKS_SRC;
+}
 #ifndef RC_RM_MIN_BLOCKS_F64
 #define RC_RM_MIN_BLOCKS_F64 6
 #endif
@@ -62,7 +130,7 @@ constexpr int rm_min_blocks() {
 // in index order, so the rows in flight at any moment form one contiguous band that moves down
 // the block, and a row's far neighbours (i +- band) were read by the band shortly before (an L2
 // hit). Thread (r, seg) of a group owns row r's W 16-byte slices seg, seg + nseg, ...,
-// seg + (W-1)*nseg (V = 16/sizeof(TS) columns each), so one warp-wide load covers contiguous
+// seg + (W-1)*nseg (V = 16/sizeof(TM) columns each), so one warp-wide load covers contiguous
 // 16-byte slices and the row's index data serve W*V columns. Within a CTA the index data of
 // a row are fetched ahead (Pol::fetch1 two groups early, Pol::fetch2 one group early), so
 // only the gathers wait on memory.
@@ -78,13 +146,14 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
 // rc_batch.cu passes its own CTA numbering), so one arithmetic serves both launch forms.
 // SRC (the correction filter): y also gets sig[c] * src(i, c), where src is a row-major block
 // with the same leading dimension and sig holds one coefficient per column (ld entries).
-template <class Pol, class TS, class TC, int W, class IX, bool SRC = false>
+// TM: element type of x, z, y and src in memory (TS, or bfloat16 for FP32 steps).
+template <class Pol, class TS, class TC, int W, class IX, bool SRC = false, class TM = TS>
 __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg, int64_t ld, int groups, int64_t cta,
-                                             const TS* __restrict__ x, const TS* z, TS* y, TC alpha, TC beta,
+                                             const TM* __restrict__ x, const TM* z, TM* y, TC alpha, TC beta,
                                              TC gamma, int64_t pf_z, int64_t pf_x,
-                                             const TS* __restrict__ src = nullptr,
+                                             const TM* __restrict__ src = nullptr,
                                              const float* __restrict__ sig = nullptr) {
-    constexpr int V = Pack16<TS>::V;
+    constexpr int V = Slice<TS, TM>::V;
     const int rows_per_iter = blockDim.x / nseg;
     const int rloc = threadIdx.x / nseg;
     if (rloc >= rows_per_iter) return;
@@ -115,7 +184,7 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
         if (pf_z > 0) {
 #pragma unroll
             for (int w = 0; w < W; ++w) {
-                if ((((off + w * wstride) * (IX)sizeof(TS)) & 127) != 0) continue;  // one per 128-byte line
+                if ((((off + w * wstride) * (IX)sizeof(TM)) & 127) != 0) continue;  // one per 128-byte line
                 if (z && i + pf_z < n) prefetch_l2(z + (IX)(i + pf_z) * ldx + off + w * wstride);
                 if (SRC && i + pf_z < n) prefetch_l2(src + (IX)(i + pf_z) * ldx + off + w * wstride);
                 if (i + pf_x < n) prefetch_l2(x + (IX)(i + pf_x) * ldx + off + w * wstride);
@@ -125,10 +194,10 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
 #pragma unroll
         for (int v = 0; v < W * V; ++v) acc[v] = s_zero(TC());
         op.row(i, p0, [&](int64_t j, TC a) {
-            const TS* xj = x + ((IX)j * ldx + off);
+            const TM* xj = x + ((IX)j * ldx + off);
 #pragma unroll
             for (int w = 0; w < W; ++w) {
-                const Pack16<TS> p = ld16_ro(xj + w * wstride);
+                const Slice<TS, TM> p = ldv_ro<TS, TM>(xj + w * wstride);
 #pragma unroll
                 for (int v = 0; v < V; ++v) acc[w * V + v] = s_fma(a, s_cvt<TC>(p.v[v]), acc[w * V + v]);
             }
@@ -136,11 +205,11 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
 #pragma unroll
         for (int w = 0; w < W; ++w) {
             const IX o = oi + w * wstride;
-            const Pack16<TS> xi = ld16_ro(x + o);
-            Pack16<TS> out;
+            const Slice<TS, TM> xi = ldv_ro<TS, TM>(x + o);
+            Slice<TS, TM> out;
             if (SRC) {
-                const Pack16<TS> si = ld16_ro(src + o);
-                const Pack16<TS> zi = z ? ld16(z + o) : Pack16<TS>{};
+                const Slice<TS, TM> si = ldv_ro<TS, TM>(src + o);
+                const Slice<TS, TM> zi = z ? ldv<TS, TM>(z + o) : Slice<TS, TM>{};
 #pragma unroll
                 for (int v = 0; v < V; ++v) {
                     TC r = s_mul(alpha, acc[w * V + v]);
@@ -150,7 +219,7 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
                     out.v[v] = s_cvt<TS>(r);
                 }
             } else if (z) {
-                const Pack16<TS> zi = ld16(z + o);
+                const Slice<TS, TM> zi = ldv<TS, TM>(z + o);
 #pragma unroll
                 for (int v = 0; v < V; ++v) {
                     TC r = s_mul(alpha, acc[w * V + v]);
@@ -166,7 +235,7 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
                     out.v[v] = s_cvt<TS>(r);
                 }
             }
-            st16(y + o, out);
+            stv<TS, TM>(y + o, out);
         }
         p0 = p1;
         p1 = p2;
@@ -180,12 +249,12 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
 // 9 gathers per row instead of 27 (the per-row form is bound by L1 throughput). Thread (r, seg)
 // of a CTA takes rows cta*rows_per_iter*run + r*run .. + run, the CTA a contiguous range.
 // The sums are formed in a different order than rm_step_rows (a rounding-level difference).
-template <class TD, class TS, class TC, int W, class IX, bool SRC>
+template <class TD, class TS, class TC, int W, class IX, bool SRC, class TM = TS>
 __device__ __forceinline__ void rm_step_rows27(const StencilRows<TD, TC, 27>& op, int64_t n, int nseg, int64_t ld,
-                                               int run, int64_t cta, const TS* __restrict__ x, const TS* z, TS* y,
+                                               int run, int64_t cta, const TM* __restrict__ x, const TM* z, TM* y,
                                                TC alpha, TC beta, TC gamma, int64_t pf_z, int64_t pf_x,
-                                               const TS* __restrict__ src, const float* __restrict__ sig) {
-    constexpr int V = Pack16<TS>::V;
+                                               const TM* __restrict__ src, const float* __restrict__ sig) {
+    constexpr int V = Slice<TS, TM>::V;
     const int rows_per_iter = blockDim.x / nseg;
     const int rloc = threadIdx.x / nseg;
     if (rloc >= rows_per_iter) return;
@@ -214,10 +283,10 @@ __device__ __forceinline__ void rm_step_rows27(const StencilRows<TD, TC, 27>& op
             for (int dy = -1; dy <= 1; ++dy) {
                 const bool vy = dy < 0 ? vym : (dy > 0 ? vyp : true);
                 if (vz && vy) {
-                    const TS* xj = x + ((IX)(j + dy * sy + dz * sz) * ldx + off);
+                    const TM* xj = x + ((IX)(j + dy * sy + dz * sz) * ldx + off);
 #pragma unroll
                     for (int w = 0; w < W; ++w) {
-                        const Pack16<TS> pk = ld16_ro(xj + w * wstride);
+                        const Slice<TS, TM> pk = ldv_ro<TS, TM>(xj + w * wstride);
 #pragma unroll
                         for (int v = 0; v < V; ++v) q[w * V + v] = s_add(q[w * V + v], s_cvt<TC>(pk.v[v]));
                     }
@@ -244,7 +313,7 @@ __device__ __forceinline__ void rm_step_rows27(const StencilRows<TD, TC, 27>& op
         if (pf_z > 0 && i + pf_z < n) {
 #pragma unroll
             for (int w = 0; w < W; ++w) {
-                if ((((off + w * wstride) * (IX)sizeof(TS)) & 127) != 0) continue;
+                if ((((off + w * wstride) * (IX)sizeof(TM)) & 127) != 0) continue;
                 if (z) prefetch_l2(z + (IX)(i + pf_z) * ldx + off + w * wstride);
                 if (SRC) prefetch_l2(src + (IX)(i + pf_z) * ldx + off + w * wstride);
                 if (i + pf_x < n) prefetch_l2(x + (IX)(i + pf_x) * ldx + off + w * wstride);
@@ -254,11 +323,11 @@ __device__ __forceinline__ void rm_step_rows27(const StencilRows<TD, TC, 27>& op
 #pragma unroll
         for (int w = 0; w < W; ++w) {
             const IX o = oi + w * wstride;
-            const Pack16<TS> xi = ld16_ro(x + o);
-            Pack16<TS> zi{}, si{};
-            if (z) zi = ld16(z + o);
-            if (SRC) si = ld16_ro(src + o);
-            Pack16<TS> out;
+            const Slice<TS, TM> xi = ldv_ro<TS, TM>(x + o);
+            Slice<TS, TM> zi{}, si{};
+            if (z) zi = ldv<TS, TM>(z + o);
+            if (SRC) si = ldv_ro<TS, TM>(src + o);
+            Slice<TS, TM> out;
 #pragma unroll
             for (int v = 0; v < V; ++v) {
                 const int e = w * V + v;
@@ -270,7 +339,7 @@ __device__ __forceinline__ void rm_step_rows27(const StencilRows<TD, TC, 27>& op
                 if (SRC) r = s_fma(sg[e], s_cvt<TC>(si.v[v]), r);
                 out.v[v] = s_cvt<TS>(r);
             }
-            st16(y + o, out);
+            stv<TS, TM>(y + o, out);
         }
 #pragma unroll
         for (int v = 0; v < W * V; ++v) {
@@ -333,15 +402,15 @@ __device__ __forceinline__ void to_cm_tile(int64_t n, int64_t s, const TS* __res
 
 // Last step of the correction filter: V[i + c*ldv] = coef[c] * V[i + c*ldv] + beta * E[i*ld + c]
 // (x_m = c_m(lambda_c) v_c + a e_m, scaled by 1/(m+1)); one 32x32 tile, threads 32 x 8.
-template <class TS>
-__device__ __forceinline__ void corr_to_cm_tile(int64_t n, int64_t s, const TS* __restrict__ E, int64_t ld,
+template <class TM>
+__device__ __forceinline__ void corr_to_cm_tile(int64_t n, int64_t s, const TM* __restrict__ E, int64_t ld,
                                                 double* __restrict__ Vc, int64_t ldv, const double* __restrict__ coef,
-                                                double beta, int64_t r0, int64_t c0, TS (&tile)[32][33]) {
+                                                double beta, int64_t r0, int64_t c0, float (&tile)[32][33]) {
     const int tx = threadIdx.x, ty = threadIdx.y;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         const int64_t r = r0 + ty + 8 * j, c = c0 + tx;
-        tile[ty + 8 * j][tx] = (r < n && c < s) ? E[r * ld + c] : s_zero(TS());
+        tile[ty + 8 * j][tx] = (r < n && c < s) ? elem_f(E[r * ld + c]) : 0.0f;
     }
     __syncthreads();
 #pragma unroll

@@ -159,7 +159,7 @@ int64_t solve_footprint(const rc_op* op, const rc_solve_params& p, int sm_count)
         // correction filter: the FP32 residual block and the coefficient table
         const int64_t ld32 = rcb::rm_leading_dim(op->dtype, P32, ss);
         const int64_t dmax = p.poly_degree_max > 0 ? p.poly_degree_max : 200;
-        t += round_2m(n * ld32 * 4) + round_2m((dmax + 1) * ld32 * 4 + ld32 * 8 + 512);
+        t += round_2m(n * ld32 * (int64_t)sizeof(rc_corr_t)) + round_2m((dmax + 1) * ld32 * 4 + ld32 * 8 + 512);
     }
     return t;
 }

@@ -24,6 +24,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 #include "rc_common.cuh"
 #include "rc_cpoly.h"
@@ -60,10 +61,10 @@ private:
     rc_status randomize_cols(void* X, int64_t c0, int64_t c1);
     rc_status deflate(void* X, int64_t s);
     rc_status ortho(int64_t s);
-    rc_status rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool read_back, float* R32 = nullptr);
-    rc_status rr_fused(int64_t s, int64_t res_count, bool* ok, float* R32 = nullptr);
-    rc_status r32_block(int64_t s, float** out);
-    rc_status ritz_and_residuals(XtArgs a, int64_t s, int64_t res_count, float* R32);
+    rc_status rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool read_back, rc_corr_t* R32 = nullptr);
+    rc_status rr_fused(int64_t s, int64_t res_count, bool* ok, rc_corr_t* R32 = nullptr);
+    rc_status r32_block(int64_t s, rc_corr_t** out);
+    rc_status ritz_and_residuals(XtArgs a, int64_t s, int64_t res_count, rc_corr_t* R32);
     rc_status lanczos(int which, double tol, double* lmin, double* lmax);
     void tic(int ph);
     void toc(int ph);
@@ -91,6 +92,7 @@ private:
     // MIXED correction filter: the residual block of the current Ritz vectors (row-major FP32),
     // valid while haveR_ (written by the last Rayleigh-Ritz step, consumed by the next filter)
     bool haveR_ = false;
+    bool rWritten_ = false;  // set by ritz_and_residuals when it wrote the residual block
     int64_t corr_iters_ = 0, corr_steps_ = 0;
 
     std::vector<double> eigValues_, eigVecResiduals_, VtAVeigValue_, subspaceResiduals_;
@@ -226,7 +228,8 @@ rc_status Solver::ortho(int64_t s) {
 // which also writes a row-major copy, then R = A Y - Y diag(lam) in one pass over that copy
 // (rc_resid.cu). Otherwise (complex or callback operators, wider blocks): the dual GEMM (A X) Q
 // with the residual norms reduced on the fly.
-rc_status Solver::ritz_and_residuals(XtArgs a, int64_t s, int64_t res_count, float* R32) {
+rc_status Solver::ritz_and_residuals(XtArgs a, int64_t s, int64_t res_count, rc_corr_t* R32) {
+    rWritten_ = false;
     if (resid_supported(op_, s) && xt2_supported(dtype_, a.k, a.nc)) {
         const int64_t ldrm = rm_leading_dim(RC_REAL64, P64, s);
         void* yrm = nullptr;
@@ -238,28 +241,33 @@ rc_status Solver::ritz_and_residuals(XtArgs a, int64_t s, int64_t res_count, flo
         a.Yrm = (double*)yrm;
         a.ldyr = ldrm;
         RC_TRY(xt(ctx_, dtype_, a));
-        return resid_block(ctx_, op_, (const double*)yrm, ldrm, s, dlam_, res_count, dres_, R32,
-                           R32 ? rm_leading_dim(RC_REAL64, P32, s) : 0);
+        RC_TRY(resid_block(ctx_, op_, (const double*)yrm, ldrm, s, dlam_, res_count, dres_, R32,
+                           R32 ? rm_leading_dim(RC_REAL64, P32, s) : 0));
+        rWritten_ = R32 != nullptr;
+        return RC_OK;
     }
     a.Y2 = nullptr;  // only the residual norms of (A X) Q are needed
     a.lam = dlam_;
     a.res_count = res_count;
     a.res = dres_;
-    if (R32) {
-        a.R32 = R32;
-        a.ldr = rm_leading_dim(RC_REAL64, P32, s);
+    if constexpr (std::is_same<rc_corr_t, float>::value) {  // the dual GEMM writes FP32 residual blocks only
+        if (R32) {
+            a.R32 = reinterpret_cast<float*>(R32);
+            a.ldr = rm_leading_dim(RC_REAL64, P32, s);
+            rWritten_ = true;
+        }
     }
     return xt(ctx_, dtype_, a);
 }
 
-rc_status Solver::r32_block(int64_t s, float** out) {
+rc_status Solver::r32_block(int64_t s, rc_corr_t** out) {
     void* p = nullptr;
-    RC_TRY(rc_slot(ctx_, S_R32, (size_t)n_ * rm_leading_dim(RC_REAL64, P32, s) * sizeof(float), &p));
-    *out = (float*)p;
+    RC_TRY(rc_slot(ctx_, S_R32, (size_t)n_ * rm_leading_dim(RC_REAL64, P32, s) * sizeof(rc_corr_t), &p));
+    *out = (rc_corr_t*)p;
     return RC_OK;
 }
 
-rc_status Solver::rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool read_back, float* R32) {
+rc_status Solver::rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool read_back, rc_corr_t* R32) {
     StepArgs st;
     st.s = s;
     st.x = X; st.xp = P64; st.ldx = n_;
@@ -296,7 +304,7 @@ rc_status Solver::rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool rea
 // problem. Accepted only when the scaled Gram matrix is well conditioned (smallest Cholesky pivot
 // >= 1e-3, no shift needed); otherwise *ok = false, V_ still holds V_f and the caller
 // orthonormalises and repeats the Rayleigh-Ritz step.
-rc_status Solver::rr_fused(int64_t s, int64_t res_count, bool* ok, float* R32) {
+rc_status Solver::rr_fused(int64_t s, int64_t res_count, bool* ok, rc_corr_t* R32) {
     StepArgs st;
     st.s = s;
     st.x = V_; st.xp = P64; st.ldx = n_;
@@ -493,10 +501,11 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
                 int64_t steps = 0;
                 if (phase == PH_CORR32 && haveR_) {
                     // the correction filter: V_ holds the Ritz vectors, dlam_ their values and the
-                    // R32 slot their residual block; its two FP32 work blocks fit in T1_
-                    float* R32 = nullptr;
+                    // R32 slot their residual block; its two work blocks (FP32 or bfloat16) fit in T1_
+                    rc_corr_t* R32 = nullptr;
                     RC_TRY(r32_block(subspaceSize, &R32));
-                    const size_t rmb = (size_t)n_ * rm_leading_dim(RC_REAL64, P32, subspaceSize) * sizeof(float);
+                    const size_t rmb =
+                        (size_t)n_ * rm_leading_dim(RC_REAL64, P32, subspaceSize) * sizeof(rc_corr_t);
                     const size_t blk = (size_t)n_ * subspaceSize * esz_;
                     void* bufA = T1_;
                     void* bufB = (char*)T1_ + ((rmb + 255) / 256) * 256;
@@ -540,7 +549,7 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
             bool fused = false;
             // the residual block for the next correction filter, once the residuals approach the
             // switch tolerance
-            float* R32 = nullptr;
+            rc_corr_t* R32 = nullptr;
             const double prevResidual = residualHistory.empty() ? 1e300 : residualHistory.back();
             if (corrOk && phase != PH_FP64 && (phase == PH_CORR32 || prevResidual < 1e3 * switchTol))
                 RC_TRY(r32_block(subspaceSize, &R32));
@@ -558,7 +567,7 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
                 RC_TRY(rr(V_, W_, subspaceSize, residualCheckCount, true, R32));
                 toc(PH_EIG);
             }
-            haveR_ = R32 != nullptr;
+            haveR_ = R32 != nullptr && rWritten_;
             flush();
             count_ortho_ += 1;
             count_opapply_ += subspaceSize + residualCheckCount;
@@ -890,6 +899,7 @@ rc_status Solver::run(const void* v0, double* evals_out, void* evecs_out, double
         r.time_filter_steps_ms = ctx_->step_ms - step_ms0_;
         r.correction_iterations = corr_iters_;
         r.correction_degree_steps = corr_steps_;
+        r.correction_element_bytes = (int64_t)sizeof(rc_corr_t);
         std::memcpy(info, &r, std::min(sz, sizeof(r)));
     }
     return RC_OK;
