@@ -32,7 +32,7 @@ rm_step_kernel(Pol op, int64_t n, int nseg, int64_t ld, int groups, const TS* __
 // Degree step of the correction filter: y = alpha A x + beta x + gamma z + sig[c] src, with x, z,
 // y and src stored as TM (FP32, or bfloat16 with FP32 arithmetic).
 template <class Pol, class TS, class TC, int W, class IX, class TM>
-__global__ void __launch_bounds__(kRmThreads, rm_src_min_blocks<TM>())
+__global__ void __launch_bounds__(kRmThreads, rm_src_min_blocks<TM, IX>())
 rm_step_src_kernel(Pol op, int64_t n, int nseg, int64_t ld, int groups, const TM* __restrict__ x, const TM* z, TM* y,
                    TC alpha, TC beta, TC gamma, int64_t pf_z, int64_t pf_x, const TM* __restrict__ src,
                    const float* __restrict__ sig) {

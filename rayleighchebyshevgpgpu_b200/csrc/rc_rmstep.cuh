@@ -110,12 +110,16 @@ constexpr int kRmThreads = 256;
 #define RC_RM_MIN_BLOCKS_SRC 6
 #endif
 #ifndef RC_RM_MIN_BLOCKS_SRC_BF16
-#define RC_RM_MIN_BLOCKS_SRC_BF16 4
+#define RC_RM_MIN_BLOCKS_SRC_BF16 0
 #endif
-// bfloat16 blocks: 8 columns per thread need the 64 registers of 4 resident CTAs per SM
-template <class TM>
+// bfloat16 blocks (8 columns per thread, source coefficients re-read from L1): 6 resident CTAs
+// with 32-bit offsets, 5 with 64-bit offsets (which spill at 6), unless the build sets the count
+template <class TM, class IX>
 constexpr int rm_src_min_blocks() {
-    return sizeof(TM) == 2 ? RC_RM_MIN_BLOCKS_SRC_BF16 : RC_RM_MIN_BLOCKS_SRC;
+    return sizeof(TM) != 2               ? RC_RM_MIN_BLOCKS_SRC
+           : RC_RM_MIN_BLOCKS_SRC_BF16 > 0 ? RC_RM_MIN_BLOCKS_SRC_BF16
+           : sizeof(IX) == 4             ? 6
+                                         : 5;
 }
 #ifndef RC_RM_MIN_BLOCKS_F64
 #define RC_RM_MIN_BLOCKS_F64 6
@@ -161,8 +165,11 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
     const IX wstride = (IX)nseg * (IX)V;
     const IX ldx = (IX)ld;
     const int64_t stride = rows_per_iter;
-    TC sg[SRC ? W * V : 1];
-    if (SRC) {
+    // source coefficients: held in registers, or (bfloat16 blocks, 8 columns per thread, where
+    // registers bound the resident CTAs) re-read from L1 per row
+    constexpr bool kSigReg = sizeof(TM) != 2;
+    TC sg[SRC && kSigReg ? W * V : 1];
+    if (SRC && kSigReg) {
 #pragma unroll
         for (int w = 0; w < W; ++w)
 #pragma unroll
@@ -215,7 +222,9 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
                     TC r = s_mul(alpha, acc[w * V + v]);
                     r = s_fma(beta, s_cvt<TC>(xi.v[v]), r);
                     if (z) r = s_fma(gamma, s_cvt<TC>(zi.v[v]), r);
-                    r = s_fma(sg[w * V + v], s_cvt<TC>(si.v[v]), r);
+                    const TC sgv = kSigReg ? sg[kSigReg ? w * V + v : 0]
+                                           : s_from<TC>((double)__ldg(sig + off + w * wstride + v), 0.0);
+                    r = s_fma(sgv, s_cvt<TC>(si.v[v]), r);
                     out.v[v] = s_cvt<TS>(r);
                 }
             } else if (z) {
