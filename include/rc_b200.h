@@ -218,17 +218,22 @@ typedef struct rc_solve_params {
     rc_randomize_fn randomize_fn;  /* optional host randomizer for start/refresh blocks */
     void* randomize_user;
     const void* lanczos_v0;        /* optional HOST start vector for the bounds (n scalars) */
-    double mixed_switch_tol;       /* MIXED: relative residual at which the FP64 sweep starts (default 1e-6) */
+    double mixed_switch_tol;       /* MIXED: relative residual at which the plain FP32 filter gives way to
+                                      the correction filter (or, where that is unsupported or
+                                      mixed_refine = 1, to the FP64 filter). Default 0: the correction
+                                      filter from the first Rayleigh-Ritz step, the FP64 filter at 1e-6;
+                                      1e-6 for both under the request server, which batches the plain
+                                      FP32 filter applications of concurrent solves */
     int verbose;                   /* print per-iteration lines like verboseFlag */
     int phase_timing;              /* record CUDA-event time per phase (TIMING_ buckets) */
     int orth_mode;                 /* 0: Rayleigh-Ritz on the filtered block with the Cholesky factor of its
                                       scaled Gram matrix folded in, CholeskyQR2 when that matrix is
                                       ill-conditioned; 1: always CholeskyQR2 then Rayleigh-Ritz */
-    int mixed_refine;              /* MIXED, after the switch tolerance: 0 (default) the FP32 correction
-                                      filter (the recurrence applied to the residual block A V - V diag(lam)
-                                      of the Ritz vectors, whose FP32 rounding error shrinks with the
-                                      residual; real operators, subspace <= 96; FP64 filter otherwise or
-                                      when it stalls); 1 the FP64 filter */
+    int mixed_refine;              /* MIXED, after the switch tolerance: 0 (default) the correction filter
+                                      (the recurrence applied to the residual block A V - V diag(lam) of
+                                      the Ritz vectors, stored in bfloat16 with FP32 arithmetic, whose
+                                      rounding error shrinks with the residual; real operators, subspace
+                                      <= 96; FP64 filter otherwise or when it stalls); 1 the FP64 filter */
 } rc_solve_params;
 
 typedef struct rc_solve_info {
@@ -260,7 +265,7 @@ typedef struct rc_solve_info {
     int64_t fused_rr_fallbacks;    /* of those, rejected for conditioning and redone after CholeskyQR2 */
     double time_filter_steps_ms;   /* part of time_filter_ms spent in the fused degree-step launches
                                       themselves (row-major filter, transposes excluded; phase_timing = 1) */
-    int64_t correction_iterations; /* MIXED: inner iterations that ran the FP32 correction filter */
+    int64_t correction_iterations; /* MIXED: inner iterations that ran the correction filter */
     int64_t correction_degree_steps; /* of degree_steps, those of the correction filter */
     int64_t correction_element_bytes; /* bytes per stored element of the correction filter's residual
                                          and recurrence blocks: 2 (bfloat16) or 4 (FP32) */

@@ -517,7 +517,7 @@ void rc_solve_params_default(rc_solve_params* p) {
     p->lanczos_max_iter = 10000;
     p->mode = 0;
     p->seed = 3141592;
-    p->mixed_switch_tol = 1e-6;
+    p->mixed_switch_tol = 0.0;  // by operator: correction filter at once, FP64 filter at 1e-6
 }
 
 rc_status rc_solve(rc_ctx* ctx, const rc_op* op_c, const rc_solve_params* params, const void* v0, double* evals_out,

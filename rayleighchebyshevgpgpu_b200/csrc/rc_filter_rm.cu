@@ -167,12 +167,13 @@ static rc_status run_rm_filter(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, 
     return RC_OK;
 }
 
-// The correction filter (FP32 storage, real operators). V holds Ritz vectors v_c with Ritz values
-// lam_c, and R = A V - V diag(lam) (row-major FP32, leading dimension ld). With x_k = c_k v + a e_k
-// (c_k the scalar recurrence at lam_c) the recurrence of run_rm_filter becomes
+// The correction filter (real operators; blocks stored as TM = rc_corr_t, bfloat16 by default,
+// FP32 arithmetic). V holds Ritz vectors v_c with Ritz values lam_c, and R = A V - V diag(lam)
+// (row-major, leading dimension ld). With x_k = c_k v + a e_k (c_k the scalar recurrence at
+// lam_c) the recurrence of run_rm_filter becomes
 //   e_0 = 0, e_1 = R, e_k = a A e_{k-1} + b e_{k-1} - e_{k-2} + c_{k-1} R,
 // and the result x_m/(m+1) = coef_c v_c + a e_m/(m+1) is formed in FP64. e_k is small (of the size
-// of the residual), so its FP32 rounding perturbs the filtered block by FP32 rounding times the
+// of the residual), so its rounding perturbs the filtered block by the storage rounding times the
 // residual instead of times the block: the subspace keeps converging past the FP32 floor of the
 // plain FP32 filter. e_2 -> A, e_3 -> B (e_1 = R is read as x_{k-2}), then e_k over e_{k-2}.
 template <class Pol, class TS, class TC, int W, class IX, class TM>

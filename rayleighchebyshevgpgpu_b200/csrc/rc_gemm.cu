@@ -14,7 +14,8 @@
 //         48 columns. Dual form (32-row tiles of X and W, 8-row warp slabs) also forms W T for the
 //         columns that need it and reduces
 //         ||(W T)_c - lam_c (X T)_c||^2 for c < res_count; with R32 it writes the residual block
-//         R = W T - (X T) diag(lam) in row-major FP32 (the source term of the correction filter).
+//         R = W T - (X T) diag(lam) in row-major FP32 (the source term of an FP32-storage
+//         correction filter; native real operators take R from rc_resid.cu instead).
 // These replace cublasDgemm(OP_T, OP_N) and cublasDgemm(OP_N, OP_N) plus the residual kernel
 // of the reference (RayleighChebyshevLMCuda.h:2139-2161, :2200-2285).
 //

@@ -11,9 +11,12 @@
 // Storage/compute precision of a block: FP64 (double / c128) or FP32 (float / c64).
 enum { P64 = 0, P32 = 1 };
 
-// Storage of the residual block read by the correction filter: bfloat16 (default) or FP32
-// (RC_CORR_BF16=0). The block only feeds the correction e_k, which is of the size of the residual,
-// so its 8-bit mantissa perturbs the filtered vectors by 2^-9 of a residual-sized term.
+// Storage of the correction filter's residual block R and recurrence blocks e_k: bfloat16
+// (default) or FP32 (RC_CORR_BF16=0); the arithmetic is FP32 either way. e_k is of the size of the
+// residual, so the 8-bit mantissa perturbs the filtered vectors by about 2^-9 of a residual-sized
+// term, and the error keeps shrinking with the residual: on the 128^3 7-point and 256^3 27-point
+// workloads the solves take the same inner iterations as with FP32 storage, with eigenvalues
+// equal to a few units in the 15th digit.
 #ifndef RC_CORR_BF16
 #define RC_CORR_BF16 1
 #endif

@@ -3,7 +3,7 @@
 // The reference forms tmp = A*V with a second SpMM and then runs its residuals kernel
 // (RayleighChebyshevLMCuda.h:2235, :2274-2280; cuda_kernels.cu:307-382). Here the sparse product,
 // the subtraction, the column norms ||R_c|| (c < res_count) and, for the correction filter, the
-// row-major FP32 copy of R are one kernel over the row-major FP64 copy of Y that the Ritz GEMM
+// row-major bfloat16 (rc_corr_t) copy of R are one kernel over the row-major FP64 copy of Y that the Ritz GEMM
 // writes beside the column-major one (xt2): the filter's degree-step arithmetic (rc_rmstep.cuh
 // layout: 16-byte slices, consecutive row groups per CTA), so a neighbour row is one contiguous
 // run and the far neighbours (i +- band) are L2 hits. Nothing n x s is written in FP64.

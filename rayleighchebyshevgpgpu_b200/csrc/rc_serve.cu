@@ -156,7 +156,7 @@ int64_t solve_footprint(const rc_op* op, const rc_solve_params& p, int sm_count)
     if (rcb::resid_supported(op, ss))                                 // row-major copy of the Ritz vectors
         t += round_2m(n * rcb::rm_leading_dim(op->dtype, P64, ss) * 8);
     if (p.precision == RC_PREC_MIXED && p.mixed_refine == 0 && rcb::rm_corr_supported(op, ss)) {
-        // correction filter: the FP32 residual block and the coefficient table
+        // correction filter: the residual block (rc_corr_t) and the coefficient table
         const int64_t ld32 = rcb::rm_leading_dim(op->dtype, P32, ss);
         const int64_t dmax = p.poly_degree_max > 0 ? p.poly_degree_max : 200;
         t += round_2m(n * ld32 * (int64_t)sizeof(rc_corr_t)) + round_2m((dmax + 1) * ld32 * 4 + ld32 * 8 + 512);

@@ -15,10 +15,13 @@
 //   * Ritz vectors V*Q are not renormalised (V and Q are orthonormal);
 //   * after an outer pass only the stale tail columns are refreshed (the CPU LM refreshes the
 //     buffer range, RayleighChebyshevLM.h:1086-1092; the GPU reference the whole block, :1176-1179);
-//   * MIXED precision: the filter runs in FP32/c64 until the residuals reach mixed_switch_tol
-//     or stall (it never stops in this phase), then as the FP32 correction filter on the residual
-//     block of the Ritz vectors (rc_filter_rm.cu), which converges like the FP64 filter; FP64
-//     filter when the correction filter is unsupported, switched off, or stalls.
+//   * MIXED precision: the first filter application runs in FP32 (there is no residual block
+//     yet), then the correction filter (bfloat16 storage, FP32 arithmetic) on the residual block
+//     of the Ritz vectors (rc_filter_rm.cu), which converges like the FP64 filter. Operators
+//     without it run the FP32/c64 filter until the residuals reach mixed_switch_tol (1e-6) or
+//     stall (never stopping in that phase), then the FP64 filter; a set mixed_switch_tol also
+//     delays the correction filter to that residual. The FP64 filter also takes over when the
+//     correction filter stalls.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -89,7 +92,7 @@ private:
     int64_t fused_ok_ = 0, fused_fallback_ = 0;
     double* hbuf_ = nullptr;
     int64_t ss_cap_ = 0;
-    // MIXED correction filter: the residual block of the current Ritz vectors (row-major FP32),
+    // MIXED correction filter: the residual block of the current Ritz vectors (row-major rc_corr_t),
     // valid while haveR_ (written by the last Rayleigh-Ritz step, consumed by the next filter)
     bool haveR_ = false;
     bool rWritten_ = false;  // set by ritz_and_residuals when it wrote the residual block
@@ -426,8 +429,13 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
     const int64_t filterRepetitionCount = P_.filter_repetition > 0 ? P_.filter_repetition : 1;
     const int stopCondition = (P_.stop_condition == RC_STOP_DEFAULT) ? RC_STOP_COMBINATION : P_.stop_condition;
     const bool mixed = P_.precision == RC_PREC_MIXED && op_->kind != 2;
-    const double switchTol = P_.mixed_switch_tol > 0 ? P_.mixed_switch_tol : 1e-6;
-    // MIXED phases: 0 plain FP32 filter, 1 FP32 correction filter, 2 FP64 filter
+    // relative residual at which the plain FP32 filter gives way: by default at the first
+    // Rayleigh-Ritz step to the correction filter (a bfloat16 correction step moves fewer bytes than
+    // a plain FP32 step and converges like the FP64 filter), else at 1e-6 to the FP64 filter.
+    // Under the request server the plain FP32 filter runs to 1e-6 either way: its applications are
+    // the ones the server batches across solves.
+    const double switchTolSet = P_.mixed_switch_tol > 0 ? P_.mixed_switch_tol : (ctx_->serve ? 1e-6 : 0.0);
+    // MIXED phases: 0 plain FP32 filter, 1 correction filter, 2 FP64 filter
     enum { PH_PLAIN32 = 0, PH_CORR32 = 1, PH_FP64 = 2 };
 
     bool completedBasisFlag = false;
@@ -444,6 +452,7 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
         if (applyCountCumulative > 0) RC_TRY(randomize_cols(V_, subspaceSize - lastFoundCount, subspaceSize));
         haveR_ = false;
         const bool corrOk = mixed && P_.mixed_refine == 0 && rm_corr_supported(op_, subspaceSize);
+        const double switchTol = switchTolSet > 0 ? switchTolSet : (corrOk ? HUGE_VAL : 1e-6);
 
         tic(PH_ORTHO);
         RC_TRY(ortho(subspaceSize));  // the reference orthogonalizes twice here (:1195-1196)

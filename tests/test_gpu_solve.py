@@ -67,8 +67,8 @@ def test_complex_tight_binding_vs_lapack(ctx, precision):
 
 @pytest.mark.parametrize("kind,dims,k", [(5, (80, 72), 32), (7, (18, 17, 16), 16), (27, (16, 15, 14), 16)])
 def test_mixed_correction_filter_matches_fp64(ctx, kind, dims, k):
-    """MIXED precision past the switch tolerance runs the FP32 correction filter (the recurrence on
-    the residual block of the Ritz vectors): it reaches tol 1e-10 with no FP64 degree step and the
+    """MIXED precision past the switch tolerance runs the correction filter (the recurrence on the
+    residual block of the Ritz vectors, bfloat16 storage, FP32 arithmetic): it reaches tol 1e-10 with no FP64 degree step and the
     FP64 path's eigenvalues; mixed_refine = 1 keeps the FP64 refinement filter."""
     n = int(np.prod(dims))
     diag = (4.0 if kind == 5 else (6.0 if kind == 7 else 1.0)) + np.random.default_rng(kind).uniform(0, 3, n)
