@@ -325,10 +325,13 @@ def run_ours(args):
     ceb = int(infos[-1].get("correction_element_bytes", 4) or 4)
     bytes_corr_step = b_a32 + 4 * P.n * s * ceb
     bytes_fp64_step = b_a64 + 3 * P.n * s * 8
-    fsteps = sum(i["degree_steps"] for i in infos)
+    # A correction filter of degree m launches m - 1 steps (e_1 = R comes from the residual kernel
+    # of the Rayleigh-Ritz step), so its launches are its degree steps less its applications.
     f64steps = sum(i["fp64_degree_steps"] for i in infos)
-    csteps = sum(i["correction_degree_steps"] for i in infos)
-    p32steps = fsteps - f64steps - csteps
+    csteps_deg = sum(i["correction_degree_steps"] for i in infos)
+    p32steps = sum(i["degree_steps"] for i in infos) - f64steps - csteps_deg
+    csteps = csteps_deg - sum(i["correction_iterations"] for i in infos)
+    fsteps = p32steps + csteps + f64steps
     tsteps = sum(i["time_filter_steps_ms"] for i in infos) * 1e-3
     alg_bytes = p32steps * bytes_fp32_step + csteps * bytes_corr_step + f64steps * bytes_fp64_step
     achieved = alg_bytes / tsteps / 1e9 if tsteps > 0 else None
