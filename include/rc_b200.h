@@ -221,9 +221,7 @@ typedef struct rc_solve_params {
     double mixed_switch_tol;       /* MIXED: relative residual at which the plain FP32 filter gives way to
                                       the correction filter (or, where that is unsupported or
                                       mixed_refine = 1, to the FP64 filter). Default 0: the correction
-                                      filter from the first Rayleigh-Ritz step, the FP64 filter at 1e-6;
-                                      1e-6 for both under the request server, which batches the plain
-                                      FP32 filter applications of concurrent solves */
+                                      filter from the first Rayleigh-Ritz step, the FP64 filter at 1e-6 */
     int verbose;                   /* print per-iteration lines like verboseFlag */
     int phase_timing;              /* record CUDA-event time per phase (TIMING_ buckets) */
     int orth_mode;                 /* 0: Rayleigh-Ritz on the filtered block with the Cholesky factor of its

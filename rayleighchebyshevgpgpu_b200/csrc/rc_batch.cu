@@ -8,6 +8,10 @@
 // concatenates the solves' own CTA ranges, and a solve whose degree is below k skips its range.
 // The per-solve arithmetic is the single-solve row-major filter's (rc_rmstep.cuh), so a solve
 // gets the same values whether it runs alone, in a batch, or outside the server.
+// A batch also carries correction-filter applications (prec kBatchCorr, the MIXED refinement of
+// rc_filter_rm.cu): they skip the entry layout change, run their steps k = 2..m in a third step
+// kernel (bfloat16 blocks, the residual block as the source term) and form V = coef v + a e_m/(m+1)
+// in the exit layout change.
 //
 // The batch description lives in a device table that a memcpy node refreshes from pinned host
 // memory at the start of the batch, so one captured CUDA graph per (D, table slot) serves every
@@ -84,6 +88,54 @@ batch_step_kernel(const BatchTable* __restrict__ T, int k) {
     }
 }
 
+// Degree-step k (2 <= k <= m) of every correction-filter application of the batch, with the
+// single-solve correction filter's buffer rotation (run_rm_corr): e_1 = R, e_k over e_{k-2}.
+template <class Pol>
+__device__ __noinline__ void batch_corr_step_typed(const Pol pol, const BatchJob& J, int k, int64_t cta) {
+    using TM = rc_corr_t;
+    const TM* R = (const TM*)J.R;
+    TM* A = (TM*)J.bufA;
+    TM* B = (TM*)J.bufB;
+    const TM* xk1 = k == 2 ? R : ((k - 1) % 2 == 0 ? A : B);  // e_{k-1}
+    TM* y = k % 2 == 0 ? A : B;                                 // e_k
+    const TM* z = k == 2 ? nullptr : (k == 3 ? R : y);          // e_{k-2}
+    const float ta = s_from<float>(J.a, 0.0), tb = s_from<float>(J.b, 0.0);
+    const float tg = k == 2 ? s_zero(float()) : s_from<float>(-1.0, 0.0);
+    rm_step_rows<Pol, float, float, 1, uint32_t, true, TM>(pol, J.n, J.nseg, J.ld, J.groups, cta, xk1, z, y, ta, tb,
+                                                           tg, J.pf_z, J.pf_x, R, J.sig + k * J.ld);
+}
+
+// 4 resident CTAs per SM: the out-of-line per-operator step (which keeps each operator's code
+// apart, as batch_step_typed does) spills at the single-solve kernel's 6.
+constexpr int kBatchCorrBlocksPerSm = 4;
+
+__global__ void __launch_bounds__(kRmThreads, kBatchCorrBlocksPerSm)
+batch_corr_step_kernel(const BatchTable* __restrict__ T, int k) {
+    __shared__ int64_t ends[kMaxBatchJobs];
+    const int nj = T->njobs;
+    for (int j = threadIdx.x; j < nj; j += blockDim.x) ends[j] = T->jobs[j].vcta1;
+    __syncthreads();
+    const int64_t total = T->total_vctas;
+    int j = 0;
+    for (int64_t v = blockIdx.x; v < total; v += gridDim.x) {
+        while (j < nj && ends[j] <= v) ++j;
+        if (j >= nj) break;
+        const BatchJob& J = T->jobs[j];
+        if (J.prec != kBatchCorr || k < 2 || k > J.degree) continue;
+        const int64_t cta = v - J.vcta0;
+        if (J.kind == 0) {
+            CsrRows<float, float> pol{J.rowptr, J.colind, (const float*)J.vals};
+            batch_corr_step_typed(pol, J, k, cta);
+        } else if (J.kind == 7) {
+            StencilRows<float, float, 7> pol{J.nx, J.ny, J.nz, (const float*)J.diag, J.offd, 0.0};
+            batch_corr_step_typed(pol, J, k, cta);
+        } else {
+            StencilRows<float, float, 5> pol{J.nx, J.ny, J.nz, (const float*)J.diag, J.offd, 0.0};
+            batch_corr_step_typed(pol, J, k, cta);
+        }
+    }
+}
+
 // Layout changes of every solve: to_rm (x0 = X, column-major FP64 -> row-major storage) and
 // to_cm (X = x_m / (m+1)). Virtual tiles as above; a barrier closes each tile because the
 // shared tile is reused by the next one.
@@ -105,7 +157,12 @@ batch_transpose_kernel(const BatchTable* __restrict__ T) {
         const BatchJob& J = T->jobs[j];
         const int64_t t = v - J.tile0;
         const int64_t r0 = (t % J.tiles_x) * 32, c0 = (t / J.tiles_x) * 32;
-        if (TO_RM) {
+        if (J.prec == kBatchCorr) {  // no entry layout change; the exit forms coef v + a e_m / (m+1)
+            if (TO_RM) continue;
+            const void* em = J.degree == 1 ? J.R : (J.degree % 2 == 0 ? J.bufA : J.bufB);
+            corr_to_cm_tile<rc_corr_t>(J.n, J.s, (const rc_corr_t*)em, J.ld, J.V, J.ldv, J.coef,
+                                       J.a / (double)(J.degree + 1), r0, c0, tile32);
+        } else if (TO_RM) {
             if (J.prec == P32) to_rm_tile<double, float>(J.n, J.s, J.V, J.ldv, (float*)J.bufA, J.ld, r0, c0, tile32);
             else to_rm_tile<double, double>(J.n, J.s, J.V, J.ldv, (double*)J.bufA, J.ld, r0, c0, tile64);
         } else {
@@ -179,6 +236,57 @@ bool batch_job_describe(const rc_ctx* ctx, const rc_op* op, void* V, int64_t ldv
     return true;
 }
 
+bool batch_job_describe_corr(const rc_ctx* ctx, const rc_op* op, double* V, int64_t ldv, int64_t s, int64_t degree,
+                             double a, double b, const rc_corr_t* R, const float* sig, const double* coef,
+                             void* bufA, void* bufB, BatchJob* J) {
+    if (op->kind == 2 || op->dtype != RC_REAL64 || degree < 1 || s < 1) return false;
+    if (op->kind == 1 && op->skind != 5 && op->skind != 7) return false;
+    const int64_t ld = rm_leading_dim(RC_REAL64, P32, s);
+    if ((op->n + 1) * ld >= ((int64_t)1 << 32)) return false;
+    const int vec = (int)(16 / sizeof(rc_corr_t));
+    if (ld % vec != 0) return false;
+    const int nseg = (int)(ld / vec);
+    if (nseg > kRmThreads) return false;
+    const bool csr = op->kind == 0;
+    if (csr ? op->vals32 == nullptr : op->diag32 == nullptr) return false;
+    // the single-solve correction filter's choices (run_rm_corr)
+    const int groups = ctx->rm_groups > 0 ? ctx->rm_groups : (csr ? 4 : 8);
+    const int64_t rows_per_cta = (int64_t)groups * (kRmThreads / nseg);
+    std::memset(J, 0, sizeof(*J));
+    J->kind = csr ? 0 : op->skind;
+    J->prec = kBatchCorr;
+    J->nseg = nseg;
+    J->groups = groups;
+    J->n = op->n;
+    J->ld = ld;
+    J->ldv = ldv;
+    J->s = s;
+    J->degree = degree;
+    J->vcta1 = (op->n + rows_per_cta - 1) / rows_per_cta;
+    J->tiles_x = (op->n + 31) / 32;
+    J->tile1 = J->tiles_x * ((s + 31) / 32);
+    J->rowptr = op->rowptr;
+    J->colind = op->colind;
+    J->vals = op->vals32;
+    J->diag = op->diag32;
+    J->offd = op->offdiag;
+    J->nx = op->nx;
+    J->ny = op->ny;
+    J->nz = op->nz;
+    J->V = V;
+    J->bufA = bufA;
+    J->bufB = bufB;
+    J->a = a;
+    J->b = b;
+    const int64_t band = csr ? op->band : (op->skind == 5 ? op->nx : op->nx * op->ny);
+    J->pf_z = ctx->pf_rows;
+    J->pf_x = ctx->pf_rows > 0 ? ctx->pf_rows + band : 0;
+    J->R = R;
+    J->sig = sig;
+    J->coef = coef;
+    return true;
+}
+
 struct BatchRunner {
     int device = 0;
     int sm_count = 148;
@@ -232,7 +340,12 @@ cudaStream_t batch_runner_stream(BatchRunner* R) { return R->stream; }
 BatchCounters batch_runner_counters(const BatchRunner* R) { return R->counters; }
 
 // The batch's launches on R->stream, reading table `tab` (device).
-static cudaError_t issue(BatchRunner* R, int slot, int64_t depth, bool has32, bool has64, int64_t* launches) {
+static int64_t batch_launches(int64_t depth, bool has32, bool has64, bool hasC) {
+    return depth * ((has32 ? 1 : 0) + (has64 ? 1 : 0)) + (hasC ? std::max<int64_t>(depth - 1, 0) : 0) + 2;
+}
+
+static cudaError_t issue(BatchRunner* R, int slot, int64_t depth, bool has32, bool has64, bool hasC,
+                         int64_t* launches) {
     const unsigned gs = (unsigned)(R->sm_count * rm_min_blocks<float>());
     const unsigned gt = (unsigned)(R->sm_count * kBatchTileBlocksPerSm);
     const dim3 tblk(32, 8);
@@ -240,12 +353,14 @@ static cudaError_t issue(BatchRunner* R, int slot, int64_t depth, bool has32, bo
     if (e != cudaSuccess) return e;
     batch_transpose_kernel<true><<<gt, tblk, 0, R->stream>>>(R->dev[slot]);
     const unsigned gs64 = (unsigned)(R->sm_count * rm_min_blocks<double>());
+    const unsigned gsc = (unsigned)(R->sm_count * kBatchCorrBlocksPerSm);
     for (int64_t k = 1; k <= depth; ++k) {
         if (has32) batch_step_kernel<float><<<gs, kRmThreads, 0, R->stream>>>(R->dev[slot], (int)k);
         if (has64) batch_step_kernel<double><<<gs64, kRmThreads, 0, R->stream>>>(R->dev[slot], (int)k);
+        if (hasC && k >= 2) batch_corr_step_kernel<<<gsc, kRmThreads, 0, R->stream>>>(R->dev[slot], (int)k);
     }
     batch_transpose_kernel<false><<<gt, tblk, 0, R->stream>>>(R->dev[slot]);
-    *launches = depth * ((has32 ? 1 : 0) + (has64 ? 1 : 0)) + 2;
+    *launches = batch_launches(depth, has32, has64, hasC);
     return cudaGetLastError();
 }
 
@@ -263,7 +378,7 @@ rc_status batch_run(BatchRunner* R, const BatchJob* jobs, int njobs, cudaEvent_t
     BatchTable* T = R->host[slot];
     T->njobs = njobs;
     int64_t vc = 0, tc = 0, depth = 0;
-    bool has32 = false, has64 = false;
+    bool has32 = false, has64 = false, hasC = false;
     for (int j = 0; j < njobs; ++j) {
         BatchJob J = jobs[j];
         const int64_t nv = J.vcta1, nt = J.tile1;  // local counts from batch_job_describe
@@ -274,7 +389,7 @@ rc_status batch_run(BatchRunner* R, const BatchJob* jobs, int njobs, cudaEvent_t
         vc += nv;
         tc += nt;
         depth = std::max(depth, J.degree);
-        (J.prec == P32 ? has32 : has64) = true;
+        (J.prec == kBatchCorr ? hasC : (J.prec == P32 ? has32 : has64)) = true;
         T->jobs[j] = J;
     }
     T->total_vctas = vc;
@@ -283,7 +398,7 @@ rc_status batch_run(BatchRunner* R, const BatchJob* jobs, int njobs, cudaEvent_t
     cudaError_t e = cudaSuccess;
     if (R->use_graphs && depth <= kMaxGraphDepth) {
         // graph key: depth, table slot and which precisions have step kernels
-        const int64_t kind = depth * 4 + (has32 ? 1 : 0) + (has64 ? 2 : 0);
+        const int64_t kind = depth * 8 + (has32 ? 1 : 0) + (has64 ? 2 : 0) + (hasC ? 4 : 0);
         const auto key = std::make_pair(kind, slot);
         auto it = R->graphs.find(key);
         if (it == R->graphs.end()) {
@@ -291,7 +406,7 @@ rc_status batch_run(BatchRunner* R, const BatchJob* jobs, int njobs, cudaEvent_t
             cudaGraphExec_t ge = nullptr;
             e = cudaStreamBeginCapture(R->stream, cudaStreamCaptureModeThreadLocal);
             if (e == cudaSuccess) {
-                cudaError_t ei = issue(R, slot, depth, has32, has64, &launches);
+                cudaError_t ei = issue(R, slot, depth, has32, has64, hasC, &launches);
                 e = cudaStreamEndCapture(R->stream, &g);
                 if (ei != cudaSuccess) e = ei;
             }
@@ -306,10 +421,10 @@ rc_status batch_run(BatchRunner* R, const BatchJob* jobs, int njobs, cudaEvent_t
             R->counters.graphs_built++;
         }
         e = cudaGraphLaunch(it->second, R->stream);
-        launches = depth * ((has32 ? 1 : 0) + (has64 ? 1 : 0)) + 2;
+        launches = batch_launches(depth, has32, has64, hasC);
         R->counters.graph_launches++;
     } else {
-        e = issue(R, slot, depth, has32, has64, &launches);
+        e = issue(R, slot, depth, has32, has64, hasC, &launches);
     }
     if (e == cudaSuccess) e = cudaEventRecord(R->done[slot], R->stream);
     if (e != cudaSuccess) {

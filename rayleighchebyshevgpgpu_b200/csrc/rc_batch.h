@@ -11,11 +11,12 @@ namespace rcb {
 constexpr int kMaxBatchJobs = 64;   // filter applications per batch
 constexpr int kBatchSlots = 4;      // device tables in flight (ring)
 constexpr int64_t kMaxGraphDepth = 256;  // deeper batches launch without a graph
+constexpr int32_t kBatchCorr = 2;        // BatchJob::prec of a correction-filter application
 
 // One solve's filter application X <- P_m(A')X as the batched kernels read it.
 struct BatchJob {
     int32_t kind;     // 0 CSR, 5 / 7 / 27 stencil (real)
-    int32_t prec;     // P32 or P64 (storage and compute)
+    int32_t prec;     // P32 or P64 (storage and compute), or kBatchCorr (rc_corr_t storage, FP32)
     int32_t nseg;     // 16-byte slices per row-major row / slices per thread
     int32_t groups;   // consecutive row groups per virtual CTA
     int64_t n, ld, ldv, s, degree;
@@ -33,6 +34,9 @@ struct BatchJob {
     void* bufB;
     double a, b;           // x_k = a A x_{k-1} + b x_{k-1} - x_{k-2}
     int64_t pf_z, pf_x;    // L2 prefetch distances (rows)
+    const void* R;         // kBatchCorr: the residual block (e_1), row-major rc_corr_t
+    const float* sig;      // kBatchCorr: source coefficients, (degree + 1) x ld
+    const double* coef;    // kBatchCorr: weight of V in the result, one per column
 };
 
 struct BatchTable {
@@ -60,6 +64,13 @@ struct BatchRunner;
 // operator must already exist for prec == RC_PREC_MIXED.
 bool batch_job_describe(const rc_ctx* ctx, const rc_op* op, void* V, int64_t ldv, int64_t s, int64_t degree,
                         double a, double b, int prec, void* bufA, void* bufB, size_t buf_bytes, BatchJob* J);
+
+// The same for a correction-filter application (rm_filter_corr): V holds the Ritz vectors, R their
+// residual block, sig and coef the tables corr_coef_kernel wrote. CSR and 5/7-point stencils with
+// 32-bit offsets; the 27-point stencil keeps the single-solve run form (rm_step_rows27).
+bool batch_job_describe_corr(const rc_ctx* ctx, const rc_op* op, double* V, int64_t ldv, int64_t s, int64_t degree,
+                             double a, double b, const rc_corr_t* R, const float* sig, const double* coef,
+                             void* bufA, void* bufB, BatchJob* J);
 
 rc_status batch_runner_create(int device, int sm_count, bool use_graphs, BatchRunner** out, std::string* err);
 void batch_runner_destroy(BatchRunner* R);

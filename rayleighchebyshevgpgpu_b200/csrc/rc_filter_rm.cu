@@ -285,6 +285,11 @@ rc_status rm_filter_corr(rc_ctx* ctx, rc_op* op, double* V, int64_t ldv, int64_t
     corr_coef_kernel<<<1, 128, 0, ctx->stream>>>(s, ld, degree, a, b, lam_dev, sig, coef);
     ctx->launches++;
     RC_CU(ctx, cudaGetLastError());
+    if (ctx->serve) {  // under the request server: one job of a batched launch
+        bool handled = false;
+        RC_TRY(serve_filter_corr(ctx, op, V, ldv, s, degree, a, b, R, sig, coef, bufA, bufB, &handled));
+        if (handled) return RC_OK;
+    }
     const int64_t n = op->n;
     const int64_t band = op->kind == 0 ? op->band : (op->skind == 5 ? op->nx : op->nx * op->ny);
     rc_corr_t* A = (rc_corr_t*)bufA;

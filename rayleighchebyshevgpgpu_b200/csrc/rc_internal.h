@@ -173,6 +173,10 @@ rc_status filter_apply(rc_ctx* ctx, rc_op* op, void* V, int64_t ld, int64_t s, i
 // single-solve path (rc_serve.cu).
 rc_status serve_filter(rc_ctx* ctx, rc_op* op, void* V, int64_t ld, int64_t s, int64_t degree, double a, double b,
                        int prec, void* bufA, void* bufB, size_t buf_bytes, bool* handled);
+// The same for a correction-filter application (rm_filter_corr, after corr_coef_kernel).
+rc_status serve_filter_corr(rc_ctx* ctx, rc_op* op, double* V, int64_t ldv, int64_t s, int64_t degree, double a,
+                            double b, const rc_corr_t* R, const float* sig, const double* coef, void* bufA,
+                            void* bufB, bool* handled);
 // Correction filter (rc_filter_rm.cu), the MIXED precision refinement: V (FP64 column-major,
 // leading dimension ldv) holds Ritz vectors with Ritz values lam_dev (device) and R (row-major
 // rc_corr_t, leading dimension rm_leading_dim(RC_REAL64, P32, s)) their residual block A V - V diag(lam);

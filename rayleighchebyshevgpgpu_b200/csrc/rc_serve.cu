@@ -321,13 +321,12 @@ using namespace rcserve;
 
 namespace rcb {
 
-rc_status serve_filter(rc_ctx* ctx, rc_op* op, void* V, int64_t ld, int64_t s, int64_t degree, double a, double b,
-                       int prec, void* bufA, void* bufB, size_t buf_bytes, bool* handled) {
-    *handled = false;
+// Post one described filter application to the batcher and wait until its batch is launched;
+// the solve's stream then waits for the batch before it reads V.
+static rc_status serve_post(rc_ctx* ctx, const BatchJob& job, bool* handled) {
     ServeHook* h = ctx->serve;
-    if (!h) return RC_OK;
     PendingJob pj;
-    if (!batch_job_describe(ctx, op, V, ld, s, degree, a, b, prec, bufA, bufB, buf_bytes, &pj.job)) return RC_OK;
+    pj.job = job;
     RC_CU(ctx, cudaEventRecord(h->worker->ready, ctx->stream));
     pj.ready = h->worker->ready;
     Server* S = h->server;
@@ -343,6 +342,25 @@ rc_status serve_filter(rc_ctx* ctx, rc_op* op, void* V, int64_t ld, int64_t s, i
     RC_CU(ctx, cudaStreamWaitEvent(ctx->stream, pj.done, 0));
     *handled = true;
     return RC_OK;
+}
+
+rc_status serve_filter(rc_ctx* ctx, rc_op* op, void* V, int64_t ld, int64_t s, int64_t degree, double a, double b,
+                       int prec, void* bufA, void* bufB, size_t buf_bytes, bool* handled) {
+    *handled = false;
+    if (!ctx->serve) return RC_OK;
+    BatchJob job;
+    if (!batch_job_describe(ctx, op, V, ld, s, degree, a, b, prec, bufA, bufB, buf_bytes, &job)) return RC_OK;
+    return serve_post(ctx, job, handled);
+}
+
+rc_status serve_filter_corr(rc_ctx* ctx, rc_op* op, double* V, int64_t ldv, int64_t s, int64_t degree, double a,
+                            double b, const rc_corr_t* R, const float* sig, const double* coef, void* bufA,
+                            void* bufB, bool* handled) {
+    *handled = false;
+    if (!ctx->serve) return RC_OK;
+    BatchJob job;
+    if (!batch_job_describe_corr(ctx, op, V, ldv, s, degree, a, b, R, sig, coef, bufA, bufB, &job)) return RC_OK;
+    return serve_post(ctx, job, handled);
 }
 
 }  // namespace rcb

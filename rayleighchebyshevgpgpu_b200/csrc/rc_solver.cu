@@ -431,10 +431,8 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
     const bool mixed = P_.precision == RC_PREC_MIXED && op_->kind != 2;
     // relative residual at which the plain FP32 filter gives way: by default at the first
     // Rayleigh-Ritz step to the correction filter (a bfloat16 correction step moves fewer bytes than
-    // a plain FP32 step and converges like the FP64 filter), else at 1e-6 to the FP64 filter.
-    // Under the request server the plain FP32 filter runs to 1e-6 either way: its applications are
-    // the ones the server batches across solves.
-    const double switchTolSet = P_.mixed_switch_tol > 0 ? P_.mixed_switch_tol : (ctx_->serve ? 1e-6 : 0.0);
+    // a plain FP32 step and converges like the FP64 filter), else at 1e-6 to the FP64 filter
+    const double switchTolSet = P_.mixed_switch_tol > 0 ? P_.mixed_switch_tol : 0.0;
     // MIXED phases: 0 plain FP32 filter, 1 correction filter, 2 FP64 filter
     enum { PH_PLAIN32 = 0, PH_CORR32 = 1, PH_FP64 = 2 };
 
