@@ -95,6 +95,28 @@ __device__ __forceinline__ void stv(TM* p, const Slice<TS, TM>& v) {
     }
     *reinterpret_cast<uint4*>(p) = u;
 }
+// Two FP32 fused multiply-adds in one packed instruction (sm_100 fma.rn.f32x2): c_q = a_q x_q + c_q
+// rounded as two fmaf, so the packed and scalar forms give the same bits.
+__device__ __forceinline__ void ffma2(float a0, float a1, float x0, float x1, float& c0, float& c1) {
+    asm("{\n\t.reg .b64 ra, rx, rc;\n\t"
+        "mov.b64 ra, {%2, %3};\n\t"
+        "mov.b64 rx, {%4, %5};\n\t"
+        "mov.b64 rc, {%0, %1};\n\t"
+        "fma.rn.f32x2 rc, ra, rx, rc;\n\t"
+        "mov.b64 {%0, %1}, rc;\n\t}"
+        : "+f"(c0), "+f"(c1)
+        : "f"(a0), "f"(a1), "f"(x0), "f"(x1));
+}
+__device__ __forceinline__ void fmul2(float a0, float a1, float x0, float x1, float& r0, float& r1) {
+    asm("{\n\t.reg .b64 ra, rx, rr;\n\t"
+        "mov.b64 ra, {%2, %3};\n\t"
+        "mov.b64 rx, {%4, %5};\n\t"
+        "mul.rn.f32x2 rr, ra, rx;\n\t"
+        "mov.b64 {%0, %1}, rr;\n\t}"
+        : "=f"(r0), "=f"(r1)
+        : "f"(a0), "f"(a1), "f"(x0), "f"(x1));
+}
+
 __device__ __forceinline__ float elem_f(float v) { return v; }
 __device__ __forceinline__ float elem_f(__nv_bfloat16 v) { return __bfloat162float(v); }
 
@@ -168,6 +190,8 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
     // source coefficients: held in registers, or (bfloat16 blocks, 8 columns per thread, where
     // registers bound the resident CTAs) re-read from L1 per row
     constexpr bool kSigReg = sizeof(TM) != 2;
+    // bfloat16 blocks (TS = TC = float): the FP32 arithmetic in packed pairs (ffma2, fmul2)
+    constexpr bool kPacked = sizeof(TM) == 2;
     TC sg[SRC && kSigReg ? W * V : 1];
     if (SRC && kSigReg) {
 #pragma unroll
@@ -205,8 +229,14 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
 #pragma unroll
             for (int w = 0; w < W; ++w) {
                 const Slice<TS, TM> p = ldv_ro<TS, TM>(xj + w * wstride);
+                if constexpr (kPacked) {
 #pragma unroll
-                for (int v = 0; v < V; ++v) acc[w * V + v] = s_fma(a, s_cvt<TC>(p.v[v]), acc[w * V + v]);
+                    for (int v = 0; v < V; v += 2)
+                        ffma2(a, a, p.v[v], p.v[v + 1], acc[w * V + v], acc[w * V + v + 1]);
+                } else {
+#pragma unroll
+                    for (int v = 0; v < V; ++v) acc[w * V + v] = s_fma(a, s_cvt<TC>(p.v[v]), acc[w * V + v]);
+                }
             }
         });
 #pragma unroll
@@ -214,7 +244,22 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
             const IX o = oi + w * wstride;
             const Slice<TS, TM> xi = ldv_ro<TS, TM>(x + o);
             Slice<TS, TM> out;
-            if (SRC) {
+            if constexpr (SRC && kPacked) {
+                const Slice<TS, TM> si = ldv_ro<TS, TM>(src + o);
+                const Slice<TS, TM> zi = z ? ldv<TS, TM>(z + o) : Slice<TS, TM>{};
+                const float* sgp = sig + off + w * wstride;
+#pragma unroll
+                for (int v = 0; v < V; v += 2) {
+                    const float2 sg2 = __ldg(reinterpret_cast<const float2*>(sgp + v));
+                    float r0, r1;
+                    fmul2(alpha, alpha, acc[w * V + v], acc[w * V + v + 1], r0, r1);
+                    ffma2(beta, beta, xi.v[v], xi.v[v + 1], r0, r1);
+                    if (z) ffma2(gamma, gamma, zi.v[v], zi.v[v + 1], r0, r1);
+                    ffma2(sg2.x, sg2.y, si.v[v], si.v[v + 1], r0, r1);
+                    out.v[v] = r0;
+                    out.v[v + 1] = r1;
+                }
+            } else if (SRC) {
                 const Slice<TS, TM> si = ldv_ro<TS, TM>(src + o);
                 const Slice<TS, TM> zi = z ? ldv<TS, TM>(z + o) : Slice<TS, TM>{};
 #pragma unroll
