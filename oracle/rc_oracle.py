@@ -7,6 +7,9 @@ Each function restates the reference routine it cites (paths relative to the ref
   pm, pm_prime, pm_prime_first_root, inverse_pm, xstar, upper_xstar, star_degree_and_bound
       LanczosCpoly.h:234-270, :400-415, :371-398, :416-473, :285-305, :498-555
   filter_block   LanczosCpolyOperatorLM.h:192-304 (same recurrence as LanczosCpolyOperatorLMCuda.h:194-265)
+  correction_filter  no reference counterpart: the same filter written on Ritz pairs as
+                 x_k = c_k(lambda) v + a e_k (the MIXED-precision correction form), with the storage
+                 rounding of R and e_k as a parameter (round_bf16 emulates bfloat16 storage)
   lanczos_bounds LanczosMaxMinFinder.h:248-544 (tridiagonal extremes by LAPACK dstebz there,
                  by scipy's eigvalsh_tridiagonal here)
   solve          RayleighChebyshevLM.h:712-1776 (getMinEigenSystem and its base routine), with the
@@ -173,6 +176,48 @@ def filter_block(A, X: np.ndarray, m: int, g1: float, g2: float, reps: int = 1) 
             vnm2, vnm1 = vnm1, vn
         V = vnm1 * (1.0 / (m + 1))
     return V
+
+
+def round_bf16(x) -> np.ndarray:
+    """Values rounded to bfloat16 (round to nearest, ties to even, via float32), returned as float64:
+    the storage rounding of the correction filter's blocks."""
+    f = np.ascontiguousarray(x, dtype=np.float32)
+    u = f.view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def correction_filter(A, V: np.ndarray, lam: np.ndarray, m: int, g1: float, g2: float, store=None) -> np.ndarray:
+    """filter_block(A, V, m, g1, g2) written on Ritz pairs (v_c, lam_c). With a = g2 g1, b = g2 and the
+    scalar recurrence c_0 = 1, c_1 = a lam + b, c_k = (a lam + b) c_{k-1} - c_{k-2}, the filter's
+    x_k = (aA + b) x_{k-1} - x_{k-2} is x_k = c_k v + a e_k with
+        e_0 = 0, e_1 = R = A V - V diag(lam), e_k = (aA + b) e_{k-1} - e_{k-2} + c_{k-1} R,
+    and the result is x_m/(m+1) = (c_m v + a e_m)/(m+1). `store` rounds R and every e_k as stored
+    (None: exact); the rest is float64. No reference counterpart (the MIXED-precision refinement)."""
+    rnd = store if store is not None else (lambda x: x)
+    a, b = g2 * g1, g2
+    lam = np.asarray(lam, dtype=np.float64)
+    R = rnd(A @ V - V * lam)
+    t = a * lam + b
+    cm2, cm1 = np.ones_like(lam), t.copy()  # c_0, c_1
+    em2, em1 = np.zeros_like(V), R            # e_0, e_1
+    for _k in range(2, m + 1):
+        ek = rnd(a * (A @ em1) + b * em1 - em2 + cm1 * R)
+        cm2, cm1 = cm1, t * cm1 - cm2
+        em2, em1 = em1, ek
+    return (cm1 * V + a * em1) / (m + 1)
+
+
+def filter_block_stored(A, X: np.ndarray, m: int, g1: float, g2: float, store) -> np.ndarray:
+    """filter_block with every intermediate x_k rounded by `store` (the plain reduced-precision
+    filter, for comparison with correction_filter)."""
+    V = store(np.array(X, copy=True))
+    vnm2 = V
+    vnm1 = store(g2 * (g1 * (A @ V) + V))
+    for _k in range(2, m + 1):
+        vn = store(g2 * (g1 * (A @ vnm1) + vnm1) - vnm2)
+        vnm2, vnm1 = vnm1, vn
+    return vnm1 * (1.0 / (m + 1))
 
 
 # ------------------------------------------------------------------------------------------
