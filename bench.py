@@ -187,11 +187,11 @@ def run_ours(args):
     import torch.distributed as dist
 
     from rayleighchebyshevgpgpu_b200 import problems
+    from rayleighchebyshevgpgpu_b200 import replicas
     from rayleighchebyshevgpgpu_b200 import runtime as R
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    env = replicas.rank_env()
+    world, rank, local = env.world, env.rank, env.local
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
@@ -201,11 +201,7 @@ def run_ours(args):
             dist.barrier()
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, world, device="cuda")
 
     P = problems.config2(args.side)
     incr, buf = problems.block_sizes(P.k)
@@ -307,7 +303,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         if i > 0:
             e2e_t.append(time.perf_counter() - t0)
-    e2e_value = P.k * world / max_over_ranks(statistics.median(e2e_t))
+    e2e_value = replicas.job_rate(P.k, world, max_over_ranks(statistics.median(e2e_t)))
     assert np.array_equal(res_e.evals, res_mixed.evals)
 
     # ---- roofline of the dominant kernel: the fused filter degree-step (rm_step_kernel) ----
@@ -365,7 +361,7 @@ def run_ours(args):
             cpu = {"value": None, "unit": "eigenpairs/s", "cores": None, "kind": "reference",
                    "sample": f"unavailable: {e}"}
 
-    value = P.k * world / (t_mixed * 1e-3)
+    value = replicas.job_rate(P.k, world, t_mixed * 1e-3)
     line = {
         "metric": METRIC, "value": value, "unit": "eigenpairs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_mixed, "higher_is_better": True, "scaling": "weak",
@@ -374,7 +370,7 @@ def run_ours(args):
         "tts_ms": {"mixed_p50": statistics.median(times), "mixed_p99": float(np.percentile(times, 99)),
                    "fp64_p50": statistics.median(t64) if t64 else None,
                    "fp64_p99": float(np.percentile(t64, 99)) if t64 else None},
-        "fp64_eigenpairs_per_s": P.k * world / (t_fp64 * 1e-3) if t_fp64 else None,
+        "fp64_eigenpairs_per_s": replicas.job_rate(P.k, world, t_fp64 * 1e-3) if t_fp64 else None,
         "speedup_mixed_vs_fp64": (t_fp64 / t_mixed) if t_fp64 else None,
         "accuracy": {"max_rel_eig_diff_mixed_vs_fp64": eig_err, "max_subspace_angle_mixed_vs_fp64": angle,
                      "max_rel_residual": max_res_rel, "found": int(res_mixed.info["found"])},
