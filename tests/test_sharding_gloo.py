@@ -1,0 +1,122 @@
+"""Row sharding of the solve (rayleighchebyshevgpgpu_b200/sharding.py) on the CPU: the slab partition and
+halo plan, and, on 2 and 3 gloo ranks, a sharded Chebyshev filter (halo exchange per degree step) and a
+sharded Gram matrix (all-reduce) against the single-process oracle."""
+import json
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from oracle import rc_oracle as O
+from rayleighchebyshevgpgpu_b200 import problems
+from rayleighchebyshevgpgpu_b200 import sharding as S
+
+DIMS = (8, 6, 10)   # nx, ny, nz: z-slabs of nx*ny = 48 rows
+S_COLS = 5
+DEGREE = 7
+
+
+def _problem():
+    P = problems.small_laplacian(DIMS, seed=9, vmax=2.0, k=4)
+    rp, ci, v = P.csr()
+    return P, np.asarray(rp), np.asarray(ci), np.asarray(v)
+
+
+def _block(n):
+    return np.random.default_rng(4).standard_normal((n, S_COLS))
+
+
+def test_partition_rows_whole_planes():
+    r = S.partition_rows(480, 3, quantum=48)
+    assert r == [(0, 192), (192, 336), (336, 480)]
+    assert S.partition_rows(10, 4) == [(0, 3), (3, 6), (6, 8), (8, 10)]
+    with pytest.raises(ValueError):
+        S.partition_rows(480, 11, quantum=48)
+    with pytest.raises(ValueError):
+        S.partition_rows(100, 2, quantum=48)
+
+
+def test_shard_plan_halos_are_neighbouring_planes():
+    P, rp, ci, v = _problem()
+    plan = S.shard_plan(rp, ci, S.partition_rows(P.n, 3, quantum=48))
+    assert [(s.lo, s.hi) for s in plan] == [(0, 48), (48, 48), (48, 0)]
+    assert [(s.send_down, s.send_up) for s in plan] == [(0, 48), (48, 48), (48, 0)]
+    lrp, lci, lv = S.local_csr(rp, ci, v, plan[1])
+    assert lrp[0] == 0 and lrp[-1] == lci.size == lv.size
+    assert lci.min() >= 0 and lci.max() < plan[1].ext_rows
+
+
+def test_shard_plan_rejects_couplings_beyond_the_neighbour():
+    n = 12
+    rows = [[i, (i + 7) % n] for i in range(n)]  # couples each row 7 rows away (wraps)
+    rp = np.cumsum([0] + [len(r) for r in rows])
+    ci = np.concatenate([sorted(r) for r in rows])
+    with pytest.raises(ValueError):
+        S.shard_plan(rp, ci, S.partition_rows(n, 3))
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank: int, world: int, port: int, out_dir: str):
+    import datetime
+
+    import scipy.sparse as sp
+    import torch
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        P, rp, ci, v = _problem()
+        plan = S.shard_plan(rp, ci, S.partition_rows(P.n, world, quantum=DIMS[0] * DIMS[1]))
+        sh = plan[rank]
+        lrp, lci, lv = S.local_csr(rp, ci, v, sh)
+        A_l = sp.csr_matrix((lv, lci, lrp), shape=(sh.rows, sh.ext_rows))
+        X = _block(P.n)
+        g1, g2 = O.gammas(DEGREE, 14.0, -0.5)
+        own = slice(sh.lo, sh.lo + sh.rows)
+        # x_k = g2 (g1 A x_{k-1} + x_{k-1}) - x_{k-2}, one halo exchange of x_{k-1} per step
+        ext = torch.zeros((sh.ext_rows, S_COLS), dtype=torch.float64)
+        ext[own] = torch.from_numpy(X[sh.r0:sh.r1])
+        xkm2 = ext[own].clone()
+        S.exchange_halo(ext, sh)
+        xk = g2 * (g1 * torch.from_numpy(A_l @ ext.numpy()) + ext[own])
+        for _k in range(2, DEGREE + 1):
+            nxt = torch.zeros_like(ext)
+            nxt[own] = xk
+            S.exchange_halo(nxt, sh)
+            y = g2 * (g1 * torch.from_numpy(A_l @ nxt.numpy()) + xk) - xkm2
+            xkm2, xk = xk, y
+        filt = (xk / (DEGREE + 1)).numpy()
+        # Gram matrix of the filtered block: local product, summed over ranks
+        G = torch.from_numpy(filt.T @ filt)
+        S.allreduce_sum(G)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+    np.save(os.path.join(out_dir, f"filt{rank}.npy"), filt)
+    np.save(os.path.join(out_dir, f"gram{rank}.npy"), G.numpy())
+    with open(os.path.join(out_dir, f"rank{rank}.json"), "w") as f:
+        json.dump({"r0": sh.r0, "r1": sh.r1}, f)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_filter_and_gram_match_the_oracle(tmp_path, world):
+    mp.start_processes(_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    P, rp, ci, v = _problem()
+    A = O.csr_matrix(rp, ci, v)
+    g1, g2 = O.gammas(DEGREE, 14.0, -0.5)
+    F = O.filter_block(A, _block(P.n), DEGREE, g1, g2)
+    G = F.T @ F
+    for r in range(world):
+        rng = json.load(open(tmp_path / f"rank{r}.json"))
+        filt = np.load(tmp_path / f"filt{r}.npy")
+        np.testing.assert_allclose(filt, F[rng["r0"]:rng["r1"]], rtol=0, atol=1e-13 * np.abs(F).max())
+        np.testing.assert_allclose(np.load(tmp_path / f"gram{r}.npy"), G, rtol=1e-12, atol=1e-12 * np.abs(G).max())
