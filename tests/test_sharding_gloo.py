@@ -1,6 +1,8 @@
 """Row sharding of the solve (rayleighchebyshevgpgpu_b200/sharding.py) on the CPU: the slab partition and
-halo plan, and, on 2 and 3 gloo ranks, a sharded Chebyshev filter (halo exchange per degree step) and a
-sharded Gram matrix (all-reduce) against the single-process oracle."""
+halo plan, and, on 2 and 3 gloo ranks, a sharded Chebyshev filter (halo exchange per degree step), a
+sharded Gram matrix (all-reduce) and a whole sharded filter + Rayleigh-Ritz step (Gram and projection
+all-reduces, replicated small eigensolve, residual norms by all-reduce) against one process. The
+per-rank arithmetic here is numpy; on GPUs it is the library's kernels."""
 import json
 import os
 import socket
@@ -120,3 +122,77 @@ def test_sharded_filter_and_gram_match_the_oracle(tmp_path, world):
         filt = np.load(tmp_path / f"filt{r}.npy")
         np.testing.assert_allclose(filt, F[rng["r0"]:rng["r1"]], rtol=0, atol=1e-13 * np.abs(F).max())
         np.testing.assert_allclose(np.load(tmp_path / f"gram{r}.npy"), G, rtol=1e-12, atol=1e-12 * np.abs(G).max())
+
+
+def _rr_single(A, X, m, g1, g2):
+    """One filter + Rayleigh-Ritz step on one process: filtered block F, CholeskyQR basis, Ritz values
+    and residual norms of the Ritz vectors."""
+    F = O.filter_block(A, X, m, g1, g2)
+    G = F.T @ F
+    Lc = np.linalg.cholesky(G)
+    T = np.linalg.inv(Lc).T                      # F T has orthonormal columns
+    H = T.T @ (F.T @ (A @ F)) @ T
+    lam, Q = np.linalg.eigh(0.5 * (H + H.T))
+    Y = F @ (T @ Q)
+    res = np.linalg.norm(A @ Y - Y * lam, axis=0)
+    return lam, res
+
+
+def _rr_rank_main(rank: int, world: int, port: int, out_dir: str):
+    import datetime
+
+    import scipy.sparse as sp
+    import torch
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        P, rp, ci, v = _problem()
+        plan = S.shard_plan(rp, ci, S.partition_rows(P.n, world, quantum=DIMS[0] * DIMS[1]))
+        sh = plan[rank]
+        lrp, lci, lv = S.local_csr(rp, ci, v, sh)
+        A_l = sp.csr_matrix((lv, lci, lrp), shape=(sh.rows, sh.ext_rows))
+        own = slice(sh.lo, sh.lo + sh.rows)
+
+        def apply(x_own):  # A x on the own rows: one halo exchange, then the local product
+            ext = torch.zeros((sh.ext_rows, x_own.shape[1]), dtype=torch.float64)
+            ext[own] = torch.from_numpy(x_own)
+            S.exchange_halo(ext, sh)
+            return A_l @ ext.numpy()
+
+        def allsum(a):
+            return S.allreduce_sum(torch.from_numpy(np.ascontiguousarray(a))).numpy()
+
+        g1, g2 = O.gammas(DEGREE, 14.0, -0.5)
+        X = _block(P.n)[sh.r0:sh.r1]
+        xkm2, xk = X, g2 * (g1 * apply(X) + X)
+        for _k in range(2, DEGREE + 1):
+            xkm2, xk = xk, g2 * (g1 * apply(xk) + xk) - xkm2
+        F = xk / (DEGREE + 1)
+        G = allsum(F.T @ F)                              # Gram: one all-reduce
+        T = np.linalg.inv(np.linalg.cholesky(G)).T       # replicated small work
+        AF = apply(F)
+        H = T.T @ allsum(F.T @ AF) @ T                   # projection: one all-reduce
+        lam, Q = np.linalg.eigh(0.5 * (H + H.T))         # replicated small eigensolve
+        TQ = T @ Q
+        Y, AY = F @ TQ, AF @ TQ
+        res = np.sqrt(allsum(np.sum((AY - Y * lam) ** 2, axis=0)))  # residual norms: one all-reduce
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+    np.save(os.path.join(out_dir, f"rr{rank}.npy"), np.stack([lam, res]))
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_rayleigh_ritz_step_matches_single_process(tmp_path, world):
+    mp.start_processes(_rr_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    P, rp, ci, v = _problem()
+    A = O.csr_matrix(rp, ci, v)
+    g1, g2 = O.gammas(DEGREE, 14.0, -0.5)
+    lam, res = _rr_single(A, _block(P.n), DEGREE, g1, g2)
+    for r in range(world):
+        got = np.load(tmp_path / f"rr{r}.npy")
+        np.testing.assert_allclose(got[0], lam, rtol=1e-12, atol=1e-12)       # every rank, the same Ritz values
+        np.testing.assert_allclose(got[1], res, rtol=1e-8, atol=1e-10 * np.abs(lam).max())
