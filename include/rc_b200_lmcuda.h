@@ -31,6 +31,7 @@
 #include <complex>
 #include <cstdint>
 #include <cstring>
+#include <iosfwd>
 #include <map>
 #include <stdexcept>
 #include <string>
@@ -51,6 +52,21 @@
 #endif
 
 namespace rcb200 {
+
+/* The stop-condition names of the reference's RC_Types.h, in the order of RC_STOP_*. */
+struct RC_Types {
+    enum StopCondition { DEFAULT, COMBINATION, EIGENVALUE_ONLY, RESIDUAL_ONLY };
+};
+
+/* The RC_STOP_* value of a StopCondition enumerator (this header's RC_Types, or the reference's
+ * global RC_Types when the caller still includes RC_Types.h): DEFAULT means COMBINATION. */
+template <class E>
+inline int stop_condition_value(E e) {
+    static_assert(std::is_enum<E>::value, "a StopCondition enumerator");
+    const int v = (int)e;
+    if (v < RC_STOP_DEFAULT || v > RC_STOP_RESIDUAL_ONLY) throw std::runtime_error("setStopCondition: unknown stop condition");
+    return v == RC_STOP_DEFAULT ? RC_STOP_COMBINATION : v;
+}
 
 template <class D> struct dtype_of;
 template <> struct dtype_of<double> { static constexpr int value = RC_REAL64; };
@@ -145,13 +161,33 @@ public:
         else if (s == "RESIDUAL_ONLY") p_.stop_condition = RC_STOP_RESIDUAL_ONLY;
         else throw std::runtime_error("setStopCondition: unknown stop condition " + s);
     }
+    // the enum form (:370-395)
+    template <class E, typename std::enable_if<std::is_enum<E>::value, int>::type = 0>
+    void setStopCondition(E e) { p_.stop_condition = stop_condition_value(e); }
     void setMaxMinTolerance(double val = 1.0e-6) { p_.max_min_tol = val; }
     void setMaxInnerLoopCount(RAY_INT val) { p_.max_inner_loop = val; }
+    // a fixed inner iteration count (:419) is not offered by the GPU solver
+    void setFixedIterationCount(bool val) {
+        if (val) throw std::runtime_error("setFixedIterationCount: fixed iteration counts are not supported");
+    }
     void setNonRandomStartFlag(bool val = true) { nonRandomStart_ = val; }
     void setVerboseFlag(bool val = true) { p_.verbose = val ? 1 : 0; }
     void setMinIntervalPolyDegreeMax(RAY_INT polyDegMax) { p_.poly_degree_max = polyDegMax; }
     void setFilterRepetitionCount(RAY_INT repetitionCount) { p_.filter_repetition = repetitionCount; }
     void setMaxSpectralBoundsIter(RAY_INT iterCount) { p_.lanczos_max_iter = iterCount; }
+    // Host-implementation switches, accepted for source compatibility: the small eigensolve is always
+    // the GPU Jacobi, verbose lines go to stdout, and there is no per-subspace or eigen-diagnostic output.
+    void setVerboseSubspaceFlag(bool = true) {}
+    void setEigDiagnosticsFlag(bool = true) {}
+    void setUseJacobi(bool) {}
+    void setResultsStream(std::ostream&) {}
+    // The interval stop rules (:494-512): each entry point here selects its own, as the reference's
+    // entry points set them (getMinEigenSystem: hard stop at the bound; getMinIntervalEigenSystem: the
+    // guard-eigenvalue test), so the toggles are accepted and have no effect.
+    void setIntervalStopCondition(bool = true) {}
+    void clearIntervalStopCondition() {}
+    void setHardIntervalStop(bool = true) {}
+    void clearHardIntervalStop() {}
     // no reference counterpart: FP32 filter with FP64 Rayleigh-Ritz (RC_PREC_MIXED), and the
     // per-phase CUDA-event timing behind getTimingData
     void setMixedPrecision(bool val = true) { p_.precision = val ? RC_PREC_MIXED : RC_PREC_FP64; }
@@ -188,7 +224,10 @@ public:
                    subspaceIncrementSize, bufferSize, vStart, oP, randOp, eigValues, eigVectors);
     }
 
-    // ---- getters (:489, :534-560) ----
+    // ---- getters (:469-478, :489, :519, :534-560) ----
+    double getMinEigValueEst() const { return info_.min_eig_est; }
+    double getMaxEigValueEst() const { return info_.max_eig_est; }
+    RAY_INT getSpectralBoundsIterCount() const { return (RAY_INT)info_.lanczos_iterations; }
     double getGuardEigenvalue() const { return info_.guard_value; }
     std::vector<double> getEigVectorResiduals() const { return residuals_; }
     std::map<std::string, double> getFinalData() const {

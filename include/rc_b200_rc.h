@@ -68,6 +68,9 @@ public:
         else if (s == "RESIDUAL_ONLY") p_.stop_condition = RC_STOP_RESIDUAL_ONLY;
         else throw std::runtime_error("RayleighChebyshev: unknown stopping condition " + s);
     }
+    // the enum form (:309-338)
+    template <class E, typename std::enable_if<std::is_enum<E>::value, int>::type = 0>
+    void setStopCondition(E e) { p_.stop_condition = stop_condition_value(e); }
     void setMaxMinTolerance(double val = 1.0e-6) { p_.max_min_tol = val; }
     void setMaxInnerLoopCount(long val) { p_.max_inner_loop = val; }
     void setNonRandomStartFlag(bool val = true) { nonRandomStart_ = val; }
@@ -86,6 +89,12 @@ public:
     void setEigDiagnosticsFlag(bool = true) {}
     void setUseJacobi(bool) {}
     void setResultsStream(std::ostream&) {}
+    // the interval stop rules (:402-420): each entry point selects its own, as the reference's entry
+    // points set them, so the toggles are accepted and have no effect
+    void setIntervalStopCondition(bool = true) {}
+    void clearIntervalStopCondition() {}
+    void setHardIntervalStop(bool = true) {}
+    void clearHardIntervalStop() {}
     // no reference counterpart: FP32 / bfloat16 filter with FP64 Rayleigh-Ritz (RC_PREC_MIXED), and
     // per-phase CUDA-event timing behind getTimingData
     void setMixedPrecision(bool val = true) { p_.precision = val ? RC_PREC_MIXED : RC_PREC_FP64; }

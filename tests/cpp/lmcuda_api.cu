@@ -69,6 +69,11 @@ template <class Op>
 static void run(const char* name, Op& op, long n, int k) {
     rcb200::RayleighChebyshevLMCuda<Mat<double>, Vec<double>, Op, Rand, double> rc;
     rc.setStopCondition("RESIDUAL_ONLY");
+    rc.setStopCondition(rcb200::RC_Types::RESIDUAL_ONLY);  // the enum form, same condition
+    rc.setUseJacobi(true);                                  // host-implementation switches: no effect
+    rc.setVerboseSubspaceFlag(false);
+    rc.setEigDiagnosticsFlag(false);
+    rc.setFixedIterationCount(false);
     Vec<double> vStart(n);
     Rand rnd;
     std::vector<double> evals;
@@ -80,8 +85,9 @@ static void run(const char* name, Op& op, long n, int k) {
     for (long i = 0; i < found; ++i) std::printf("%s%.17g", i ? ", " : "", evals[i]);
     std::printf("], \"residuals\": [");
     for (long i = 0; i < found; ++i) std::printf("%s%.6g", i ? ", " : "", res[i]);
-    std::printf("], \"opapply\": %ld, \"evec0\": [%.17g, %.17g]}\n", (long)counts.at("OpApply"), evecs.mData[0],
-                evecs.mData[1]);
+    std::printf("], \"opapply\": %ld, \"evec0\": [%.17g, %.17g], \"bounds\": [%.17g, %.17g], \"lanczos\": %ld}\n",
+                (long)counts.at("OpApply"), evecs.mData[0], evecs.mData[1], rc.getMinEigValueEst(),
+                rc.getMaxEigValueEst(), (long)rc.getSpectralBoundsIterCount());
 }
 
 int main() {

@@ -73,6 +73,11 @@ template <class Op>
 static void run(const char* name, Op& op, long n, int k) {
     rcb200::RayleighChebyshev<Vec, Op, Rand, double> rc;
     rc.setStopCondition("residual_only");
+    rc.setStopCondition(rcb200::RC_Types::RESIDUAL_ONLY);  // the enum form, same condition
+    rc.setUseJacobi(true);                                  // CPU-implementation switches: no effect
+    rc.setVerboseSubspaceFlag(false);
+    rc.setEigDiagnosticsFlag(false);
+    rc.setIntervalStopCondition(false);
     Vec vStart(n);
     Rand rnd;
     std::vector<double> evals;

@@ -61,6 +61,7 @@ def test_interface_three_operator_kinds_match_lapack(tmp_path, built_lib):
         np.testing.assert_allclose(d["evals"], dense, rtol=1e-10)
         ev = np.asarray(d["evals"])
         assert np.max(np.asarray(d["residuals"]) / np.abs(ev)) <= 1e-10, d
-        assert d["opapply"] > 0
+        assert d["opapply"] > 0 and d["lanczos"] > 0
+        assert abs(d["bounds"][0] - dense[0]) <= 1e-2 * abs(dense[0]) and d["bounds"][1] > dense[-1], d
     # the fused CSR and stencil forms of the same matrix agree to rounding
     np.testing.assert_allclose(rows[0]["evals"], rows[1]["evals"], rtol=1e-12)
