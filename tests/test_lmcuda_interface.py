@@ -65,3 +65,26 @@ def test_interface_three_operator_kinds_match_lapack(tmp_path, built_lib):
         assert abs(d["bounds"][0] - dense[0]) <= 1e-2 * abs(dense[0]) and d["bounds"][1] > dense[-1], d
     # the fused CSR and stencil forms of the same matrix agree to rounding
     np.testing.assert_allclose(rows[0]["evals"], rows[1]["evals"], rtol=1e-12)
+
+
+def test_stop_condition_enumerators_map_to_the_c_abi(tmp_path):
+    """setStopCondition's enum form: the reference's RC_Types order (DEFAULT, COMBINATION, EIGENVALUE_ONLY,
+    RESIDUAL_ONLY) maps onto RC_STOP_*, DEFAULT meaning COMBINATION; a foreign enum with the same order works."""
+    src = tmp_path / "stop.cpp"
+    src.write_text(
+        '#include <cstdio>\n#include "rc_b200_lmcuda.h"\n'
+        'struct RC_Types { enum StopCondition {DEFAULT, COMBINATION, EIGENVALUE_ONLY, RESIDUAL_ONLY}; };\n'
+        'int main() {\n'
+        '  using R = rcb200::RC_Types;\n'
+        '  std::printf("%d %d %d %d %d %d\\n", rcb200::stop_condition_value(R::DEFAULT),\n'
+        '    rcb200::stop_condition_value(R::COMBINATION), rcb200::stop_condition_value(R::EIGENVALUE_ONLY),\n'
+        '    rcb200::stop_condition_value(R::RESIDUAL_ONLY), rcb200::stop_condition_value(::RC_Types::RESIDUAL_ONLY),\n'
+        '    RC_STOP_RESIDUAL_ONLY);\n'
+        '  return 0;\n}\n')
+    exe = str(tmp_path / "stop")
+    gxx = shutil.which("g++") or "g++"
+    r = subprocess.run([gxx, "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include",
+                        str(src), "-o", exe], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=60).stdout.split()
+    assert out == ["1", "1", "2", "3", "3", "3"]
