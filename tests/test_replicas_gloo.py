@@ -2,7 +2,6 @@
 ranks), on the CPU with two gloo ranks."""
 import json
 import os
-import socket
 
 import pytest
 import torch.multiprocessing as mp
@@ -10,21 +9,16 @@ import torch.multiprocessing as mp
 from rayleighchebyshevgpgpu_b200 import replicas
 
 
-def _free_port() -> int:
-    with socket.socket() as s:
-        s.bind(("127.0.0.1", 0))
-        return s.getsockname()[1]
-
-
-def _rank_main(rank: int, world: int, port: int, out_dir: str):
+def _rank_main(rank: int, world: int, out_dir: str):
     import datetime
 
     import torch.distributed as dist
 
-    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(world), RANK=str(rank),
-                      LOCAL_RANK=str(rank))
+    os.environ.update(WORLD_SIZE=str(world), RANK=str(rank), LOCAL_RANK=str(rank))
     env = replicas.rank_env()
-    dist.init_process_group("gloo", rank=env.rank, world_size=env.world, timeout=datetime.timedelta(seconds=60))
+    # rendezvous through a file in the test's directory: no ports to collide
+    dist.init_process_group("gloo", init_method="file://" + os.path.join(out_dir, "store"), rank=env.rank,
+                            world_size=env.world, timeout=datetime.timedelta(seconds=60))
     try:
         # each rank's own device time; the slowest sets the job's time
         mine = 1.5 + env.rank
@@ -49,7 +43,7 @@ def test_single_process_defaults(monkeypatch):
 
 def test_two_gloo_ranks_take_the_slowest_time(tmp_path):
     world = 2
-    mp.start_processes(_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+    mp.start_processes(_rank_main, args=(world, str(tmp_path)), nprocs=world, join=True,
                        start_method="spawn")
     rows = [json.load(open(tmp_path / f"rank{r}.json")) for r in range(world)]
     for r, d in enumerate(rows):

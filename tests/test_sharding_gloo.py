@@ -5,7 +5,6 @@ all-reduces, replicated small eigensolve, residual norms by all-reduce) against 
 per-rank arithmetic here is numpy; on GPUs it is the library's kernels."""
 import json
 import os
-import socket
 
 import numpy as np
 import pytest
@@ -59,21 +58,16 @@ def test_shard_plan_rejects_couplings_beyond_the_neighbour():
         S.shard_plan(rp, ci, S.partition_rows(n, 3))
 
 
-def _free_port() -> int:
-    with socket.socket() as s:
-        s.bind(("127.0.0.1", 0))
-        return s.getsockname()[1]
-
-
-def _rank_main(rank: int, world: int, port: int, out_dir: str):
+def _rank_main(rank: int, world: int, out_dir: str):
     import datetime
 
     import scipy.sparse as sp
     import torch
     import torch.distributed as dist
 
-    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
-    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    # rendezvous through a file in the test's directory: no ports to collide
+    dist.init_process_group("gloo", init_method="file://" + os.path.join(out_dir, "store"), rank=rank,
+                            world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
         P, rp, ci, v = _problem()
         plan = S.shard_plan(rp, ci, S.partition_rows(P.n, world, quantum=DIMS[0] * DIMS[1]))
@@ -110,7 +104,7 @@ def _rank_main(rank: int, world: int, port: int, out_dir: str):
 
 @pytest.mark.parametrize("world", [2, 3])
 def test_sharded_filter_and_gram_match_the_oracle(tmp_path, world):
-    mp.start_processes(_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+    mp.start_processes(_rank_main, args=(world, str(tmp_path)), nprocs=world, join=True,
                        start_method="spawn")
     P, rp, ci, v = _problem()
     A = O.csr_matrix(rp, ci, v)
@@ -138,15 +132,16 @@ def _rr_single(A, X, m, g1, g2):
     return lam, res
 
 
-def _rr_rank_main(rank: int, world: int, port: int, out_dir: str):
+def _rr_rank_main(rank: int, world: int, out_dir: str):
     import datetime
 
     import scipy.sparse as sp
     import torch
     import torch.distributed as dist
 
-    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
-    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    # rendezvous through a file in the test's directory: no ports to collide
+    dist.init_process_group("gloo", init_method="file://" + os.path.join(out_dir, "store"), rank=rank,
+                            world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
         P, rp, ci, v = _problem()
         plan = S.shard_plan(rp, ci, S.partition_rows(P.n, world, quantum=DIMS[0] * DIMS[1]))
@@ -186,7 +181,7 @@ def _rr_rank_main(rank: int, world: int, port: int, out_dir: str):
 
 @pytest.mark.parametrize("world", [2, 3])
 def test_sharded_rayleigh_ritz_step_matches_single_process(tmp_path, world):
-    mp.start_processes(_rr_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+    mp.start_processes(_rr_rank_main, args=(world, str(tmp_path)), nprocs=world, join=True,
                        start_method="spawn")
     P, rp, ci, v = _problem()
     A = O.csr_matrix(rp, ci, v)
