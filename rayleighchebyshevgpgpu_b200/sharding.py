@@ -15,7 +15,10 @@ on the CPU):
   shard_plan       each rank's rows, halo extent and neighbours' halo needs, from the CSR pattern;
   local_csr        the rank's rows with columns rebased to its extended block [halo_lo | own | halo_hi];
   exchange_halo    fills the halo rows of an extended row-major block from the neighbours;
-  allreduce_sum    sums a Gram matrix (or any tensor) over ranks.
+  allreduce_sum    sums a Gram matrix (or any tensor) over ranks;
+  extended_csr     the rank's operator on its whole extended block, halo rows empty: with it, one
+                   unsharded row-major degree step over the extended block computes the rank's rows
+                   (the halo rows of the result are discarded and refilled by the next exchange).
 The device side of the sharded solve (the degree-step kernel reading the extended block, with the
 exchange between steps) is not part of this build: every run here has one GPU.
 """
@@ -134,3 +137,11 @@ def allreduce_sum(t, group=None):
 
     dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
     return t
+
+
+def extended_csr(rowptr, colind, vals, sh: Shard):
+    """The rank's operator as a square CSR matrix on its extended block (ext_rows rows): its own rows
+    at [lo, lo + rows) with columns in the extended numbering, the halo rows empty."""
+    lrp, lci, lv = local_csr(rowptr, colind, vals, sh)
+    rp = np.concatenate([np.zeros(sh.lo, dtype=np.int32), lrp, np.full(sh.hi, lrp[-1], dtype=np.int32)])
+    return rp, lci, lv

@@ -191,3 +191,19 @@ def test_sharded_rayleigh_ritz_step_matches_single_process(tmp_path, world):
         got = np.load(tmp_path / f"rr{r}.npy")
         np.testing.assert_allclose(got[0], lam, rtol=1e-12, atol=1e-12)       # every rank, the same Ritz values
         np.testing.assert_allclose(got[1], res, rtol=1e-8, atol=1e-10 * np.abs(lam).max())
+
+
+def test_extended_csr_is_square_with_empty_halo_rows():
+    P, rp, ci, v = _problem()
+    plan = S.shard_plan(rp, ci, S.partition_rows(P.n, 3, quantum=48))
+    for sh in plan:
+        erp, eci, ev = S.extended_csr(rp, ci, v, sh)
+        assert erp.size == sh.ext_rows + 1 and erp[0] == 0 and erp[-1] == eci.size == ev.size
+        assert np.all(np.diff(erp[:sh.lo + 1]) == 0) and np.all(np.diff(erp[sh.lo + sh.rows:]) == 0)
+        assert eci.min() >= 0 and eci.max() < sh.ext_rows
+        # the own rows of the extended operator times an extended block equal the global rows
+        E = O.csr_matrix(erp, eci, ev)
+        A = O.csr_matrix(rp, ci, v)
+        x = _block(P.n)
+        xe = x[sh.r0 - sh.lo:sh.r1 + sh.hi]
+        np.testing.assert_array_equal((E @ xe)[sh.lo:sh.lo + sh.rows], (A @ x)[sh.r0:sh.r1])
