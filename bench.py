@@ -3,10 +3,17 @@
 Workload (configuration 2): lowest 64 eigenpairs of the 3D 7-point Dirichlet Laplacian on 128^3
 (n = 2,097,152; CSR with FP64 values and int32 indices, 14,581,760 nnz) plus a U[0,4) potential
 (seed 2); start block N(0,1) (seed 3), subspace 64 + 32 buffer; stop test RESIDUAL_ONLY at 1e-10.
-A "step" is one whole solve (Lanczos bounds, filtered subspace iteration, closing FP64 sweep)
-from the operator and start block resident in HBM to eigenvalues and residuals on the host.
+A "step" is one whole solve (Lanczos bounds, then filtered subspace iteration with Rayleigh-Ritz
+until every residual <= 1e-10) from the operator and start block resident in HBM to eigenvalues
+and residuals on the host. MIXED: the first filter application in FP32, every later one as the
+correction filter (bfloat16 storage, FP32 arithmetic); everything else FP64.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--side 128]
+
+--impl reference times the reference's own CPU solver (built from its sources into oracle/_ref) on
+the same workload: each step is one bounded sample (one inner iteration of its solve), and the
+reported time-to-solution is an estimate from those samples and the iteration counts of the
+reference's own full solve of this workload (tests/golden/config2_solve.json).
 
 Multi-GPU: the solve does not shard across GPUs in this build; N processes run N independent
 replicas (one per GPU) and the value is the aggregate eigenpairs/s (weak scaling).
@@ -29,10 +36,32 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "time-to-solution & eigenpairs/s at resid<=1e-10, mixed vs FP64 on 1 B200; p50/p99"
-# Degree-steps of a whole FP64 solve of configuration 2 on the GPU path: multiplies the reference CPU
-# per-degree-step time into its time-to-solution estimate (the CPU solve itself runs for hours).
-# Measured by this bench (fp64 leg, info.degree_steps); refreshed when the solver changes.
-CONFIG2_FP64_DEGREE_STEPS = 1659
+# The reference's own CPU solve of the benchmark workload (RayleighChebyshevLM::getMinEigenSystem built
+# from its sources, run once to completion by tests/golden/make_golden_large.py): eigenvalues for the
+# parity check and the reference's own iteration and operator-apply counts for the CPU time estimate.
+REF_SOLVE_FIXTURE = os.path.join(ROOT, "tests", "golden", "config2_solve.json")
+DTYPE = "f64 (Rayleigh-Ritz, orthonormalisation, residuals); filter: bf16 storage with f32 arithmetic"
+
+
+def reference_solve_fixture(side: int):
+    try:
+        g = json.load(open(REF_SOLVE_FIXTURE))
+    except (OSError, ValueError):
+        return None
+    return g if g.get("side") == side else None
+
+
+def reference_counts(g) -> dict | None:
+    """Inner iterations and filter degree-steps of the reference's own solve, from its counters
+    (RayleighChebyshevLM.h:1224-1294): every inner iteration adds starDegree*s (filter), s
+    (formVtAV) and residualCheckCount (= incr on a single outer pass) to OpApply, and one to
+    'eigenvalue'."""
+    if not g:
+        return None
+    s = g["incr"] + g["buffer"]
+    iters = int(g["count_eigenvalue"])
+    steps = (int(g["count_opapply"]) - iters * (s + g["incr"])) // s
+    return {"inner_iterations": iters, "degree_steps": steps}
 
 
 def profile_dram_bytes_per_row():
@@ -58,7 +87,7 @@ def parse():
     ap.add_argument("--side", type=int, default=128)
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--cpu-sample-degree", type=int, default=4)
+    ap.add_argument("--cpu-sample-degree", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-count", type=int, default=64,
                     help="requests of the configuration-4 serving stream run after the timed solves (0: skip)")
@@ -112,68 +141,135 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def config_dict(args, k, incr, buf, n, nnz):
+def config_dict(args, k, incr, buf, n, nnz, world=1):
     return {"workload": f"config2: 3D 7-point Laplacian {args.side}^3 + U[0,4) potential, CSR fp64/int32, "
                         f"lowest {k} eigenpairs, tol 1e-10 RESIDUAL_ONLY",
             "n": n, "nnz": nnz, "k": k, "subspace": incr + buf, "increment": incr, "buffer": buf,
             "operator_form": "csr", "start_block": "N(0,1) seed 3",
-            "l2": "inputs larger than L2 (start block 1.6 GB, operator 183 MB)"}
+            "l2": "inputs larger than L2 (start block 1.6 GB, operator 183 MB)",
+            "parallelism": f"replicas x{world}"}
 
 
 # ---------------------------------------------------------------------------------------------
-# CPU baseline: the reference's own filter (LanczosCpolyOperatorLM::apply) built from its
-# sources (oracle/_ref), a few degree-steps on the full configuration-2 block, all host threads.
+# CPU baseline: the reference's own CPU solver (RayleighChebyshevLM, built from its sources into
+# oracle/_ref) on the full benchmark block, all host threads. One sample = one inner iteration of
+# its solve, phase by phase: `degree` filter degree-steps (LanczosCpolyOperatorLM::apply), one
+# modified Gram-Schmidt orthogonalisation, and one Rayleigh-Ritz step (formVtAV, Jacobi,
+# createEigenVectorsAndResiduals). The time-to-solution estimate is
+#   filter seconds per degree-step x the reference solve's degree-steps
+#   + (orthogonalisation + Rayleigh-Ritz seconds) x its inner iterations,
+# with both counts from the reference's own full solve of this workload (tests/golden).
 # ---------------------------------------------------------------------------------------------
-def cpu_reference_sample(P, incr, buf, degree, rp, ci, v):
-    from oracle import rc_oracle as O
-    from oracle import ref_io
-    s = incr + buf
-    threads = os.cpu_count() or 1
-    start = P.start_block(s)
-    if ref_io.ref_available():
-        d = tempfile.mkdtemp()
-        path = os.path.join(d, "c2.bin")
-        ref_io.write_problem(path, rp, ci, v, start)
-        lmin, lmax = 0.4, 10.4
-        r = ref_io.run_ref("filter", path, degree=degree, bound=lmax, shift=-lmin, reps=1, threads=threads)
-        os.remove(path)
-        return r["seconds"] / degree, threads, "reference"
-    # oracle port (numpy/scipy, single thread BLAS-free SpMM)
-    A = O.csr_matrix(rp, ci, v)
-    g1, g2 = O.gammas(degree, 10.4, -0.4)
-    t0 = time.perf_counter()
-    O.filter_block(A, start.T, degree, g1, g2)
-    return (time.perf_counter() - t0) / degree, 1, "port"
+class ReferenceSampler:
+    def __init__(self, P, incr, buf, rp, ci, v, degree):
+        from oracle import ref_io
+        self.ref_io = ref_io
+        self.P, self.incr, self.buf, self.degree = P, incr, buf, degree
+        self.s = incr + buf
+        self.threads = os.cpu_count() or 1
+        self.kind = "reference" if ref_io.ref_available() else "port"
+        g = reference_solve_fixture(round(P.n ** (1 / 3)))
+        self.lmin = g["min_eig_est"] if g else 0.4
+        self.lmax = g["max_eig_est"] if g else 16.0
+        self.dir = tempfile.mkdtemp()
+        self.path = os.path.join(self.dir, "c2.bin")
+        if self.kind == "reference":
+            ref_io.write_problem(self.path, rp, ci, v, P.start_block(self.s))
+        else:
+            from oracle import rc_oracle as O
+            self.A = O.csr_matrix(rp, ci, v)
+            self.X = P.start_block(self.s).T.copy()
+
+    def sample(self) -> dict:
+        """Seconds of one sample: filter per degree-step, orthogonalisation, Rayleigh-Ritz."""
+        if self.kind == "reference":
+            r = self.ref_io.run_ref("phases", self.path, degree=self.degree, bound=self.lmax, shift=-self.lmin,
+                                    rescheck=self.incr, threads=self.threads)
+            return {"filter_step": r["filter_seconds"] / self.degree, "ortho": r["ortho_seconds"],
+                    "rr": r["rr_seconds"], "threads": r["threads"]}
+        # oracle port: numpy/scipy, the same three phases
+        from oracle import rc_oracle as O
+        g1, g2 = O.gammas(self.degree, self.lmax, -self.lmin)
+        t0 = time.perf_counter()
+        V = O.filter_block(self.A, self.X, self.degree, g1, g2)
+        t1 = time.perf_counter()
+        V, _ = np.linalg.qr(V)
+        t2 = time.perf_counter()
+        W = self.A @ V
+        lam, Q = np.linalg.eigh(V.T @ W)
+        Y = V @ Q
+        np.linalg.norm(self.A @ Y[:, :self.incr] - Y[:, :self.incr] * lam[:self.incr], axis=0)
+        t3 = time.perf_counter()
+        return {"filter_step": (t1 - t0) / self.degree, "ortho": t2 - t1, "rr": t3 - t2, "threads": 1}
+
+    def estimate(self, samples: list, counts: dict) -> dict:
+        f = statistics.median([x["filter_step"] for x in samples])
+        o = statistics.median([x["ortho"] for x in samples])
+        r = statistics.median([x["rr"] for x in samples])
+        tts = f * counts["degree_steps"] + (o + r) * counts["inner_iterations"]
+        return {"tts_s": tts, "filter_step_s": f, "ortho_s": o, "rr_s": r,
+                "sample_s": statistics.median([x["filter_step"] * self.degree + x["ortho"] + x["rr"] for x in samples])}
+
+    def close(self):
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
+
+
+def describe_estimate(kind, threads, degree, s, est, counts, g):
+    meas = (f"; the reference's full solve of this workload, run to completion once on {g['reference_threads']} "
+            f"threads of the build machine, took {g['reference_seconds']:.0f} s") if g else ""
+    return (f"estimate: one inner iteration of the reference CPU solver ({kind}, {threads} threads) on the full "
+            f"{s}-column block per step ({degree} filter degree-steps {est['filter_step_s'] * 1e3:.0f} ms each, "
+            f"orthogonalisation {est['ortho_s'] * 1e3:.0f} ms, Rayleigh-Ritz {est['rr_s'] * 1e3:.0f} ms); "
+            f"time-to-solution = filter time per degree-step x {counts['degree_steps']} degree-steps + "
+            f"(orthogonalisation + Rayleigh-Ritz) x {counts['inner_iterations']} inner iterations, the counts of "
+            f"the reference's own solve (excludes its Lanczos bounds){meas}")
+
+
+def reference_counts_or_default(side):
+    counts = reference_counts(reference_solve_fixture(side))
+    # without the fixture (another grid side): this library's FP64 solve of configuration 2 took
+    # 116 inner iterations and 1659 degree-steps
+    return counts or {"inner_iterations": 116, "degree_steps": 1659}
 
 
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
     from rayleighchebyshevgpgpu_b200 import problems
     P = problems.config2(args.side)
     incr, buf = problems.block_sizes(P.k)
     rp, ci, v = P.csr()
-    per_step = []
-    kind, threads = "reference", os.cpu_count() or 1
+    sampler = ReferenceSampler(P, incr, buf, rp, ci, v, args.cpu_sample_degree)
+    samples, wall = [], []
     for i in range(args.warmup + args.steps):
-        t, threads, kind = cpu_reference_sample(P, incr, buf, args.cpu_sample_degree, rp, ci, v)
+        t0 = time.perf_counter()
+        x = sampler.sample()
         if i >= args.warmup:
-            per_step.append(t)
-    t_step = statistics.median(per_step)
-    tts = t_step * CONFIG2_FP64_DEGREE_STEPS
-    value = P.k / tts
+            samples.append(x)
+            wall.append(time.perf_counter() - t0)
+    sampler.close()
+    g = reference_solve_fixture(args.side)
+    counts = reference_counts_or_default(args.side)
+    est = sampler.estimate(samples, counts)
+    value = P.k / est["tts_s"]
+    threads = samples[-1]["threads"]
+    desc = describe_estimate(sampler.kind, threads, args.cpu_sample_degree, incr + buf, est, counts, g)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "eigenpairs/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": tts * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": config_dict(args, P.k, incr, buf, P.n, len(ci)),
-        "cpu_baseline": {"value": value, "unit": "eigenpairs/s", "cores": threads, "kind": kind,
-                         "sample": f"{args.cpu_sample_degree} degree-steps of the reference CPU filter "
-                                   f"(LanczosCpolyOperatorLM::apply) on the full {incr + buf}-column block, "
-                                   f"{t_step * 1e3:.1f} ms/step, x {CONFIG2_FP64_DEGREE_STEPS} degree-steps of a "
-                                   f"whole FP64 solve; a lower bound (excludes Lanczos, orthogonalisation, "
-                                   f"Rayleigh-Ritz)"},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.median(wall) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(args, P.k, incr, buf, P.n, len(ci), world),
+        "estimate": True,
+        "estimate_rule": "tts = filter_s_per_degree_step * reference_degree_steps + (ortho_s + rr_s) * "
+                         "reference_inner_iterations; a step is one timed sample (one inner iteration)",
+        "reference_tts_s": est["tts_s"],
+        "cpu_baseline": {"value": value, "unit": "eigenpairs/s", "cores": threads, "kind": sampler.kind,
+                         "sample": desc},
         "e2e": {"value": value, "unit": "eigenpairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -281,6 +377,27 @@ def run_ours(args):
         angle = float(np.arcsin(min(1.0, sin_max)))
         del D
     max_res_rel = float(np.max(res_mixed.residuals / np.maximum(np.abs(res_mixed.evals), 0.1)))
+    # residuals recomputed outside the library: torch's own sparse CSR product in FP64 on the returned
+    # eigenvectors (rows of the k x n blocks), relative to max(|lambda|, 0.1) as the stop test
+    with torch.no_grad():
+        A_t = torch.sparse_csr_tensor(torch.from_numpy(rp.astype(np.int64)), torch.from_numpy(ci.astype(np.int64)),
+                                      torch.from_numpy(v), size=(P.n, P.n), dtype=torch.float64, device="cuda")
+        indep = {}
+        for name, vecs, evals in (("mixed", mixed_vecs, res_mixed.evals), ("fp64", fp64_vecs, res64.evals)):
+            AX = torch.sparse.mm(A_t, vecs.T.contiguous())
+            lam_t = torch.from_numpy(evals).cuda()
+            rn = torch.linalg.vector_norm(AX - vecs.T * lam_t, dim=0).cpu().numpy()
+            indep[name] = float(np.max(rn / np.maximum(np.abs(evals), 0.1)))
+            del AX
+        del A_t
+    # parity with the reference's own CPU solve of this workload (tests/golden fixture)
+    gref = reference_solve_fixture(args.side)
+    parity = None
+    if gref:
+        ev_ref = np.asarray(gref["eigenvalues"])
+        parity = {"reference": "RayleighChebyshevLM CPU solve, same operator, start block, block sizes, stop test",
+                  "max_rel_eig_err_mixed": float(np.max(np.abs(res_mixed.evals - ev_ref) / np.abs(ev_ref))),
+                  "max_rel_eig_err_fp64": float(np.max(np.abs(res64.evals - ev_ref) / np.abs(ev_ref)))}
 
     # ---- end to end through the C ABI with host buffers (pinned), copies inside the timed region ----
     rp_h = torch.from_numpy(rp).pin_memory()
@@ -346,17 +463,19 @@ def run_ours(args):
         # block row (the residual block)
         corr_row = per_row.get("corr", per_row["fp32"] + s * ceb)
         traffic = P.n * (p32steps * per_row["fp32"] + csteps * corr_row + f64steps * per_row["fp64"]) / fsteps
-    # ---- CPU baseline (rank 0, N = 1) ----
+    # ---- CPU baseline (rank 0, N = 1): two samples of the reference's own CPU solver ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            t_step, threads, kind = cpu_reference_sample(P, incr, buf, args.cpu_sample_degree, rp, ci, v)
-            steps_solve = info64["degree_steps"] if info64 else CONFIG2_FP64_DEGREE_STEPS
-            tts_cpu = t_step * steps_solve
-            cpu = {"value": P.k / tts_cpu, "unit": "eigenpairs/s", "cores": threads, "kind": kind,
-                   "sample": f"{args.cpu_sample_degree} degree-steps of the reference CPU filter on the full "
-                             f"{s}-column block ({t_step * 1e3:.1f} ms/step) x {steps_solve} degree-steps of this "
-                             f"run's FP64 solve; lower bound (excludes Lanczos, orthogonalisation, Rayleigh-Ritz)"}
+            sampler = ReferenceSampler(P, incr, buf, rp, ci, v, args.cpu_sample_degree)
+            samples = [sampler.sample() for _ in range(2)]
+            sampler.close()
+            counts = reference_counts_or_default(args.side)
+            est = sampler.estimate(samples, counts)
+            cpu = {"value": P.k / est["tts_s"], "unit": "eigenpairs/s", "cores": samples[-1]["threads"],
+                   "kind": sampler.kind,
+                   "sample": describe_estimate(sampler.kind, samples[-1]["threads"], args.cpu_sample_degree, s, est,
+                                               counts, reference_solve_fixture(args.side))}
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "eigenpairs/s", "cores": None, "kind": "reference",
                    "sample": f"unavailable: {e}"}
@@ -365,15 +484,17 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": "eigenpairs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_mixed, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32 filter + f64", "data": "synthetic",
-        "config": dict(config_dict(args, P.k, incr, buf, P.n, nnz), parallelism=f"replicas x{world}"),
+        "vs_baseline": None, "dtype": DTYPE, "data": "synthetic",
+        "config": config_dict(args, P.k, incr, buf, P.n, nnz, world),
         "tts_ms": {"mixed_p50": statistics.median(times), "mixed_p99": float(np.percentile(times, 99)),
                    "fp64_p50": statistics.median(t64) if t64 else None,
                    "fp64_p99": float(np.percentile(t64, 99)) if t64 else None},
         "fp64_eigenpairs_per_s": replicas.job_rate(P.k, world, t_fp64 * 1e-3) if t_fp64 else None,
         "speedup_mixed_vs_fp64": (t_fp64 / t_mixed) if t_fp64 else None,
         "accuracy": {"max_rel_eig_diff_mixed_vs_fp64": eig_err, "max_subspace_angle_mixed_vs_fp64": angle,
-                     "max_rel_residual": max_res_rel, "found": int(res_mixed.info["found"])},
+                     "max_rel_residual": max_res_rel,
+                     "max_rel_residual_independent": indep,
+                     "vs_reference_solve": parity, "found": int(res_mixed.info["found"])},
         "solve_info": {"mixed": {k2: infos[-1][k2] for k2 in ("inner_iterations", "degree_steps", "fp64_degree_steps",
                                                                "correction_iterations", "correction_degree_steps",
                                                                "mixed_iterations", "lanczos_iterations",

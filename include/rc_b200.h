@@ -145,6 +145,39 @@ rc_status rc_spmm(rc_ctx* ctx, const rc_op* op, const void* X, int64_t ldx, void
 rc_status rc_filter(rc_ctx* ctx, const rc_op* op, void* X, int64_t ld, int64_t s, int64_t degree,
                     int64_t repetition, double gamma1, double gamma2, int precision);
 
+/* The filter above in correction form, the MIXED-precision refinement step of rc_solve (no
+ * reference counterpart; it computes LanczosCpolyOperatorLMCuda::apply, LanczosCpolyOperatorLMCuda.h:194-265,
+ * on Ritz pairs). V (n x s, DEVICE, FP64) holds Ritz vectors v_c with Ritz values lam[c] (HOST, s
+ * doubles). With a = gamma2*gamma1, b = gamma2, the scalar recurrence c_0 = 1, c_1 = a lam + b,
+ * c_k = (a lam + b) c_{k-1} - c_{k-2}, and the residual block R = A V - V diag(lam):
+ *   e_1 = R,  e_k = a*A*e_{k-1} + b*e_{k-1} - e_{k-2} + c_{k-1} R,
+ *   V <- (c_m V + a e_m)/(m+1)     (= x_m/(m+1) of rc_filter in exact arithmetic),
+ * with R and every e_k stored in bfloat16 and FP32 arithmetic; the last combination is FP64.
+ * Real CSR or 5/7/27-point stencil operators, 1 <= s <= 96, degree >= 1. Returns after the work
+ * is complete. */
+rc_status rc_filter_correction(rc_ctx* ctx, const rc_op* op, void* V, int64_t ld, int64_t s, const double* lam,
+                               int64_t degree, double gamma1, double gamma2);
+
+/* One correction-filter application of rc_filter_correction_batch. */
+typedef struct rc_correction_job {
+    size_t struct_size;            /* sizeof(rc_correction_job), or 0 */
+    const rc_op* op;
+    void* V;                       /* DEVICE n x s FP64 block, leading dimension ld; distinct per job */
+    int64_t ld;
+    int64_t s;
+    const double* lam;             /* HOST, s Ritz values */
+    int64_t degree;
+    double gamma1, gamma2;
+} rc_correction_job;
+
+/* Several rc_filter_correction applications (up to 64, each with its own operator, block, degree
+ * and coefficients) whose degree steps run as one batched launch per step: the request server's
+ * batched correction-filter kernels, with each block's arithmetic equal to rc_filter_correction's.
+ * Jobs those kernels do not take (27-point stencils, blocks with 64-bit element offsets) run
+ * through the single-block kernels in the same call. batched (optional out): the number of jobs
+ * that ran in the batched launches. No reference counterpart. */
+rc_status rc_filter_correction_batch(rc_ctx* ctx, int njobs, const rc_correction_job* jobs, int* batched);
+
 /* Spectral bounds by single-vector Lanczos with Sturm multisection of the tridiagonal
  * every 5 steps (LanczosMaxMinFinder.h:248-544, Dstebz_C.h:112). v0: optional start
  * vector (HOST, n scalars; NULL = internal uniform[-1,1] draw from `seed`).
@@ -172,14 +205,18 @@ rc_status rc_rayleigh_ritz(rc_ctx* ctx, const rc_op* op, void* V, void* W, int64
  * Replaces DSYEV/ZHPEVX (RayleighChebyshevLMCuda.h:614,618) and JacobiDiagonalizer. */
 rc_status rc_small_eigh(rc_ctx* ctx, int dtype, int64_t s, const void* H, double* evals, void* Q);
 
-/* rc_small_eigh for callers that must not allocate device memory (for example inside a CUDA
- * stream capture, under a fixed memory budget, or from a callback of another library): same
- * arguments and results, but the device staging and work memory come from one fixed array of
- * this library (about 1 MiB, held on every GPU that loads the library until the process exits),
- * and no cudaMalloc/cudaFree is called. s must be at most 128 (RC_ERR_INVALID otherwise). The
- * first call on a device looks up the array's device address, so make that first call before
- * any stream capture. All calls share the array: calls whose GPU work overlaps (several host
- * threads, or several contexts on one device) race on it and must be serialised by the caller.
+/* rc_small_eigh for callers that must not allocate device memory: code running under a fixed
+ * device-memory budget negotiated at start-up, where a cudaMalloc can fail or take memory another
+ * tenant of the GPU counts on, and callbacks invoked from another library's allocator or from an
+ * operator apply(), where allocating would re-enter that library. Same arguments and results, but
+ * the device staging and work memory come from one fixed array of this library (about 1 MiB, held
+ * on every GPU that loads the library until the process exits), and no cudaMalloc/cudaFree is
+ * called. s must be at most 128 (RC_ERR_INVALID otherwise). The first call on a device (and the
+ * first after its CUDA context is re-created) looks up the array's device address, which may load
+ * the library's module on the device: make that first call before any stream capture. All calls
+ * share the array: calls whose GPU work overlaps (several host threads, or several contexts on one
+ * device) race on it and must be serialised by the caller. The call copies H in and the results
+ * out through host memory and returns when they are on the host.
  * This entry point has no counterpart in the reference. */
 rc_status rc_small_eigh_noalloc(rc_ctx* ctx, int dtype, int64_t s, const void* H, double* evals, void* Q);
 

@@ -14,14 +14,21 @@ import numpy as np
 
 ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
 REF_BIN = os.path.join(ORACLE_DIR, "_ref", "ref_harness")
+# Where the reference sources lie: RC_REFERENCE_DIR, else the mount point of this build machine.
+REFERENCE_DIR = os.environ.get("RC_REFERENCE_DIR", "/root/reference")
 
 
 def ref_available() -> bool:
     return os.path.exists(REF_BIN) and os.access(REF_BIN, os.X_OK)
 
 
-def build_ref(reference_dir: str = "/root/reference") -> bool:
+def reference_present(reference_dir: str | None = None) -> bool:
+    return os.path.isdir(reference_dir or REFERENCE_DIR)
+
+
+def build_ref(reference_dir: str | None = None) -> bool:
     """Compile the reference harness from the reference sources (when they are present)."""
+    reference_dir = reference_dir or REFERENCE_DIR
     if not os.path.isdir(reference_dir):
         return ref_available()
     r = subprocess.run(["make", "-C", ORACLE_DIR, f"REF={reference_dir}"], capture_output=True, text=True)

@@ -113,6 +113,20 @@ class ServerParams(C.Structure):
     ]
 
 
+class CorrectionJob(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_size_t),
+        ("op", c_vp),
+        ("V", c_vp),
+        ("ld", c_i64),
+        ("s", c_i64),
+        ("lam", c_vp),
+        ("degree", c_i64),
+        ("gamma1", C.c_double),
+        ("gamma2", C.c_double),
+    ]
+
+
 RC_REQ_QUEUED, RC_REQ_RUNNING, RC_REQ_DONE, RC_REQ_FAILED, RC_REQ_CANCELLED = 0, 1, 2, 3, 4
 REQ_STATE_NAMES = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
 
@@ -166,6 +180,8 @@ SIGNATURES = {
     "rc_cpoly_pm": (C.c_double, [c_i64, C.c_double]),
     "rc_spmm": (C.c_int, [c_vp, c_vp, c_vp, c_i64, c_vp, c_i64, c_i64, c_dp, c_dp]),
     "rc_filter": (C.c_int, [c_vp, c_vp, c_vp, c_i64, c_i64, c_i64, c_i64, C.c_double, C.c_double, C.c_int]),
+    "rc_filter_correction": (C.c_int, [c_vp, c_vp, c_vp, c_i64, c_i64, c_dp, c_i64, C.c_double, C.c_double]),
+    "rc_filter_correction_batch": (C.c_int, [c_vp, C.c_int, C.POINTER(CorrectionJob), C.POINTER(C.c_int)]),
     "rc_lanczos_bounds": (C.c_int, [c_vp, c_vp, c_vp, C.c_uint64, C.c_double, C.c_int, c_i64, c_dp, c_dp,
                                     C.POINTER(c_i64)]),
     "rc_cholqr": (C.c_int, [c_vp, C.c_int, c_vp, c_i64, c_i64, c_i64, C.POINTER(C.c_int)]),

@@ -22,7 +22,7 @@ NVCC_FLAGS = ARCH_FLAGS + [
     "--expt-relaxed-constexpr", "-Xptxas", "-O3",
 ]
 SOURCES = ["rc_filter.cu", "rc_filter_rm.cu", "rc_dense.cu", "rc_gemm.cu", "rc_noalloc.cu", "rc_lanczos.cu", "rc_solver.cu", "rc_capi.cu",
-           "rc_batch.cu", "rc_serve.cu", "rc_resid.cu"]
+           "rc_batch.cu", "rc_serve.cu", "rc_resid.cu", "rc_corrapi.cu"]
 
 
 def _nvcc() -> str:

@@ -279,12 +279,10 @@ rc_status rm_filter_corr(rc_ctx* ctx, rc_op* op, double* V, int64_t ldv, int64_t
     RC_TRY(ensure_fp32(ctx, op));
     const int64_t ld = rm_leading_dim(RC_REAL64, P32, s);
     void* tab = nullptr;
-    RC_TRY(rc_slot(ctx, S_CORR, (size_t)(degree + 1) * ld * sizeof(float) + (size_t)ld * sizeof(double) + 256, &tab));
+    RC_TRY(rc_slot(ctx, S_CORR, corr_table_bytes(degree, ld), &tab));
     float* sig = (float*)tab;
-    double* coef = (double*)((char*)tab + (((size_t)(degree + 1) * ld * sizeof(float) + 255) / 256) * 256);
-    corr_coef_kernel<<<1, 128, 0, ctx->stream>>>(s, ld, degree, a, b, lam_dev, sig, coef);
-    ctx->launches++;
-    RC_CU(ctx, cudaGetLastError());
+    double* coef = (double*)((char*)tab + corr_table_coef_offset(degree, ld));
+    RC_TRY(corr_coefficients(ctx, s, ld, degree, a, b, lam_dev, sig, coef));
     if (ctx->serve) {  // under the request server: one job of a batched launch
         bool handled = false;
         RC_TRY(serve_filter_corr(ctx, op, V, ldv, s, degree, a, b, R, sig, coef, bufA, bufB, &handled));
@@ -309,6 +307,24 @@ rc_status rm_filter_corr(rc_ctx* ctx, rc_op* op, double* V, int64_t ldv, int64_t
     }
     StencilRows<float, float, 5> pol{op->nx, op->ny, op->nz, op->diag32, op->offdiag, theta};
     return rm_corr_select(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band);
+}
+
+rc_status corr_coefficients(rc_ctx* ctx, int64_t s, int64_t ld, int64_t degree, double a, double b,
+                            const double* lam_dev, float* sig, double* coef) {
+    corr_coef_kernel<<<1, 128, 0, ctx->stream>>>(s, ld, degree, a, b, lam_dev, sig, coef);
+    ctx->launches++;
+    RC_CU(ctx, cudaGetLastError());
+    return RC_OK;
+}
+
+rc_status to_row_major_f64(rc_ctx* ctx, int64_t n, int64_t s, const double* V, int64_t ldv, double* Yrm,
+                           int64_t ld) {
+    if ((s + 31) / 32 > 65535) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "row-major copy: too many columns");
+    const dim3 tgrid((unsigned)((n + 31) / 32), (unsigned)((s + 31) / 32)), tblk(32, 8);
+    to_rm_kernel<double, double><<<tgrid, tblk, 0, ctx->stream>>>(n, s, V, ldv, Yrm, ld);
+    ctx->launches++;
+    RC_CU(ctx, cudaGetLastError());
+    return RC_OK;
 }
 
 // Row length padded to 32 bytes (two 16-byte slices); the padding columns are never read back.

@@ -79,7 +79,7 @@ struct rc_ctx {
 
 enum Slot {
     S_V = 0, S_W, S_T1, S_T2, S_FOUND, S_PART, S_SMALL, S_LANCZOS, S_RPART, S_IO, S_CB, S_EIG, S_FA, S_FB,
-    S_R32, S_CORR, S_YRM, S_COUNT
+    S_R32, S_CORR, S_YRM, S_BATCH, S_COUNT
 };
 
 struct rc_op {
@@ -186,6 +186,21 @@ bool rm_corr_supported(const rc_op* op, int64_t s);
 rc_status rm_filter_corr(rc_ctx* ctx, rc_op* op, double* V, int64_t ldv, int64_t s, int64_t degree, double a,
                          double b, const double* lam_dev, const rc_corr_t* R, void* bufA, void* bufB);
 int64_t rm_leading_dim(int dtype, int prec, int64_t s);
+// Tables of a correction-filter application of degree m over rows of leading dimension ld: the
+// source coefficients sig[k*ld + c] = c_{k-1}(lam_c) (FP32, k = 2..m) and the weights
+// coef[c] = c_m(lam_c)/(m+1) (FP64) of the Ritz vectors in the result, written by
+// corr_coefficients from the device Ritz values lam_dev (one launch on ctx->stream).
+inline size_t corr_table_coef_offset(int64_t degree, int64_t ld) {
+    return (((size_t)(degree + 1) * ld * sizeof(float) + 255) / 256) * 256;
+}
+inline size_t corr_table_bytes(int64_t degree, int64_t ld) {
+    return corr_table_coef_offset(degree, ld) + (size_t)ld * sizeof(double) + 256;
+}
+rc_status corr_coefficients(rc_ctx* ctx, int64_t s, int64_t ld, int64_t degree, double a, double b,
+                            const double* lam_dev, float* sig, double* coef);
+// Row-major FP64 copy Yrm (leading dimension ld) of the column-major n x s block V.
+rc_status to_row_major_f64(rc_ctx* ctx, int64_t n, int64_t s, const double* V, int64_t ldv, double* Yrm,
+                           int64_t ld);
 // Build the FP32 (c64) copy of an operator's values/diagonal used by the MIXED filter.
 rc_status ensure_fp32(rc_ctx* ctx, rc_op* op);
 // Degree-step timing (ctx->step_timing): record an event on the context stream; step_flush

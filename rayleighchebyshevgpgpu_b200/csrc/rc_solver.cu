@@ -621,10 +621,10 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
                 maxGap = std::max(maxGap, std::fabs(VtAVeigValue_[i] - VtAVeigValue_[i - 1]) / spectralRange);
 
             if (P_.verbose)
-                printf("%-5ld : Degree %-3ld  Residual Max: %-10.5g  Eig Diff Max: %-10.5g  Eig Conv Factor: %-10.5g "
-                       "Max Gap %-10.5g %s\n",
+                printf("[rc] iter %ld  degree %ld  max rel residual %.4e  max eig change %.4e  change ratio %.3f  "
+                       "max gap %.4e %s\n",
                        (long)innerLoopCount, (long)starDegree, maxResidual, maxEigDiff, eigDiffRatio, maxGap,
-                       phase == PH_PLAIN32 ? "[fp32 filter]" : (phase == PH_CORR32 ? "[fp32 correction]" : ""));
+                       phase == PH_PLAIN32 ? "[fp32 filter]" : (phase == PH_CORR32 ? "[bf16 correction]" : ""));
 
             // ---- stop test (:1520-1545)
             if (stopCondition == RC_STOP_RESIDUAL_ONLY) {
@@ -708,7 +708,7 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
             }
             foundSize_ += foundCount;
             if (P_.verbose)
-                printf("\nFound Count: %3ld Largest Eig Found: %-20.15g Lambda Bound: %-20.15g \n", (long)foundSize_,
+                printf("[rc] found %ld eigenpairs, largest %.15e (bound %.15e)\n", (long)foundSize_,
                        eigValues_[foundSize_ - 1], lambdaMax);
         }
         haveR_ = false;

@@ -431,6 +431,32 @@ def filter_block(ctx: Context, op: Operator, X, s: int, degree: int, gamma1: flo
                           _PREC[precision]), ctx.h, "rc_filter")
 
 
+def filter_correction(ctx: Context, op: Operator, V, s: int, lam, degree: int, gamma1: float, gamma2: float,
+                      ld=None):
+    """V <- P_m(A')V in correction form on Ritz pairs (V, lam): rc_filter_correction."""
+    lam = np.ascontiguousarray(lam, dtype=np.float64)
+    check(lib().rc_filter_correction(ctx.h, op.h, C.c_void_p(_ptr(V)), ld or op.n, s,
+                                     lam.ctypes.data_as(capi.c_dp), degree, gamma1, gamma2),
+          ctx.h, "rc_filter_correction")
+
+
+def filter_correction_batch(ctx: Context, jobs) -> int:
+    """Several correction-filter applications in one batched launch per degree step
+    (rc_filter_correction_batch). jobs: (op, V, s, lam, degree, gamma1, gamma2) tuples.
+    Returns the number of jobs that ran in the batched launches."""
+    arr = (capi.CorrectionJob * len(jobs))()
+    keep = []
+    for j, (op, V, s, lam, degree, g1, g2) in enumerate(jobs):
+        lam = np.ascontiguousarray(lam, dtype=np.float64)
+        keep.append(lam)
+        arr[j] = capi.CorrectionJob(C.sizeof(capi.CorrectionJob), op.h, _ptr(V), op.n, s, int(lam.ctypes.data),
+                                    degree, g1, g2)
+    batched = C.c_int()
+    check(lib().rc_filter_correction_batch(ctx.h, len(jobs), arr, C.byref(batched)), ctx.h,
+          "rc_filter_correction_batch")
+    return batched.value
+
+
 def lanczos_bounds(ctx: Context, op: Operator, v0=None, seed: int = 1, tol: float = 1e-6, which: str = "max",
                    max_iter: int = 10000):
     lmin, lmax, it = C.c_double(), C.c_double(), C.c_int64()

@@ -76,6 +76,24 @@ def test_server_struct_layouts_match_header(built_lib):
     assert out[4] == _capi.RequestInfo.device_bytes.offset
 
 
+def test_correction_job_layout_matches_header(built_lib):
+    import subprocess
+    import tempfile
+    src = ('#include "rc_b200.h"\n#include <stdio.h>\n#include <stddef.h>\nint main(){printf("%zu %zu %zu",'
+           'sizeof(rc_correction_job), offsetof(rc_correction_job, lam), offsetof(rc_correction_job, gamma2));'
+           'return 0;}\n')
+    d = tempfile.mkdtemp()
+    with open(os.path.join(d, "t.c"), "w") as f:
+        f.write(src)
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), os.path.join(d, "t.c"), "-o",
+                           os.path.join(d, "t")])
+    out = [int(x) for x in subprocess.check_output([os.path.join(d, "t")]).decode().split()]
+    from rayleighchebyshevgpgpu_b200 import _capi
+    assert out[0] == ctypes.sizeof(_capi.CorrectionJob)
+    assert out[1] == _capi.CorrectionJob.lam.offset
+    assert out[2] == _capi.CorrectionJob.gamma2.offset
+
+
 def test_server_calls_without_a_server_return_status(built_lib):
     from rayleighchebyshevgpgpu_b200 import _capi
     L = _capi.lib()

@@ -1,8 +1,9 @@
 """rc_small_eigh_noalloc: the small Hermitian eigensolver for callers that cannot allocate device
-memory (inside a stream capture, under a fixed memory budget, or from another library's
-callback). Its device staging and work memory is one fixed array of the library instead of the
-context's allocator. Checked through the C ABI against rc_small_eigh, the allocating entry point,
-on two calls in a row (the second reuses the array the first one left behind).
+memory (code under a fixed device-memory budget, or a callback of another library's allocator or
+operator apply(), where allocating would re-enter that library). Its device staging and work memory
+is one fixed array of the library instead of the context's allocator. Checked through the C ABI
+against rc_small_eigh, the allocating entry point, on two calls in a row (the second reuses the
+array the first one left behind).
 
 This file sorts last so that a run stopping at the first failure has already run every other test.
 """
