@@ -152,14 +152,18 @@ def config_dict(args, k, incr, buf, n, nnz, world=1):
 
 # ---------------------------------------------------------------------------------------------
 # CPU baseline: the reference's own CPU solver (RayleighChebyshevLM, built from its sources into
-# oracle/_ref) on the full benchmark block, all host threads. One sample = one inner iteration of
-# its solve, phase by phase: `degree` filter degree-steps (LanczosCpolyOperatorLM::apply), one
-# modified Gram-Schmidt orthogonalisation, and one Rayleigh-Ritz step (formVtAV, Jacobi,
-# createEigenVectorsAndResiduals). The time-to-solution estimate is
+# oracle/_ref) on the full benchmark block, all host threads. One inner iteration of its solve has
+# three phases: the filter (LanczosCpolyOperatorLM::apply, timed per degree-step), one modified
+# Gram-Schmidt orthogonalisation, and one Rayleigh-Ritz step (formVtAV, Jacobi,
+# createEigenVectorsAndResiduals). A sample times one phase; the phases rotate over the samples.
+# The time-to-solution estimate is
 #   filter seconds per degree-step x the reference solve's degree-steps
 #   + (orthogonalisation + Rayleigh-Ritz seconds) x its inner iterations,
 # with both counts from the reference's own full solve of this workload (tests/golden).
 # ---------------------------------------------------------------------------------------------
+PHASES = ("filter", "ortho", "rr")
+
+
 class ReferenceSampler:
     def __init__(self, P, incr, buf, rp, ci, v, degree):
         from oracle import ref_io
@@ -180,35 +184,35 @@ class ReferenceSampler:
             self.A = O.csr_matrix(rp, ci, v)
             self.X = P.start_block(self.s).T.copy()
 
-    def sample(self) -> dict:
-        """Seconds of one sample: filter per degree-step, orthogonalisation, Rayleigh-Ritz."""
+    def sample(self, phase: str) -> dict:
+        """Seconds of one phase of one inner iteration ("filter": per degree-step)."""
         if self.kind == "reference":
             r = self.ref_io.run_ref("phases", self.path, degree=self.degree, bound=self.lmax, shift=-self.lmin,
-                                    rescheck=self.incr, threads=self.threads)
-            return {"filter_step": r["filter_seconds"] / self.degree, "ortho": r["ortho_seconds"],
-                    "rr": r["rr_seconds"], "threads": r["threads"]}
+                                    rescheck=self.incr, threads=self.threads, do=phase)
+            sec = {"filter": r["filter_seconds"] / self.degree, "ortho": r["ortho_seconds"],
+                   "rr": r["rr_seconds"]}[phase]
+            return {"phase": phase, "seconds": sec, "wall": sec * (self.degree if phase == "filter" else 1),
+                    "threads": r["threads"]}
         # oracle port: numpy/scipy, the same three phases
         from oracle import rc_oracle as O
-        g1, g2 = O.gammas(self.degree, self.lmax, -self.lmin)
         t0 = time.perf_counter()
-        V = O.filter_block(self.A, self.X, self.degree, g1, g2)
-        t1 = time.perf_counter()
-        V, _ = np.linalg.qr(V)
-        t2 = time.perf_counter()
-        W = self.A @ V
-        lam, Q = np.linalg.eigh(V.T @ W)
-        Y = V @ Q
-        np.linalg.norm(self.A @ Y[:, :self.incr] - Y[:, :self.incr] * lam[:self.incr], axis=0)
-        t3 = time.perf_counter()
-        return {"filter_step": (t1 - t0) / self.degree, "ortho": t2 - t1, "rr": t3 - t2, "threads": 1}
+        if phase == "filter":
+            g1, g2 = O.gammas(self.degree, self.lmax, -self.lmin)
+            O.filter_block(self.A, self.X, self.degree, g1, g2)
+        elif phase == "ortho":
+            np.linalg.qr(self.X)
+        else:
+            W = self.A @ self.X
+            lam, Q = np.linalg.eigh(self.X.T @ W)
+            Y = self.X @ Q
+            np.linalg.norm(self.A @ Y[:, :self.incr] - Y[:, :self.incr] * lam[:self.incr], axis=0)
+        t = time.perf_counter() - t0
+        return {"phase": phase, "seconds": t / (self.degree if phase == "filter" else 1), "wall": t, "threads": 1}
 
     def estimate(self, samples: list, counts: dict) -> dict:
-        f = statistics.median([x["filter_step"] for x in samples])
-        o = statistics.median([x["ortho"] for x in samples])
-        r = statistics.median([x["rr"] for x in samples])
-        tts = f * counts["degree_steps"] + (o + r) * counts["inner_iterations"]
-        return {"tts_s": tts, "filter_step_s": f, "ortho_s": o, "rr_s": r,
-                "sample_s": statistics.median([x["filter_step"] * self.degree + x["ortho"] + x["rr"] for x in samples])}
+        med = {ph: statistics.median([x["seconds"] for x in samples if x["phase"] == ph]) for ph in PHASES}
+        tts = med["filter"] * counts["degree_steps"] + (med["ortho"] + med["rr"]) * counts["inner_iterations"]
+        return {"tts_s": tts, "filter_step_s": med["filter"], "ortho_s": med["ortho"], "rr_s": med["rr"]}
 
     def close(self):
         try:
@@ -220,9 +224,10 @@ class ReferenceSampler:
 def describe_estimate(kind, threads, degree, s, est, counts, g):
     meas = (f"; the reference's full solve of this workload, run to completion once on {g['reference_threads']} "
             f"threads of the build machine, took {g['reference_seconds']:.0f} s") if g else ""
-    return (f"estimate: one inner iteration of the reference CPU solver ({kind}, {threads} threads) on the full "
-            f"{s}-column block per step ({degree} filter degree-steps {est['filter_step_s'] * 1e3:.0f} ms each, "
-            f"orthogonalisation {est['ortho_s'] * 1e3:.0f} ms, Rayleigh-Ritz {est['rr_s'] * 1e3:.0f} ms); "
+    return (f"estimate: the phases of one inner iteration of the reference CPU solver ({kind}, {threads} threads) "
+            f"on the full {s}-column block, one phase per sample in rotation ({degree} filter degree-steps, "
+            f"{est['filter_step_s'] * 1e3:.0f} ms each; orthogonalisation {est['ortho_s'] * 1e3:.0f} ms; "
+            f"Rayleigh-Ritz {est['rr_s'] * 1e3:.0f} ms); "
             f"time-to-solution = filter time per degree-step x {counts['degree_steps']} degree-steps + "
             f"(orthogonalisation + Rayleigh-Ritz) x {counts['inner_iterations']} inner iterations, the counts of "
             f"the reference's own solve (excludes its Lanczos bounds){meas}")
@@ -246,12 +251,13 @@ def run_reference_arm(args):
     rp, ci, v = P.csr()
     sampler = ReferenceSampler(P, incr, buf, rp, ci, v, args.cpu_sample_degree)
     samples, wall = [], []
-    for i in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        x = sampler.sample()
+    # warm-up samples rotate from the filter; timed samples cover every phase at least once
+    for i in range(args.warmup + max(args.steps, len(PHASES))):
+        ph = PHASES[(i - args.warmup) % len(PHASES)] if i >= args.warmup else PHASES[i % len(PHASES)]
+        x = sampler.sample(ph)
         if i >= args.warmup:
             samples.append(x)
-            wall.append(time.perf_counter() - t0)
+            wall.append(x["wall"])
     sampler.close()
     g = reference_solve_fixture(args.side)
     counts = reference_counts_or_default(args.side)
@@ -261,12 +267,13 @@ def run_reference_arm(args):
     desc = describe_estimate(sampler.kind, threads, args.cpu_sample_degree, incr + buf, est, counts, g)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "eigenpairs/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.median(wall) * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.fmean(wall) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": config_dict(args, P.k, incr, buf, P.n, len(ci), world),
         "estimate": True,
         "estimate_rule": "tts = filter_s_per_degree_step * reference_degree_steps + (ortho_s + rr_s) * "
-                         "reference_inner_iterations; a step is one timed sample (one inner iteration)",
+                         "reference_inner_iterations (medians over the samples); a step is one timed sample of "
+                         "one phase of an inner iteration, phases in rotation",
         "reference_tts_s": est["tts_s"],
         "cpu_baseline": {"value": value, "unit": "eigenpairs/s", "cores": threads, "kind": sampler.kind,
                          "sample": desc},
@@ -468,7 +475,7 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             sampler = ReferenceSampler(P, incr, buf, rp, ci, v, args.cpu_sample_degree)
-            samples = [sampler.sample() for _ in range(2)]
+            samples = [sampler.sample(ph) for ph in PHASES]
             sampler.close()
             counts = reference_counts_or_default(args.side)
             est = sampler.estimate(samples, counts)

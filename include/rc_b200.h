@@ -145,6 +145,25 @@ rc_status rc_spmm(rc_ctx* ctx, const rc_op* op, const void* X, int64_t ldx, void
 rc_status rc_filter(rc_ctx* ctx, const rc_op* op, void* X, int64_t ld, int64_t s, int64_t degree,
                     int64_t repetition, double gamma1, double gamma2, int precision);
 
+/* Leading dimension of the filter's row-major blocks for s columns: s rounded up to 32 bytes of
+ * elements of dtype in the storage precision (double/c128 for RC_PREC_FP64, float/c64 for
+ * RC_PREC_MIXED). 0 for bad arguments. */
+int64_t rc_rm_leading_dim(int dtype, int precision, int64_t s);
+
+/* One degree step of the filter on ROW-MAJOR device blocks (row i holds its s columns
+ * contiguously; leading dimension ld >= s, a multiple of 32 bytes of elements):
+ *   y = alpha*A*x + beta*x + gamma*z
+ * the step of LanczosCpolyOperatorLMCuda::apply (LanczosCpolyOperatorLMCuda.h:241-257: the user
+ * SpMM out = alpha*A*in + beta*out, then the substract kernel) fused into one pass. Storage and
+ * arithmetic: double/c128 (RC_PREC_FP64) or float/c64 (RC_PREC_MIXED). z may be NULL (no gamma
+ * term); y may alias z but not x. alpha, beta, gamma: (re, im) pairs. CSR and stencil operators.
+ * The kernels are the filter's own, so each row is computed exactly as rc_filter computes it:
+ * a row-sharded filter runs this step on each rank's extended block (own rows plus the halo rows
+ * its rows couple to, filled by an exchange between steps) and matches the unsharded filter bit
+ * for bit. No reference counterpart as a separate call. */
+rc_status rc_filter_step_rm(rc_ctx* ctx, const rc_op* op, const void* x, const void* z, void* y, int64_t ld,
+                            int64_t s, const double* alpha, const double* beta, const double* gamma, int precision);
+
 /* The filter above in correction form, the MIXED-precision refinement step of rc_solve (no
  * reference counterpart; it computes LanczosCpolyOperatorLMCuda::apply, LanczosCpolyOperatorLMCuda.h:194-265,
  * on Ritz pairs). V (n x s, DEVICE, FP64) holds Ritz vectors v_c with Ritz values lam[c] (HOST, s

@@ -9,10 +9,11 @@
 //   ref_harness solve   <problem.bin> k=16 tol=1e-10 incr=16 buffer=8 stop=RESIDUAL_ONLY [threads=N]
 //   ref_harness filter  <problem.bin> degree=m bound=B shift=S reps=1 out=<file> [threads=N]
 //   ref_harness lanczos <problem.bin> tol=1e-6 which=max|both
-//   ref_harness phases  <problem.bin> degree=m bound=B shift=S rescheck=k [threads=N]
+//   ref_harness phases  <problem.bin> degree=m bound=B shift=S rescheck=k [do=filter,ortho,rr] [threads=N]
 //       one inner iteration of RayleighChebyshevLM on the start block, phase by phase: the filter
 //       (LanczosCpolyOperatorLM::apply, degree m), then orthogonalize (modified Gram-Schmidt),
-//       formVtAV + computeVtVeigensystem (Jacobi) + createEigenVectorsAndResiduals, each timed
+//       formVtAV + computeVtVeigensystem (Jacobi) + createEigenVectorsAndResiduals, each timed;
+//       `do` selects the phases that run (default all)
 //   ref_harness cpoly   mmax=200 [shift=S bound=B star=L degmax=D]
 //
 // problem.bin (little endian): "RCPB", int32 version=1, int64 n, nnz, s_start, has_lz0,
@@ -123,7 +124,8 @@ public:
 // run on the caller's block with the member set-up getMinEigenSystem does (:917-998).
 class RCPhaseProbe : public RayleighChebyshevLM<HVec, HCsrOp, HRand, double> {
 public:
-    void run(std::vector<HVec>& V, HCsrOp& op, long resCheck, double& t_ortho, double& t_rr) {
+    void run(std::vector<HVec>& V, HCsrOp& op, long resCheck, bool do_ortho, bool do_rr, double& t_ortho,
+             double& t_rr) {
         const long s = (long)V.size();
         OpPtr = &op;
         vArray = V;
@@ -136,12 +138,14 @@ public:
         VtAVeigVector.initialize(s, s);
         VtAVeigValue.assign(s, 0.0);
         const auto t0 = std::chrono::steady_clock::now();
-        orthogonalize(vArray);
+        if (do_ortho) orthogonalize(vArray);
         const auto t1 = std::chrono::steady_clock::now();
-        formVtAV(vArray, VtAV);
-        computeVtVeigensystem(VtAV, VtAVeigValue, VtAVeigVector);
-        std::vector<double> res;
-        createEigenVectorsAndResiduals(VtAVeigVector, vArray, resCheck, res);
+        if (do_rr) {
+            formVtAV(vArray, VtAV);
+            computeVtVeigensystem(VtAV, VtAVeigValue, VtAVeigVector);
+            std::vector<double> res;
+            createEigenVectorsAndResiduals(VtAVeigVector, vArray, resCheck, res);
+        }
         const auto t2 = std::chrono::steady_clock::now();
         t_ortho = std::chrono::duration<double>(t1 - t0).count();
         t_rr = std::chrono::duration<double>(t2 - t1).count();
@@ -315,15 +319,21 @@ int main(int argc, char** argv) {
         const long resCheck = getl(kv, "rescheck", P.s_start);
         std::vector<HVec> V(P.s_start);
         for (long c = 0; c < P.s_start; ++c) V[c].d.assign(P.start.begin() + c * P.n, P.start.begin() + (c + 1) * P.n);
+        const std::string what = kv.count("do") ? kv["do"] : std::string("filter,ortho,rr");
+        const bool do_filter = what.find("filter") != std::string::npos;
+        const bool do_ortho = what.find("ortho") != std::string::npos;
+        const bool do_rr = what.find("rr") != std::string::npos;
         LanczosCpolyOperatorLM<HVec, HCsrOp> cOp;
         cOp.initialize(op);
         cOp.setLanczosCpolyParameters(degree, 1, bound, shift);
         const auto t0 = std::chrono::steady_clock::now();
-        cOp.apply(V);
+        if (do_filter) cOp.apply(V);
         const auto t1 = std::chrono::steady_clock::now();
         double t_ortho = 0.0, t_rr = 0.0;
-        RCPhaseProbe probe;
-        probe.run(V, op, resCheck, t_ortho, t_rr);
+        if (do_ortho || do_rr) {
+            RCPhaseProbe probe;
+            probe.run(V, op, resCheck, do_ortho, do_rr, t_ortho, t_rr);
+        }
         std::printf("{\"filter_seconds\": %.9g, \"degree\": %ld, \"ortho_seconds\": %.9g, \"rr_seconds\": %.9g, "
                     "\"threads\": %d}\n",
                     std::chrono::duration<double>(t1 - t0).count(), degree, t_ortho, t_rr, threads);

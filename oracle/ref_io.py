@@ -26,15 +26,26 @@ def reference_present(reference_dir: str | None = None) -> bool:
     return os.path.isdir(reference_dir or REFERENCE_DIR)
 
 
-def build_ref(reference_dir: str | None = None) -> bool:
-    """Compile the reference harness from the reference sources (when they are present)."""
+def build_ref(reference_dir: str | None = None, targets=("_ref/ref_harness",)) -> bool:
+    """Compile the reference harness (and any other oracle/Makefile targets) from the reference
+    sources, when they are present."""
     reference_dir = reference_dir or REFERENCE_DIR
     if not os.path.isdir(reference_dir):
         return ref_available()
-    r = subprocess.run(["make", "-C", ORACLE_DIR, f"REF={reference_dir}"], capture_output=True, text=True)
+    r = subprocess.run(["make", "-C", ORACLE_DIR, f"REF={reference_dir}", *targets], capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"oracle/_ref build failed:\n{r.stdout}\n{r.stderr}")
     return ref_available()
+
+
+CONTAINERS_BIN = os.path.join(ORACLE_DIR, "_ref", "lmcuda_reference_containers")
+
+
+def build_containers_driver(reference_dir: str | None = None) -> bool:
+    """The drop-in driver over the reference's own containers (needs the built library)."""
+    if reference_present(reference_dir):
+        build_ref(reference_dir, targets=("_ref/lmcuda_reference_containers",))
+    return os.path.exists(CONTAINERS_BIN)
 
 
 def write_problem(path: str, rowptr, colind, vals, start=None, lz0=None) -> None:

@@ -180,6 +180,8 @@ SIGNATURES = {
     "rc_cpoly_pm": (C.c_double, [c_i64, C.c_double]),
     "rc_spmm": (C.c_int, [c_vp, c_vp, c_vp, c_i64, c_vp, c_i64, c_i64, c_dp, c_dp]),
     "rc_filter": (C.c_int, [c_vp, c_vp, c_vp, c_i64, c_i64, c_i64, c_i64, C.c_double, C.c_double, C.c_int]),
+    "rc_rm_leading_dim": (c_i64, [C.c_int, C.c_int, c_i64]),
+    "rc_filter_step_rm": (C.c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_i64, c_i64, c_dp, c_dp, c_dp, C.c_int]),
     "rc_filter_correction": (C.c_int, [c_vp, c_vp, c_vp, c_i64, c_i64, c_dp, c_i64, C.c_double, C.c_double]),
     "rc_filter_correction_batch": (C.c_int, [c_vp, C.c_int, C.POINTER(CorrectionJob), C.POINTER(C.c_int)]),
     "rc_lanczos_bounds": (C.c_int, [c_vp, c_vp, c_vp, C.c_uint64, C.c_double, C.c_int, c_i64, c_dp, c_dp,

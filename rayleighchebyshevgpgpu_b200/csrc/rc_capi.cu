@@ -407,6 +407,28 @@ rc_status rc_filter(rc_ctx* ctx, const rc_op* op_c, void* X, int64_t ld, int64_t
                              (size_t)op->n * (s > 0 ? s : 1) * elem_bytes(op->dtype, P64), &steps);
 }
 
+int64_t rc_rm_leading_dim(int dtype, int precision, int64_t s) {
+    if ((dtype != RC_REAL64 && dtype != RC_COMPLEX128) || (precision != RC_PREC_FP64 && precision != RC_PREC_MIXED) ||
+        s < 1)
+        return 0;
+    return rcb::rm_leading_dim(dtype, precision == RC_PREC_MIXED ? P32 : P64, s);
+}
+
+rc_status rc_filter_step_rm(rc_ctx* ctx, const rc_op* op_c, const void* x, const void* z, void* y, int64_t ld,
+                            int64_t s, const double* alpha, const double* beta, const double* gamma, int precision) {
+    RC_CHECK_CTX(ctx);
+    rc_op* op = const_cast<rc_op*>(op_c);
+    if (!op || !x || !y || s < 1 || !alpha || !beta || (z && !gamma))
+        return rc_fail(ctx, RC_ERR_INVALID, "rc_filter_step_rm: bad arguments");
+    if (x == y) return rc_fail(ctx, RC_ERR_INVALID, "rc_filter_step_rm: y must not alias x");
+    if (precision != RC_PREC_FP64 && precision != RC_PREC_MIXED)
+        return rc_fail(ctx, RC_ERR_INVALID, "rc_filter_step_rm: bad precision");
+    double a[2] = {alpha[0], op->dtype == RC_COMPLEX128 ? alpha[1] : 0.0};
+    double b[2] = {beta[0], op->dtype == RC_COMPLEX128 ? beta[1] : 0.0};
+    double g[2] = {z ? gamma[0] : 0.0, z && op->dtype == RC_COMPLEX128 ? gamma[1] : 0.0};
+    return rcb::rm_step(ctx, op, x, z, y, ld, s, a, b, g, precision);
+}
+
 rc_status rc_lanczos_bounds(rc_ctx* ctx, const rc_op* op_c, const void* v0, uint64_t seed, double tol, int which,
                             int64_t max_iter, double* lmin, double* lmax, int64_t* iters) {
     RC_CHECK_CTX(ctx);

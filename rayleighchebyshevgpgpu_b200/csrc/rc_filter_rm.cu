@@ -309,6 +309,91 @@ rc_status rm_filter_corr(rc_ctx* ctx, rc_op* op, double* V, int64_t ldv, int64_t
     return rm_corr_select(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band);
 }
 
+// ---------------------------------------------------------------------------------------
+// One degree step on caller-owned row-major blocks (rc_filter_step_rm): the kernels of the
+// filter above with the same slice, group and offset choices, so a step over any row range of
+// an operator computes each row exactly as the filter does.
+// ---------------------------------------------------------------------------------------
+template <class Pol, class TS, class TC, int W>
+static rc_status step_once_w(rc_ctx* ctx, const Pol& pol, int64_t n, int64_t ld, const TS* x, const TS* z, TS* y,
+                             TC a, TC b, TC g, int64_t band) {
+    constexpr int VEC = Pack16<TS>::V;
+    const int nseg = (int)(ld / (VEC * W));
+    if (nseg > kRmThreads) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "degree step: block too wide");
+    constexpr bool kCsr = Pol::kIsCsr;
+    constexpr bool kF32 = sizeof(real_t<TS>) == 4;
+    const int groups = ctx->rm_groups > 0 ? ctx->rm_groups : (kCsr ? (kF32 ? 4 : 2) : (kF32 ? 8 : 4));
+    const int64_t pf_z = ctx->pf_rows;
+    const int64_t pf_x = pf_z > 0 ? pf_z + band : 0;
+    if ((n + 1) * ld < ((int64_t)1 << 32))
+        launch_step<Pol, TS, TC, W, uint32_t, false>(ctx, pol, n, nseg, ld, groups, x, z, y, a, b, g, pf_z, pf_x,
+                                                     (const TS*)nullptr, nullptr);
+    else
+        launch_step<Pol, TS, TC, W, int64_t, false>(ctx, pol, n, nseg, ld, groups, x, z, y, a, b, g, pf_z, pf_x,
+                                                    (const TS*)nullptr, nullptr);
+    RC_CU(ctx, cudaGetLastError());
+    return RC_OK;
+}
+
+template <class Pol, class TS, class TC>
+static rc_status step_once(rc_ctx* ctx, const Pol& pol, int64_t n, int64_t ld, const void* x, const void* z, void* y,
+                           const double* al, const double* be, const double* ga, int64_t band) {
+    const TC a = s_from<TC>(al[0], al[1]), b = s_from<TC>(be[0], be[1]);
+    const TC g = z ? s_from<TC>(ga[0], ga[1]) : s_zero(TC());
+    const int slices = ctx->rm_slices ? ctx->rm_slices : (Pol::kIsCsr && sizeof(real_t<TS>) == 8 ? 2 : 1);
+    if (slices == 2)
+        return step_once_w<Pol, TS, TC, 2>(ctx, pol, n, ld, (const TS*)x, (const TS*)z, (TS*)y, a, b, g, band);
+    return step_once_w<Pol, TS, TC, 1>(ctx, pol, n, ld, (const TS*)x, (const TS*)z, (TS*)y, a, b, g, band);
+}
+
+template <class TS, class TC>
+static rc_status step_dispatch(rc_ctx* ctx, rc_op* op, int64_t ld, const void* x, const void* z, void* y,
+                               const double* al, const double* be, const double* ga) {
+    const int64_t n = op->n;
+    const int64_t band = op->kind == 0 ? op->band : (op->skind == 5 ? op->nx : op->nx * op->ny);
+    if (op->kind == 0) {
+        const TS* vals = (const TS*)(sizeof(real_t<TS>) == 8 ? op->vals64 : op->vals32);
+        CsrRows<TS, TC> pol{op->rowptr, op->colind, vals};
+        return step_once<CsrRows<TS, TC>, TS, TC>(ctx, pol, n, ld, x, z, y, al, be, ga, band);
+    }
+    using TD = real_t<TS>;
+    const TD* dg = (const TD*)(sizeof(TD) == 8 ? (const void*)op->diag64 : (const void*)op->diag32);
+    const double theta = 2.0 * 3.14159265358979323846 * op->flux;
+    if (op->skind == 27) {
+        if constexpr (IsComplex<TC>::value) {
+            return rc_fail(ctx, RC_ERR_UNSUPPORTED, "27-point stencil is real only");
+        } else {
+            StencilRows<TD, TC, 27> pol{op->nx, op->ny, op->nz, dg, op->offdiag, theta};
+            return step_once<StencilRows<TD, TC, 27>, TS, TC>(ctx, pol, n, ld, x, z, y, al, be, ga, band);
+        }
+    }
+    if (op->skind == 7) {
+        StencilRows<TD, TC, 7> pol{op->nx, op->ny, op->nz, dg, op->offdiag, theta};
+        pol.ph = (const TC*)(sizeof(TD) == 8 ? op->phase64 : op->phase32);
+        return step_once<StencilRows<TD, TC, 7>, TS, TC>(ctx, pol, n, ld, x, z, y, al, be, ga, band);
+    }
+    StencilRows<TD, TC, 5> pol{op->nx, op->ny, op->nz, dg, op->offdiag, theta};
+    pol.ph = (const TC*)(sizeof(TD) == 8 ? op->phase64 : op->phase32);
+    return step_once<StencilRows<TD, TC, 5>, TS, TC>(ctx, pol, n, ld, x, z, y, al, be, ga, band);
+}
+
+rc_status rm_step(rc_ctx* ctx, rc_op* op, const void* x, const void* z, void* y, int64_t ld, int64_t s,
+                  const double* alpha, const double* beta, const double* gamma, int prec) {
+    if (op->kind == 2) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "degree step: callback operators have no row form");
+    const bool cplx = op->dtype == RC_COMPLEX128;
+    const int p = prec == RC_PREC_MIXED ? P32 : P64;
+    const int64_t q = rm_leading_dim(op->dtype, p, 1);  // the row length quantum (32 bytes)
+    if (ld < s || ld % q != 0)
+        return rc_fail(ctx, RC_ERR_INVALID, "degree step: ld must be >= s and a multiple of 32 bytes of elements");
+    if (p == P32) {
+        RC_TRY(ensure_fp32(ctx, op));
+        if (cplx) return step_dispatch<float2, float2>(ctx, op, ld, x, z, y, alpha, beta, gamma);
+        return step_dispatch<float, float>(ctx, op, ld, x, z, y, alpha, beta, gamma);
+    }
+    if (cplx) return step_dispatch<double2, double2>(ctx, op, ld, x, z, y, alpha, beta, gamma);
+    return step_dispatch<double, double>(ctx, op, ld, x, z, y, alpha, beta, gamma);
+}
+
 rc_status corr_coefficients(rc_ctx* ctx, int64_t s, int64_t ld, int64_t degree, double a, double b,
                             const double* lam_dev, float* sig, double* coef) {
     corr_coef_kernel<<<1, 128, 0, ctx->stream>>>(s, ld, degree, a, b, lam_dev, sig, coef);

@@ -186,6 +186,11 @@ bool rm_corr_supported(const rc_op* op, int64_t s);
 rc_status rm_filter_corr(rc_ctx* ctx, rc_op* op, double* V, int64_t ldv, int64_t s, int64_t degree, double a,
                          double b, const double* lam_dev, const rc_corr_t* R, void* bufA, void* bufB);
 int64_t rm_leading_dim(int dtype, int prec, int64_t s);
+// One degree step y = alpha A x + beta x + gamma z on row-major blocks (leading dimension ld, a
+// multiple of 32 bytes of elements), storage and arithmetic by prec (RC_PREC_FP64 / RC_PREC_MIXED);
+// alpha, beta, gamma are (re, im) pairs, z may be null. The filter's own step kernels.
+rc_status rm_step(rc_ctx* ctx, rc_op* op, const void* x, const void* z, void* y, int64_t ld, int64_t s,
+                  const double* alpha, const double* beta, const double* gamma, int prec);
 // Tables of a correction-filter application of degree m over rows of leading dimension ld: the
 // source coefficients sig[k*ld + c] = c_{k-1}(lam_c) (FP32, k = 2..m) and the weights
 // coef[c] = c_m(lam_c)/(m+1) (FP64) of the Ritz vectors in the result, written by

@@ -431,6 +431,23 @@ def filter_block(ctx: Context, op: Operator, X, s: int, degree: int, gamma1: flo
                           _PREC[precision]), ctx.h, "rc_filter")
 
 
+def rm_leading_dim(complex_: bool, precision: str, s: int) -> int:
+    """Leading dimension of the filter's row-major blocks (rc_rm_leading_dim)."""
+    return int(lib().rc_rm_leading_dim(capi.RC_COMPLEX128 if complex_ else capi.RC_REAL64, _PREC[precision], s))
+
+
+def filter_step_rm(ctx: Context, op: Operator, x, z, y, s: int, alpha, beta, gamma=0.0, precision: str = "fp64",
+                   ld=None):
+    """One degree step y = alpha A x + beta x + gamma z on row-major device blocks (rc_filter_step_rm)."""
+    def pair(v):
+        v = complex(v)
+        return (C.c_double * 2)(v.real, v.imag)
+    ld = ld or rm_leading_dim(op.complex_, precision, s)
+    check(lib().rc_filter_step_rm(ctx.h, op.h, C.c_void_p(_ptr(x)), C.c_void_p(_ptr(z)), C.c_void_p(_ptr(y)), ld, s,
+                                  pair(alpha), pair(beta), pair(gamma), _PREC[precision]), ctx.h,
+          "rc_filter_step_rm")
+
+
 def filter_correction(ctx: Context, op: Operator, V, s: int, lam, degree: int, gamma1: float, gamma2: float,
                       ld=None):
     """V <- P_m(A')V in correction form on Ritz pairs (V, lam): rc_filter_correction."""

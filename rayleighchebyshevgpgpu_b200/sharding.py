@@ -19,8 +19,13 @@ on the CPU):
   extended_csr     the rank's operator on its whole extended block, halo rows empty: with it, one
                    unsharded row-major degree step over the extended block computes the rank's rows
                    (the halo rows of the result are discarded and refilled by the next exchange).
-The device side of the sharded solve (the degree-step kernel reading the extended block, with the
-exchange between steps) is not part of this build: every run here has one GPU.
+and the device side of the sharded filter:
+  rank_operator    the rank's operator on its extended block on the GPU (extended CSR, or the stencil
+                   on the sub-grid of its planes plus halo planes);
+  extended_rows    a rank's extended row-major block cut from a global one;
+  sharded_filter   the Chebyshev filter on a rank's extended block: one library degree step
+                   (rc_filter_step_rm) per degree, the halo exchange between steps. Each rank's own
+                   rows come out bit for bit as the unsharded filter computes them.
 """
 from __future__ import annotations
 
@@ -145,3 +150,80 @@ def extended_csr(rowptr, colind, vals, sh: Shard):
     lrp, lci, lv = local_csr(rowptr, colind, vals, sh)
     rp = np.concatenate([np.zeros(sh.lo, dtype=np.int32), lrp, np.full(sh.hi, lrp[-1], dtype=np.int32)])
     return rp, lci, lv
+
+
+# ------------------------------------------------------------------------------------------
+# Device side (one rank's GPU)
+# ------------------------------------------------------------------------------------------
+def rank_operator(ctx, problem, sh: Shard, form: str = "csr"):
+    """The rank's operator on its extended block [halo_lo | own | halo_hi] on the GPU. CSR: the
+    extended CSR matrix (halo rows empty). Stencil (slabs of whole z-planes): the same stencil on the
+    sub-grid of the extended planes, with the diagonal of those planes; its halo rows are computed
+    with the wrong (Dirichlet) neighbours and discarded by the next exchange."""
+    from . import runtime as R
+    if form == "csr":
+        rp, ci, v = problem.csr()
+        return R.CsrOperator(ctx, *extended_csr(rp, ci, v, sh))
+    plane = problem.nx * problem.ny
+    e0, e1 = sh.r0 - sh.lo, sh.r1 + sh.hi
+    if e0 % plane or e1 % plane:
+        raise ValueError("stencil shards must be whole z-planes")
+    dims = (problem.nx, problem.ny, (e1 - e0) // plane) if len(problem.dims) == 3 else (problem.nx, (e1 - e0) // problem.nx)
+    kind = {5: 5, 7: 7, 27: 27}[problem.kind]
+    return R.StencilOperator(ctx, kind, dims, problem.diag[e0:e1], problem.offdiag, problem.flux,
+                             complex_=problem.complex_)
+
+
+def extended_rows(x_global, sh: Shard):
+    """The rank's extended block (rows [r0 - lo, r1 + hi)) of a global row-major block, as a copy."""
+    return x_global[sh.r0 - sh.lo:sh.r1 + sh.hi].clone()
+
+
+def filter_steps(ctx, op_ext, sh: Shard, x_ext, s: int, degree: int, gamma1: float, gamma2: float,
+                 precision: str = "fp64"):
+    """The rank's side of a sharded filter, one degree step at a time: a generator that runs
+    rc_filter_step_rm over the whole extended block and then yields the block x_k whose halo rows
+    must be refilled before the next step; after the last step it returns x_m/(m+1) in FP64 (c128)
+    as StopIteration.value, converted and scaled as the library's filter does at its end (the
+    scale multiplies in double). Ranks advance their generators in lockstep with an exchange
+    between yields (sharded_filter does that over torch.distributed)."""
+    import torch
+
+    from . import runtime as R
+    a, b = gamma2 * gamma1, gamma2
+    if degree < 1:
+        return x_ext.to(torch.complex128 if x_ext.is_complex() else torch.float64)
+    A = x_ext
+    B = torch.empty_like(x_ext)
+    ld = x_ext.shape[1]
+    for k in range(1, degree + 1):
+        xk1 = B if (k - 1) % 2 else A   # x_{k-1}
+        y = B if k % 2 else A           # x_k over x_{k-2}
+        torch.cuda.current_stream().synchronize()  # halo copies of the exchange are on torch's stream
+        if k == 1:
+            R.filter_step_rm(ctx, op_ext, xk1, None, y, s, a, b, 0.0, precision, ld=ld)
+        else:
+            R.filter_step_rm(ctx, op_ext, xk1, y, y, s, a, b, -1.0, precision, ld=ld)
+        ctx.synchronize()
+        yield y
+    xm = B if degree % 2 else A
+    wide = torch.complex128 if xm.is_complex() else torch.float64
+    return xm.to(wide).mul_(1.0 / (degree + 1))
+
+
+def sharded_filter(ctx, op_ext, sh: Shard, x_ext, s: int, degree: int, gamma1: float, gamma2: float,
+                   precision: str = "fp64", group=None):
+    """X <- P_m(A')X on the rank's extended row-major block x_ext (ext_rows x ld, storage precision of
+    `precision`, halo rows filled), with the recurrence of LanczosCpolyOperatorLMCuda::apply
+    (LanczosCpolyOperatorLMCuda.h:194-265): x_1 = a A x_0 + b x_0, x_k = a A x_{k-1} + b x_{k-1} - x_{k-2},
+    a = gamma2*gamma1, b = gamma2, result x_m/(m+1). One rc_filter_step_rm per degree over the whole
+    extended block, exchange_halo (torch.distributed: NCCL between GPUs) between steps. Every rank
+    calls it with the same degree and coefficients. Returns x_m/(m+1) on the extended block in FP64
+    (c128); its own rows are the rank's rows of the filtered block."""
+    gen = filter_steps(ctx, op_ext, sh, x_ext, s, degree, gamma1, gamma2, precision)
+    while True:
+        try:
+            blk = next(gen)
+        except StopIteration as e:
+            return e.value
+        exchange_halo(blk, sh, group)
