@@ -168,6 +168,7 @@ SIGNATURES = {
     "rc_ctx_synchronize": (C.c_int, [c_vp]),
     "rc_ctx_launch_count": (C.c_int, [c_vp, C.POINTER(c_i64), C.c_int]),
     "rc_ctx_device_bytes": (C.c_int, [c_vp, C.POINTER(c_i64)]),
+    "rc_ctx_counter": (C.c_int, [c_vp, C.c_char_p, C.POINTER(c_i64)]),
     "rc_op_csr_create": (C.c_int, [c_vp, C.c_int, c_i64, c_i64, c_vp, c_vp, c_vp, C.POINTER(c_vp)]),
     "rc_op_stencil_create": (C.c_int, [c_vp, C.c_int, C.c_int, c_i64, c_i64, c_i64, c_vp, C.c_double,
                                        C.c_double, C.POINTER(c_vp)]),

@@ -3,6 +3,7 @@
 // Every entry point validates its arguments, makes the context's device current, and
 // returns a status code; nothing here terminates the process (the reference's error macros
 // call exit(), cudaErrchk.h:8-51).
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cmath>
@@ -138,6 +139,9 @@ rc_status rc_ctx_create(int device, rc_ctx** out) {
         if (!std::strcmp(v, "loop")) c->csr_variant = 1;
         else if (!std::strcmp(v, "reg")) c->csr_variant = 2;
     }
+    if (const char* v = std::getenv("RCB200_STAGED")) c->staged = std::atoi(v) != 0 ? 1 : 0;
+    if (const char* v = std::getenv("RCB200_STAGED_ROWS")) c->staged_rows = std::max(0, std::atoi(v) / 4 * 4);
+    if (const char* v = std::getenv("RCB200_STAGED_STAGES")) c->staged_stages = std::max(0, std::min(4, std::atoi(v)));
     c->pf_rows = 4096;
     if (const char* v = std::getenv("RCB200_PF_ROWS")) c->pf_rows = std::max<int64_t>(0, std::atoll(v));
     if (const char* v = std::getenv("RCB200_RM_SLICES")) c->rm_slices = std::atoi(v) == 1 ? 1 : 2;
@@ -182,6 +186,14 @@ rc_status rc_ctx_launch_count(rc_ctx* ctx, int64_t* launches, int reset) {
     return RC_OK;
 }
 
+rc_status rc_ctx_counter(rc_ctx* ctx, const char* name, int64_t* value) {
+    if (!ctx || !name || !value) return RC_ERR_INVALID;
+    if (!std::strcmp(name, "launches")) *value = ctx->launches;
+    else if (!std::strcmp(name, "staged_launches")) *value = ctx->staged_launches;
+    else return rc_fail(ctx, RC_ERR_INVALID, std::string("rc_ctx_counter: unknown counter ") + name);
+    return RC_OK;
+}
+
 rc_status rc_ctx_device_bytes(rc_ctx* ctx, int64_t* bytes) {
     if (!ctx || !bytes) return RC_ERR_INVALID;
     int64_t t = ctx->op_bytes;
@@ -193,8 +205,10 @@ rc_status rc_ctx_device_bytes(rc_ctx* ctx, int64_t* bytes) {
 // ---------------------------------------------------------------------------------------
 // Operators
 // ---------------------------------------------------------------------------------------
+// Operator arrays carry 64 bytes of tail padding: the staged step kernels copy 16-byte aligned
+// spans of them, which may reach up to 15 bytes past the last element.
 static rc_status dev_copy(rc_ctx* ctx, void** dst, const void* src, size_t bytes, rc_op* op) {
-    if (cudaMalloc(dst, bytes ? bytes : 16) != cudaSuccess) {
+    if (cudaMalloc(dst, bytes + 64) != cudaSuccess) {
         cudaGetLastError();
         return rc_fail(ctx, RC_ERR_NOMEM, "cudaMalloc for operator storage failed");
     }
@@ -221,8 +235,17 @@ rc_status rc_op_csr_create(rc_ctx* ctx, int dtype, int64_t n, int64_t nnz, const
     for (int64_t k = 0; k < nnz; ++k)
         if (colind[k] < 0 || colind[k] >= n) return rc_fail(ctx, RC_ERR_INVALID, "column index out of range");
     int64_t band = 0;
+    std::vector<int64_t> offs;  // distinct column offsets, while there are few
+    bool few = true;
     for (int64_t i = 0; i < n; ++i)
-        for (int32_t k = rowptr[i]; k < rowptr[i + 1]; ++k) band = std::max<int64_t>(band, colind[k] - i);
+        for (int32_t k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+            const int64_t o = (int64_t)colind[k] - i;
+            band = std::max<int64_t>(band, o);
+            if (few && std::find(offs.begin(), offs.end(), o) == offs.end()) {
+                offs.push_back(o);
+                few = (int)offs.size() <= rc_op::kMaxOffsets;
+            }
+        }
     rc_op* op = new (std::nothrow) rc_op();
     if (!op) return RC_ERR_NOMEM;
     op->ctx = ctx;
@@ -232,6 +255,11 @@ rc_status rc_op_csr_create(rc_ctx* ctx, int dtype, int64_t n, int64_t nnz, const
     op->nnz = nnz;
     op->max_row_nnz = max_row;
     op->band = band;
+    if (few) {
+        std::sort(offs.begin(), offs.end());
+        op->n_offsets = (int)offs.size();
+        for (size_t q = 0; q < offs.size(); ++q) op->offsets[q] = offs[q];
+    }
     const size_t vsz = (dtype == RC_COMPLEX128 ? 16 : 8);
     rc_status st = dev_copy(ctx, (void**)&op->rowptr, rowptr, (size_t)(n + 1) * 4, op);
     if (st == RC_OK) st = dev_copy(ctx, (void**)&op->colind, colind, (size_t)nnz * 4, op);

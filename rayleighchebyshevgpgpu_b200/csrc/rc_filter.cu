@@ -345,7 +345,7 @@ rc_status ensure_fp32(rc_ctx* ctx, rc_op* op) {
     if (op->kind == 0 && op->vals32 == nullptr) {
         const int64_t cnt = op->nnz * (op->dtype == RC_COMPLEX128 ? 2 : 1);
         void* p = nullptr;
-        if (cudaMalloc(&p, (size_t)cnt * 4) != cudaSuccess)
+        if (cudaMalloc(&p, (size_t)cnt * 4 + 64) != cudaSuccess)  // tail padding as the other operator arrays
             return rc_fail(ctx, RC_ERR_NOMEM, "cudaMalloc failed for FP32 operator values");
         cvt_f64_f32_kernel<<<4 * kB200Sms, 256, 0, ctx->stream>>>((const double*)op->vals64, (float*)p, cnt);
         ctx->launches++;
@@ -356,7 +356,7 @@ rc_status ensure_fp32(rc_ctx* ctx, rc_op* op) {
     }
     if (op->kind == 1 && op->diag32 == nullptr) {
         void* p = nullptr;
-        if (cudaMalloc(&p, (size_t)op->n * 4) != cudaSuccess)
+        if (cudaMalloc(&p, (size_t)op->n * 4 + 64) != cudaSuccess)
             return rc_fail(ctx, RC_ERR_NOMEM, "cudaMalloc failed for FP32 stencil diagonal");
         cvt_f64_f32_kernel<<<4 * kB200Sms, 256, 0, ctx->stream>>>(op->diag64, (float*)p, op->n);
         ctx->launches++;

@@ -12,12 +12,15 @@
 //   step k:    x_k over x_{k-2}, row-major (one pass: read x_{k-1}, x_{k-2}, write x_k)
 //   to_cm:     x_m/(m+1) row-major -> X column-major (FP64)
 // Storage/compute: FP32 (c64) in MIXED precision, FP64 (c128) otherwise.
+#include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <type_traits>
 #include "rc_common.cuh"
 #include "rc_internal.h"
 #include "rc_rowops.cuh"
 #include "rc_rmstep.cuh"
+#include "rc_staged.cuh"
 
 namespace rcb {
 
@@ -52,10 +55,182 @@ rm_step27_kernel(StencilRows<TD, TC, 27> op, int64_t n, int nseg, int64_t ld, co
                                                gamma, pf_z, pf_x, src, sig);
 }
 
+// ---------------------------------------------------------------------------------------
+// The staged step (rc_staged.cuh): its plan and launch
+// ---------------------------------------------------------------------------------------
+// The distinct column offsets of an operator's rows, when they are few, and its longest row.
+struct StageOffsets {
+    int n = 0;
+    int64_t off[rc_op::kMaxOffsets] = {};
+    int64_t max_row_nnz = 0;
+};
+
+static bool stage_offsets(const rc_op* op, StageOffsets* so) {
+    so->n = 0;
+    if (op->kind == 0) {
+        if (op->n_offsets < 1) return false;
+        so->n = op->n_offsets;
+        for (int q = 0; q < op->n_offsets; ++q) so->off[q] = op->offsets[q];
+        so->max_row_nnz = op->max_row_nnz;
+        return true;
+    }
+    if (op->kind == 1 && (op->skind == 5 || op->skind == 7)) {
+        const int64_t nx = op->nx, sz = op->nx * op->ny;
+        int k = 0;
+        if (op->skind == 7) so->off[k++] = -sz;
+        so->off[k++] = -nx;
+        so->off[k++] = -1;
+        so->off[k++] = 0;
+        so->off[k++] = 1;
+        so->off[k++] = nx;
+        if (op->skind == 7) so->off[k++] = sz;
+        std::sort(so->off, so->off + k);
+        so->n = (int)(std::unique(so->off, so->off + k) - so->off);
+        so->max_row_nnz = op->skind;
+        return true;
+    }
+    return false;
+}
+
+// Group the offsets into windows (offsets at most 4 rows apart share one), then take the largest
+// chunk of rows whose stages fit half the SM's shared memory (two CTAs per SM), else the whole:
+// three stages with at least 16 rows, else two with at least 8 (or the context's rows and stages,
+// when it sets them).
+static bool staged_plan(const rc_ctx* ctx, const StageOffsets& so, int64_t n, int64_t ld, int tm_bytes, bool has_z,
+                        bool has_src, bool csr, int ta_bytes, StagedPlan* out) {
+    int nw = 0;
+    int64_t glo[kStagedMaxWin], ghi[kStagedMaxWin];
+    for (int q = 0; q < so.n; ++q) {
+        if (nw > 0 && so.off[q] - ghi[nw - 1] <= 4) {
+            ghi[nw - 1] = so.off[q];
+            continue;
+        }
+        if (nw == kStagedMaxWin) return false;
+        glo[nw] = ghi[nw] = so.off[q];
+        ++nw;
+    }
+    const int64_t rb = ld * tm_bytes;
+    if (nw == 0 || rb % 16 != 0 || rb > 16384) return false;
+    auto up = [](int64_t b) { return (b + 127) / 128 * 128; };
+    // two CTAs per SM share the SM's shared memory (the per-block opt-in limit plus the 1 KB the
+    // system reserves per block), with 1 KB reserved for each; blocks too wide for that take a
+    // whole SM
+    const int64_t budget2 = ((int64_t)ctx->smem_optin + 1024) / 2 - 1536;
+    const int64_t budget1 = (int64_t)ctx->smem_optin - 4096;
+    auto layout = [&](int R, StagedPlan& Q) {
+        int64_t off = 0;
+        Q.nwin = nw;
+        for (int w = 0; w < nw; ++w) {
+            Q.lo[w] = glo[w];
+            Q.span[w] = (int)(ghi[w] - glo[w]);
+            Q.win_off[w] = (int)off;
+            off += up((R + Q.span[w]) * rb);
+        }
+        Q.z_off = Q.src_off = Q.rp_off = Q.ci_off = Q.va_off = -1;
+        if (has_z) {
+            Q.z_off = (int)off;
+            off += up(R * rb);
+        }
+        if (has_src) {
+            Q.src_off = (int)off;
+            off += up(R * rb);
+        }
+        if (csr) {
+            Q.rp_off = (int)off;
+            off += up((int64_t)(R + 8) * 4);
+            Q.csr_cap = (int)(R * so.max_row_nnz + 8);
+            Q.ci_off = (int)off;
+            off += up((int64_t)Q.csr_cap * 4);
+            Q.va_off = (int)off;
+            off += up((int64_t)Q.csr_cap * ta_bytes);
+        }
+        Q.R = R;
+        Q.stage_bytes = (int)off;
+        return off;
+    };
+    for (int per_sm = 2; per_sm >= 1; --per_sm) {
+        const int64_t budget = per_sm == 2 ? budget2 : budget1;
+        for (int nst = 4; nst >= 2; --nst) {
+            if (ctx->staged_stages ? nst != ctx->staged_stages : nst == 4) continue;
+            const int rmin = ctx->staged_rows ? ctx->staged_rows : (nst == 3 ? 16 : 8);
+            const int rmax = ctx->staged_rows ? ctx->staged_rows : 256;
+            for (int R = rmax; R >= rmin; R -= 4) {
+                StagedPlan Q;
+                if (nst * layout(R, Q) <= budget) {
+                    Q.nstages = nst;
+                    Q.nchunks = (n + R - 1) / R;
+                    Q.ctas_per_sm = per_sm;
+                    *out = Q;
+                    return true;
+                }
+            }
+        }
+    }
+    return false;
+}
+
+template <class P, class = void>
+struct CsrValue {
+    using type = float;
+};
+template <class P>
+struct CsrValue<P, std::void_t<typename P::value_t>> {
+    using type = typename P::value_t;
+};
+
+// Launch the staged step when the operator and the blocks allow it; false leaves the step to the
+// per-row gather kernels.
+template <class Pol, class TS, class TC, int W, bool SRC, class TM>
+static bool try_staged(rc_ctx* ctx, const Pol& pol, const StageOffsets* so, int64_t n, int nseg, int64_t ld,
+                       const TM* x, const TM* z, TM* y, TC a, TC b, TC g, const TM* src, const float* sig) {
+    if (!so || !ctx->staged || so->n == 0 || nseg > kStagedThreads) return false;
+    auto al16 = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
+    if (!al16(x) || (z && !al16(z)) || !al16(y) || (SRC && !al16(src))) return false;
+    constexpr bool kCsr = Pol::kIsCsr;
+    using TA = typename CsrValue<Pol>::type;
+    StagedPlan P;
+    if (!staged_plan(ctx, *so, n, ld, (int)sizeof(TM), z != nullptr, SRC, kCsr, (int)sizeof(TA), &P)) return false;
+    StagedArgs<TM, TC> A;
+    A.n = n;
+    A.nseg = nseg;
+    A.ld = ld;
+    A.row_bytes = (int)(ld * (int64_t)sizeof(TM));
+    A.x = x;
+    A.z = z;
+    A.y = y;
+    A.src = src;
+    A.sig = sig;
+    A.alpha = a;
+    A.beta = b;
+    A.gamma = g;
+    if constexpr (kCsr) {
+        A.rowptr = pol.rowptr;
+        A.colind = pol.colind;
+        A.vals = pol.vals;
+        if (!al16(pol.rowptr) || !al16(pol.colind) || !al16(pol.vals)) return false;
+    }
+    auto kern = rm_staged_kernel<Pol, kCsr, TS, TC, W, SRC, TM, TA>;
+    // the dynamic shared-memory limit, once per device (the same value from every caller)
+    static std::atomic<unsigned long long> limit_set{0};
+    const unsigned long long bit = 1ull << (ctx->device & 63);
+    if (!(limit_set.load() & bit)) {
+        if (allow_max_smem(ctx, kern) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        limit_set.fetch_or(bit);
+    }
+    const unsigned grid = (unsigned)std::min<int64_t>(P.nchunks, (int64_t)P.ctas_per_sm * ctx->sm_count);
+    kern<<<grid, kStagedThreads, (size_t)P.nstages * P.stage_bytes, ctx->stream>>>(P, A, pol);
+    ctx->launches++;
+    ctx->staged_launches++;
+    return true;
+}
+
 template <class Pol, class TS, class TC, int W, class IX, bool SRC, class TM = TS>
 static void launch_step(rc_ctx* ctx, const Pol& pol, int64_t n, int nseg, int64_t ld, int groups, const TM* x,
                         const TM* z, TM* y, TC a, TC b, TC g, int64_t pf_z, int64_t pf_x, const TM* src,
-                        const float* sig) {
+                        const float* sig, const StageOffsets* so = nullptr) {
     const int rows_per_iter = kRmThreads / nseg;
     if constexpr (IsStencil27<Pol>::value) {
         using TD = typename IsStencil27<Pol>::diag_t;
@@ -64,6 +239,7 @@ static void launch_step(rc_ctx* ctx, const Pol& pol, int64_t n, int nseg, int64_
         rm_step27_kernel<TD, TS, TC, W, IX, SRC, TM><<<grid, kRmThreads, 0, ctx->stream>>>(pol, n, nseg, ld, x, z, y, a,
                                                                                            b, g, pf_z, pf_x, src, sig);
     } else {
+        if (try_staged<Pol, TS, TC, W, SRC, TM>(ctx, pol, so, n, nseg, ld, x, z, y, a, b, g, src, sig)) return;
         const int64_t rows_per_cta = (int64_t)groups * rows_per_iter;
         const unsigned grid = (unsigned)((n + rows_per_cta - 1) / rows_per_cta);
         if constexpr (SRC)
@@ -128,7 +304,8 @@ to_cm_kernel(int64_t n, int64_t s, const TS* __restrict__ Rr, int64_t ld, TV* __
 //   X <- x_m / (m+1) (column-major).
 template <class Pol, class TS, class TC, int W, class IX>
 static rc_status run_rm_filter(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, int64_t ldv, int64_t s,
-                               int64_t degree, double a, double b, void* bufA, void* bufB, int64_t ld, int64_t band) {
+                               int64_t degree, double a, double b, void* bufA, void* bufB, int64_t ld, int64_t band,
+                               const StageOffsets* so) {
     const int64_t pf_z = ctx->pf_rows;
     const int64_t pf_x = pf_z > 0 ? pf_z + band : 0;
     using TY = typename std::conditional<IsComplex<TC>::value, double2, double>::type;
@@ -156,7 +333,8 @@ static rc_status run_rm_filter(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, 
         // k = 1 has no x_{k-2} (gamma = 0): z is not read
         const TS* z = k >= 2 ? y : nullptr;
         launch_step<Pol, TS, TC, W, IX, false>(ctx, pol, n, nseg, ld, groups, xk1, z, y, ta, tb,
-                                               k >= 2 ? tm1 : s_zero(TC()), pf_z, pf_x, (const TS*)nullptr, nullptr);
+                                               k >= 2 ? tm1 : s_zero(TC()), pf_z, pf_x, (const TS*)nullptr, nullptr,
+                                               so);
     }
     RC_CU(ctx, cudaGetLastError());
     step_mark(ctx);
@@ -179,7 +357,7 @@ static rc_status run_rm_filter(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, 
 template <class Pol, class TS, class TC, int W, class IX, class TM>
 static rc_status run_rm_corr(rc_ctx* ctx, const Pol& pol, int64_t n, double* V, int64_t ldv, int64_t s,
                              int64_t degree, double a, double b, const TM* R, const float* sig, const double* coef,
-                             TM* A, TM* B, int64_t ld, int64_t band) {
+                             TM* A, TM* B, int64_t ld, int64_t band, const StageOffsets* so) {
     const int64_t pf_z = ctx->pf_rows;
     const int64_t pf_x = pf_z > 0 ? pf_z + band : 0;
     constexpr int VEC = Slice<TS, TM>::V;  // 8 values per 16-byte slice for bfloat16 blocks
@@ -195,7 +373,7 @@ static rc_status run_rm_corr(rc_ctx* ctx, const Pol& pol, int64_t n, double* V, 
         TM* y = k % 2 == 0 ? A : B;                                  // e_k
         const TM* z = k == 2 ? nullptr : (k == 3 ? R : y);           // e_{k-2}
         launch_step<Pol, TS, TC, W, IX, true, TM>(ctx, pol, n, nseg, ld, groups, xk1, z, y, ta, tb,
-                                                  k == 2 ? s_zero(TC()) : tm1, pf_z, pf_x, R, sig + k * ld);
+                                                  k == 2 ? s_zero(TC()) : tm1, pf_z, pf_x, R, sig + k * ld, so);
     }
     RC_CU(ctx, cudaGetLastError());
     step_mark(ctx);
@@ -213,14 +391,19 @@ static rc_status run_rm_corr(rc_ctx* ctx, const Pol& pol, int64_t n, double* V, 
 // (RCB200_RM_SLICES=1 or 2).
 template <class Pol, class TS, class TC>
 static rc_status run_rm_select(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, int64_t ldv, int64_t s,
-                               int64_t degree, double a, double b, void* bufA, void* bufB, int64_t ld, int64_t band) {
+                               int64_t degree, double a, double b, void* bufA, void* bufB, int64_t ld, int64_t band,
+                               const StageOffsets* so) {
     const bool small = (n + 1) * ld < ((int64_t)1 << 32);
     const int slices = ctx->rm_slices ? ctx->rm_slices : (Pol::kIsCsr && sizeof(real_t<TS>) == 8 ? 2 : 1);
     if (slices == 1)
-        return small ? run_rm_filter<Pol, TS, TC, 1, uint32_t>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band)
-                     : run_rm_filter<Pol, TS, TC, 1, int64_t>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band);
-    return small ? run_rm_filter<Pol, TS, TC, 2, uint32_t>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band)
-                 : run_rm_filter<Pol, TS, TC, 2, int64_t>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band);
+        return small ? run_rm_filter<Pol, TS, TC, 1, uint32_t>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band,
+                                                                  so)
+                     : run_rm_filter<Pol, TS, TC, 1, int64_t>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band,
+                                                              so);
+    return small ? run_rm_filter<Pol, TS, TC, 2, uint32_t>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band,
+                                                           so)
+                 : run_rm_filter<Pol, TS, TC, 2, int64_t>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band,
+                                                          so);
 }
 
 template <class TS, class TC>
@@ -228,10 +411,12 @@ static rc_status rm_filter_dispatch(rc_ctx* ctx, rc_op* op, void* V, int64_t ldv
                                     double a, double b, void* bufA, void* bufB, int64_t ld) {
     const int64_t n = op->n;
     const int64_t band = op->kind == 0 ? op->band : (op->skind == 5 ? op->nx : op->nx * op->ny);
+    StageOffsets so_v;
+    const StageOffsets* so = stage_offsets(op, &so_v) ? &so_v : nullptr;
     if (op->kind == 0) {
         const TS* vals = (const TS*)(sizeof(real_t<TS>) == 8 ? op->vals64 : op->vals32);
         CsrRows<TS, TC> pol{op->rowptr, op->colind, vals};
-        return run_rm_select<CsrRows<TS, TC>, TS, TC>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band);
+        return run_rm_select<CsrRows<TS, TC>, TS, TC>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band, so);
     }
     using TD = real_t<TS>;
     const TD* dg = (const TD*)(sizeof(TD) == 8 ? (const void*)op->diag64 : (const void*)op->diag32);
@@ -242,29 +427,31 @@ static rc_status rm_filter_dispatch(rc_ctx* ctx, rc_op* op, void* V, int64_t ldv
         } else {
             StencilRows<TD, TC, 27> pol{op->nx, op->ny, op->nz, dg, op->offdiag, theta};
             return run_rm_select<StencilRows<TD, TC, 27>, TS, TC>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB,
-                                                                  ld, band);
+                                                                  ld, band, so);
         }
     }
     if (op->skind == 7) {
         StencilRows<TD, TC, 7> pol{op->nx, op->ny, op->nz, dg, op->offdiag, theta};
         pol.ph = (const TC*)(sizeof(TD) == 8 ? op->phase64 : op->phase32);
         return run_rm_select<StencilRows<TD, TC, 7>, TS, TC>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld,
-                                                             band);
+                                                             band, so);
     }
     StencilRows<TD, TC, 5> pol{op->nx, op->ny, op->nz, dg, op->offdiag, theta};
     pol.ph = (const TC*)(sizeof(TD) == 8 ? op->phase64 : op->phase32);
-    return run_rm_select<StencilRows<TD, TC, 5>, TS, TC>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band);
+    return run_rm_select<StencilRows<TD, TC, 5>, TS, TC>(ctx, pol, n, V, ldv, s, degree, a, b, bufA, bufB, ld, band,
+                                                         so);
 }
 
 template <class Pol>
 static rc_status rm_corr_select(rc_ctx* ctx, const Pol& pol, int64_t n, double* V, int64_t ldv, int64_t s,
                                 int64_t degree, double a, double b, const rc_corr_t* R, const float* sig,
-                                const double* coef, rc_corr_t* A, rc_corr_t* B, int64_t ld, int64_t band) {
+                                const double* coef, rc_corr_t* A, rc_corr_t* B, int64_t ld, int64_t band,
+                                const StageOffsets* so) {
     if ((n + 1) * ld < ((int64_t)1 << 32))
         return run_rm_corr<Pol, float, float, 1, uint32_t, rc_corr_t>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig,
-                                                                      coef, A, B, ld, band);
+                                                                      coef, A, B, ld, band, so);
     return run_rm_corr<Pol, float, float, 1, int64_t, rc_corr_t>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef,
-                                                                 A, B, ld, band);
+                                                                 A, B, ld, band, so);
 }
 
 bool rm_corr_supported(const rc_op* op, int64_t s) {
@@ -292,21 +479,23 @@ rc_status rm_filter_corr(rc_ctx* ctx, rc_op* op, double* V, int64_t ldv, int64_t
     const int64_t band = op->kind == 0 ? op->band : (op->skind == 5 ? op->nx : op->nx * op->ny);
     rc_corr_t* A = (rc_corr_t*)bufA;
     rc_corr_t* B = (rc_corr_t*)bufB;
+    StageOffsets so_v;
+    const StageOffsets* so = stage_offsets(op, &so_v) ? &so_v : nullptr;
     if (op->kind == 0) {
         CsrRows<float, float> pol{op->rowptr, op->colind, (const float*)op->vals32};
-        return rm_corr_select(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band);
+        return rm_corr_select(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band, so);
     }
     const double theta = 0.0;
     if (op->skind == 27) {
         StencilRows<float, float, 27> pol{op->nx, op->ny, op->nz, op->diag32, op->offdiag, theta};
-        return rm_corr_select(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band);
+        return rm_corr_select(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band, so);
     }
     if (op->skind == 7) {
         StencilRows<float, float, 7> pol{op->nx, op->ny, op->nz, op->diag32, op->offdiag, theta};
-        return rm_corr_select(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band);
+        return rm_corr_select(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band, so);
     }
     StencilRows<float, float, 5> pol{op->nx, op->ny, op->nz, op->diag32, op->offdiag, theta};
-    return rm_corr_select(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band);
+    return rm_corr_select(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band, so);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -316,7 +505,7 @@ rc_status rm_filter_corr(rc_ctx* ctx, rc_op* op, double* V, int64_t ldv, int64_t
 // ---------------------------------------------------------------------------------------
 template <class Pol, class TS, class TC, int W>
 static rc_status step_once_w(rc_ctx* ctx, const Pol& pol, int64_t n, int64_t ld, const TS* x, const TS* z, TS* y,
-                             TC a, TC b, TC g, int64_t band) {
+                             TC a, TC b, TC g, int64_t band, const StageOffsets* so) {
     constexpr int VEC = Pack16<TS>::V;
     const int nseg = (int)(ld / (VEC * W));
     if (nseg > kRmThreads) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "degree step: block too wide");
@@ -327,23 +516,24 @@ static rc_status step_once_w(rc_ctx* ctx, const Pol& pol, int64_t n, int64_t ld,
     const int64_t pf_x = pf_z > 0 ? pf_z + band : 0;
     if ((n + 1) * ld < ((int64_t)1 << 32))
         launch_step<Pol, TS, TC, W, uint32_t, false>(ctx, pol, n, nseg, ld, groups, x, z, y, a, b, g, pf_z, pf_x,
-                                                     (const TS*)nullptr, nullptr);
+                                                     (const TS*)nullptr, nullptr, so);
     else
         launch_step<Pol, TS, TC, W, int64_t, false>(ctx, pol, n, nseg, ld, groups, x, z, y, a, b, g, pf_z, pf_x,
-                                                    (const TS*)nullptr, nullptr);
+                                                    (const TS*)nullptr, nullptr, so);
     RC_CU(ctx, cudaGetLastError());
     return RC_OK;
 }
 
 template <class Pol, class TS, class TC>
 static rc_status step_once(rc_ctx* ctx, const Pol& pol, int64_t n, int64_t ld, const void* x, const void* z, void* y,
-                           const double* al, const double* be, const double* ga, int64_t band) {
+                           const double* al, const double* be, const double* ga, int64_t band,
+                           const StageOffsets* so) {
     const TC a = s_from<TC>(al[0], al[1]), b = s_from<TC>(be[0], be[1]);
     const TC g = z ? s_from<TC>(ga[0], ga[1]) : s_zero(TC());
     const int slices = ctx->rm_slices ? ctx->rm_slices : (Pol::kIsCsr && sizeof(real_t<TS>) == 8 ? 2 : 1);
     if (slices == 2)
-        return step_once_w<Pol, TS, TC, 2>(ctx, pol, n, ld, (const TS*)x, (const TS*)z, (TS*)y, a, b, g, band);
-    return step_once_w<Pol, TS, TC, 1>(ctx, pol, n, ld, (const TS*)x, (const TS*)z, (TS*)y, a, b, g, band);
+        return step_once_w<Pol, TS, TC, 2>(ctx, pol, n, ld, (const TS*)x, (const TS*)z, (TS*)y, a, b, g, band, so);
+    return step_once_w<Pol, TS, TC, 1>(ctx, pol, n, ld, (const TS*)x, (const TS*)z, (TS*)y, a, b, g, band, so);
 }
 
 template <class TS, class TC>
@@ -351,10 +541,12 @@ static rc_status step_dispatch(rc_ctx* ctx, rc_op* op, int64_t ld, const void* x
                                const double* al, const double* be, const double* ga) {
     const int64_t n = op->n;
     const int64_t band = op->kind == 0 ? op->band : (op->skind == 5 ? op->nx : op->nx * op->ny);
+    StageOffsets so_v;
+    const StageOffsets* so = stage_offsets(op, &so_v) ? &so_v : nullptr;
     if (op->kind == 0) {
         const TS* vals = (const TS*)(sizeof(real_t<TS>) == 8 ? op->vals64 : op->vals32);
         CsrRows<TS, TC> pol{op->rowptr, op->colind, vals};
-        return step_once<CsrRows<TS, TC>, TS, TC>(ctx, pol, n, ld, x, z, y, al, be, ga, band);
+        return step_once<CsrRows<TS, TC>, TS, TC>(ctx, pol, n, ld, x, z, y, al, be, ga, band, so);
     }
     using TD = real_t<TS>;
     const TD* dg = (const TD*)(sizeof(TD) == 8 ? (const void*)op->diag64 : (const void*)op->diag32);
@@ -364,17 +556,17 @@ static rc_status step_dispatch(rc_ctx* ctx, rc_op* op, int64_t ld, const void* x
             return rc_fail(ctx, RC_ERR_UNSUPPORTED, "27-point stencil is real only");
         } else {
             StencilRows<TD, TC, 27> pol{op->nx, op->ny, op->nz, dg, op->offdiag, theta};
-            return step_once<StencilRows<TD, TC, 27>, TS, TC>(ctx, pol, n, ld, x, z, y, al, be, ga, band);
+            return step_once<StencilRows<TD, TC, 27>, TS, TC>(ctx, pol, n, ld, x, z, y, al, be, ga, band, so);
         }
     }
     if (op->skind == 7) {
         StencilRows<TD, TC, 7> pol{op->nx, op->ny, op->nz, dg, op->offdiag, theta};
         pol.ph = (const TC*)(sizeof(TD) == 8 ? op->phase64 : op->phase32);
-        return step_once<StencilRows<TD, TC, 7>, TS, TC>(ctx, pol, n, ld, x, z, y, al, be, ga, band);
+        return step_once<StencilRows<TD, TC, 7>, TS, TC>(ctx, pol, n, ld, x, z, y, al, be, ga, band, so);
     }
     StencilRows<TD, TC, 5> pol{op->nx, op->ny, op->nz, dg, op->offdiag, theta};
     pol.ph = (const TC*)(sizeof(TD) == 8 ? op->phase64 : op->phase32);
-    return step_once<StencilRows<TD, TC, 5>, TS, TC>(ctx, pol, n, ld, x, z, y, al, be, ga, band);
+    return step_once<StencilRows<TD, TC, 5>, TS, TC>(ctx, pol, n, ld, x, z, y, al, be, ga, band, so);
 }
 
 rc_status rm_step(rc_ctx* ctx, rc_op* op, const void* x, const void* z, void* y, int64_t ld, int64_t s,

@@ -63,6 +63,15 @@ struct rc_ctx {
     // consecutive row groups per CTA in the row-major filter steps: 0 = by operator kind and
     // storage precision, else 1..64. RCB200_RM_GROUPS.
     int rm_groups = 0;
+    // Degree steps with their operands staged in shared memory (rc_staged.cuh) for
+    // stencil-structured operators: 1, or 0 (default: the per-row gather kernels, measured faster
+    // on the 128^3 workloads), from RCB200_STAGED.
+    int staged = 0;
+    int64_t staged_launches = 0;
+    // staged step shape: rows per chunk (multiple of 4) and pipeline stages; 0 = the largest that
+    // fit. RCB200_STAGED_ROWS, RCB200_STAGED_STAGES.
+    int staged_rows = 0;
+    int staged_stages = 0;
     // CUDA-event pairs around the degree-step loops of the row-major filter (no transposes),
     // recorded while step_timing is set; step_flush() waits for them and adds to step_ms.
     bool step_timing = false;
@@ -91,6 +100,11 @@ struct rc_op {
     int64_t nnz = 0;
     int64_t max_row_nnz = 0;
     int64_t band = 0;  // max over entries of (column - row): distance to the farthest later neighbour
+    // distinct column offsets (column - row) of all entries, ascending, when there are at most
+    // kMaxOffsets of them (a stencil-structured matrix); n_offsets = -1 otherwise
+    static constexpr int kMaxOffsets = 32;
+    int n_offsets = -1;
+    int64_t offsets[kMaxOffsets] = {};
     int32_t* rowptr = nullptr;
     int32_t* colind = nullptr;
     void* vals64 = nullptr;

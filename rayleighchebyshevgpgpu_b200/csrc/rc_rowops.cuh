@@ -17,6 +17,7 @@ namespace rcb {
 template <class TA, class TC>
 struct CsrRows {
     static constexpr bool kIsCsr = true;
+    using value_t = TA;
     const int32_t* __restrict__ rowptr;
     const int32_t* __restrict__ colind;
     const TA* __restrict__ vals;

@@ -68,6 +68,11 @@ class Context:
         check(lib().rc_ctx_launch_count(self.h, C.byref(v), 1 if reset else 0), self.h)
         return v.value
 
+    def counter(self, name: str) -> int:
+        v = C.c_int64()
+        check(lib().rc_ctx_counter(self.h, name.encode(), C.byref(v)), self.h, "rc_ctx_counter")
+        return v.value
+
     def device_bytes(self) -> int:
         v = C.c_int64()
         check(lib().rc_ctx_device_bytes(self.h, C.byref(v)), self.h)

@@ -72,6 +72,7 @@ def test_sharded_steps_equal_unsharded_bitwise(ctx, world, form, kind, precision
         want = e.value
     # the library's own column-major filter
     Xc = torch.from_numpy(x0.copy()).cuda()
+    torch.cuda.synchronize()  # the library works on its own stream
     R.filter_block(ctx, op, Xc, S_COLS, DEGREE, G1, G2, precision=precision)
     ctx.synchronize()
     assert torch.equal(want[:, :S_COLS].to(torch.float64), Xc.T)
