@@ -169,14 +169,15 @@ rc_status rc_filter_step_rm(rc_ctx* ctx, const rc_op* op, const void* x, const v
 
 /* The filter above in correction form, the MIXED-precision refinement step of rc_solve (no
  * reference counterpart; it computes LanczosCpolyOperatorLMCuda::apply, LanczosCpolyOperatorLMCuda.h:194-265,
- * on Ritz pairs). V (n x s, DEVICE, FP64) holds Ritz vectors v_c with Ritz values lam[c] (HOST, s
- * doubles). With a = gamma2*gamma1, b = gamma2, the scalar recurrence c_0 = 1, c_1 = a lam + b,
+ * on Ritz pairs). V (n x s, DEVICE, FP64, or c128 for complex Hermitian operators) holds Ritz
+ * vectors v_c with Ritz values lam[c] (HOST, s doubles). With a = gamma2*gamma1, b = gamma2, the scalar recurrence c_0 = 1, c_1 = a lam + b,
  * c_k = (a lam + b) c_{k-1} - c_{k-2}, and the residual block R = A V - V diag(lam):
  *   e_1 = R,  e_k = a*A*e_{k-1} + b*e_{k-1} - e_{k-2} + c_{k-1} R,
  *   V <- (c_m V + a e_m)/(m+1)     (= x_m/(m+1) of rc_filter in exact arithmetic),
- * with R and every e_k stored in bfloat16 and FP32 arithmetic; the last combination is FP64.
- * Real CSR or 5/7/27-point stencil operators, 1 <= s <= 96, degree >= 1. Returns after the work
- * is complete. */
+ * with R and every e_k stored in bfloat16 (complex: real and imaginary part each a bfloat16) and
+ * FP32 (c64) arithmetic; the last combination is FP64. CSR or 5/7-point stencil operators, real or
+ * complex, and real 27-point stencils; 1 <= s <= 256, degree >= 1. Returns after the work is
+ * complete. */
 rc_status rc_filter_correction(rc_ctx* ctx, const rc_op* op, void* V, int64_t ld, int64_t s, const double* lam,
                                int64_t degree, double gamma1, double gamma2);
 
@@ -184,7 +185,7 @@ rc_status rc_filter_correction(rc_ctx* ctx, const rc_op* op, void* V, int64_t ld
 typedef struct rc_correction_job {
     size_t struct_size;            /* sizeof(rc_correction_job), or 0 */
     const rc_op* op;
-    void* V;                       /* DEVICE n x s FP64 block, leading dimension ld; distinct per job */
+    void* V;                       /* DEVICE n x s FP64 (c128) block, leading dimension ld; distinct per job */
     int64_t ld;
     int64_t s;
     const double* lam;             /* HOST, s Ritz values */
@@ -195,9 +196,9 @@ typedef struct rc_correction_job {
 /* Several rc_filter_correction applications (up to 64, each with its own operator, block, degree
  * and coefficients) whose degree steps run as one batched launch per step: the request server's
  * batched correction-filter kernels, with each block's arithmetic equal to rc_filter_correction's.
- * Jobs those kernels do not take (27-point stencils, blocks with 64-bit element offsets) run
- * through the single-block kernels in the same call. batched (optional out): the number of jobs
- * that ran in the batched launches. No reference counterpart. */
+ * Jobs those kernels do not take (complex operators, 27-point stencils, blocks with 64-bit element
+ * offsets) run through the single-block kernels in the same call. batched (optional out): the
+ * number of jobs that ran in the batched launches. No reference counterpart. */
 rc_status rc_filter_correction_batch(rc_ctx* ctx, int njobs, const rc_correction_job* jobs, int* batched);
 
 /* Spectral bounds by single-vector Lanczos with Sturm multisection of the tridiagonal

@@ -180,7 +180,10 @@ def filter_block(A, X: np.ndarray, m: int, g1: float, g2: float, reps: int = 1) 
 
 def round_bf16(x) -> np.ndarray:
     """Values rounded to bfloat16 (round to nearest, ties to even, via float32), returned as float64:
-    the storage rounding of the correction filter's blocks."""
+    the storage rounding of the correction filter's blocks. Complex values round their real and
+    imaginary parts separately (complex128 out)."""
+    if np.iscomplexobj(x):
+        return round_bf16(np.real(x)) + 1j * round_bf16(np.imag(x))
     f = np.ascontiguousarray(x, dtype=np.float32)
     u = f.view(np.uint32).astype(np.uint64)
     u = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16

@@ -485,6 +485,69 @@ __device__ __forceinline__ void rr_pair(int r, int i, int M, int sp, int& p, int
     }
 }
 
+// Rotation angle of pair (p, q) from a_pq, a_pp, a_qq; *sn = 0 (no rotation) when |a_pq| is below
+// the absolute or relative threshold.
+template <class T>
+__device__ __forceinline__ void jac_angle(T apq, double app, double aqq, double abs_tol, double rel_tol, double& c,
+                                          double& sn, T& u) {
+    c = 1.0;
+    sn = 0.0;
+    u = s_from<T>(1.0, 0.0);
+    if constexpr (!IsComplex<T>::value) {
+        // real: u = sign(apq), and the angle from one square root and one division,
+        // t = sign(d) 2|apq| / (|d| + sqrt(d^2 + 4 apq^2)) with d = aqq - app
+        const double mag = fabs(s_real(apq));
+        if (mag > abs_tol && mag * mag > rel_tol * rel_tol * fabs(app * aqq)) {
+            u = s_from<T>(s_real(apq) >= 0.0 ? 1.0 : -1.0, 0.0);
+            const double d = aqq - app;
+            const double t = copysign(2.0 * mag, d) / (fabs(d) + sqrt(d * d + 4.0 * mag * mag));
+            c = rsqrt(1.0 + t * t);
+            sn = t * c;
+        }
+    } else {
+        const double mag = sqrt(s_abs2(apq));
+        if (mag > abs_tol && mag > rel_tol * sqrt(fabs(app * aqq))) {
+            u = s_rscale(1.0 / mag, apq);
+            const double tau = (aqq - app) / (2.0 * mag);
+            const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+            c = 1.0 / sqrt(1.0 + t * t);
+            sn = t * c;
+        }
+    }
+}
+
+// The 2x2 block A[{p_i,q_i},{p_j,q_j}] <- G_i^H A G_j: columns [b_p b_q] = [a_p a_q] G_j, then rows
+// G_i^H [b_p.; b_q.]. On a diagonal block (bi == bj) with a rotation the off-diagonal entries are set
+// to exact zeros and the diagonal to its real part.
+template <class T>
+__device__ __forceinline__ void jac_block(T& a_pp, T& a_qp, T& a_pq, T& a_qq, double ci, double si, T ui, double cj,
+                                          double sj, T uj, bool diag) {
+    const T sju = s_rscale(sj, uj), sjc = s_rscale(sj, s_conj(uj));
+    const T b_pp = s_sub(s_rscale(cj, a_pp), s_mul(sjc, a_pq));
+    const T b_qp = s_sub(s_rscale(cj, a_qp), s_mul(sjc, a_qq));
+    const T b_pq = s_add(s_mul(sju, a_pp), s_rscale(cj, a_pq));
+    const T b_qq = s_add(s_mul(sju, a_qp), s_rscale(cj, a_qq));
+    const T siu = s_rscale(si, ui), sic = s_rscale(si, s_conj(ui));
+    a_pp = s_sub(s_rscale(ci, b_pp), s_mul(siu, b_qp));
+    a_qp = s_add(s_mul(sic, b_pp), s_rscale(ci, b_qp));
+    a_pq = s_sub(s_rscale(ci, b_pq), s_mul(siu, b_qq));
+    a_qq = s_add(s_mul(sic, b_pq), s_rscale(ci, b_qq));
+    if (diag && si != 0.0) {
+        a_qp = s_zero(T());
+        a_pq = s_zero(T());
+        a_pp = s_from<T>(s_real(a_pp), 0.0);
+        a_qq = s_from<T>(s_real(a_qq), 0.0);
+    }
+}
+
+// Row entries (q_p, q_q) of columns p_j, q_j of Q <- Q G_j.
+template <class T>
+__device__ __forceinline__ void jac_qrot(T& qp, T& qq, double cj, double sj, T uj) {
+    const T np = s_sub(s_rscale(cj, qp), s_mul(s_rscale(sj, s_conj(uj)), qq));
+    qq = s_add(s_mul(s_rscale(sj, uj), qp), s_rscale(cj, qq));
+    qp = np;
+}
+
 // Threads of the one-CTA Jacobi (a multiple of 32, at most 1024).
 #ifndef RC_JACOBI_THREADS
 #define RC_JACOBI_THREADS 1024
@@ -545,32 +608,10 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
                 rr_pair<T>(r, i, M, sp, p, q);
                 double c = 1.0, sn = 0.0;
                 T u = s_from<T>(1.0, 0.0);
-                if (q < s && !IsComplex<T>::value) {
-                    // real: u = sign(apq), and the angle from one square root and one division,
-                    // t = sign(d) 2|apq| / (|d| + sqrt(d^2 + 4 apq^2)) with d = aqq - app
-                    const double apq = s_real(A[p + q * ld]);
-                    const double app = s_real(A[p + p * ld]), aqq = s_real(A[q + q * ld]);
-                    const double mag = fabs(apq);
-                    if (mag > abs_tol && mag * mag > rel_tol * rel_tol * fabs(app * aqq)) {
-                        u = s_from<T>(apq >= 0.0 ? 1.0 : -1.0, 0.0);
-                        const double d = aqq - app;
-                        const double t = copysign(2.0 * mag, d) / (fabs(d) + sqrt(d * d + 4.0 * mag * mag));
-                        c = rsqrt(1.0 + t * t);
-                        sn = t * c;
-                        snbits = max(snbits, (unsigned long long)__double_as_longlong(fabs(sn)));
-                    }
-                } else if (q < s) {
-                    const T apq = A[p + q * ld];
-                    const double app = s_real(A[p + p * ld]), aqq = s_real(A[q + q * ld]);
-                    const double mag = sqrt(s_abs2(apq));
-                    if (mag > abs_tol && mag > rel_tol * sqrt(fabs(app * aqq))) {
-                        u = s_rscale(1.0 / mag, apq);
-                        const double tau = (aqq - app) / (2.0 * mag);
-                        const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-                        c = 1.0 / sqrt(1.0 + t * t);
-                        sn = t * c;
-                        snbits = max(snbits, (unsigned long long)__double_as_longlong(fabs(sn)));
-                    }
+                if (q < s) {
+                    jac_angle<T>(A[p + q * ld], s_real(A[p + p * ld]), s_real(A[q + q * ld]), abs_tol, rel_tol, c, sn,
+                                 u);
+                    snbits = max(snbits, (unsigned long long)__double_as_longlong(fabs(sn)));
                 }
                 rc[i] = c;
                 rsn[i] = sn;
@@ -595,37 +636,18 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
                 const double si = rsn[bi], sj = rsn[bj];
                 if (si == 0.0 && sj == 0.0) continue;
                 const int pi = pp[bi], qi = qq[bi], pj = pp[bj], qj = qq[bj];
-                const double ci = rc[bi], cj = rc[bj];
-                const T ui = ru[bi], uj = ru[bj];
-                const T a_pp = A[pi + pj * ld], a_qp = A[qi + pj * ld];
-                const T a_pq = A[pi + qj * ld], a_qq = A[qi + qj * ld];
-                // columns: [b_p b_q] = [a_p a_q] G_j
-                const T sju = s_rscale(sj, uj), sjc = s_rscale(sj, s_conj(uj));
-                const T b_pp = s_sub(s_rscale(cj, a_pp), s_mul(sjc, a_pq));
-                const T b_qp = s_sub(s_rscale(cj, a_qp), s_mul(sjc, a_qq));
-                const T b_pq = s_add(s_mul(sju, a_pp), s_rscale(cj, a_pq));
-                const T b_qq = s_add(s_mul(sju, a_qp), s_rscale(cj, a_qq));
-                // rows: G_i^H [b_p.; b_q.]
-                const T siu = s_rscale(si, ui), sic = s_rscale(si, s_conj(ui));
-                T n_pp = s_sub(s_rscale(ci, b_pp), s_mul(siu, b_qp));
-                T n_qp = s_add(s_mul(sic, b_pp), s_rscale(ci, b_qp));
-                T n_pq = s_sub(s_rscale(ci, b_pq), s_mul(siu, b_qq));
-                T n_qq = s_add(s_mul(sic, b_pq), s_rscale(ci, b_qq));
-                if (bi == bj && si != 0.0) {  // the rotated 2x2 diagonal block: exact zeros off-diagonal
-                    n_qp = s_zero(T());
-                    n_pq = s_zero(T());
-                    n_pp = s_from<T>(s_real(n_pp), 0.0);
-                    n_qq = s_from<T>(s_real(n_qq), 0.0);
-                }
-                A[pi + pj * ld] = n_pp;
-                A[qi + pj * ld] = n_qp;
-                A[pi + qj * ld] = n_pq;
-                A[qi + qj * ld] = n_qq;
+                T a_pp = A[pi + pj * ld], a_qp = A[qi + pj * ld];
+                T a_pq = A[pi + qj * ld], a_qq = A[qi + qj * ld];
+                jac_block<T>(a_pp, a_qp, a_pq, a_qq, rc[bi], si, ru[bi], rc[bj], sj, ru[bj], bi == bj);
+                A[pi + pj * ld] = a_pp;
+                A[qi + pj * ld] = a_qp;
+                A[pi + qj * ld] = a_pq;
+                A[qi + qj * ld] = a_qq;
                 if (bi != bj) {
-                    A[pj + pi * ld] = s_conj(n_pp);
-                    A[pj + qi * ld] = s_conj(n_qp);
-                    A[qj + pi * ld] = s_conj(n_pq);
-                    A[qj + qi * ld] = s_conj(n_qq);
+                    A[pj + pi * ld] = s_conj(a_pp);
+                    A[pj + qi * ld] = s_conj(a_qp);
+                    A[qj + pi * ld] = s_conj(a_pq);
+                    A[qj + qi * ld] = s_conj(a_qq);
                 }
             }
             // Q <- Q G_j (columns p_j, q_j of rows 0..s-1)
@@ -634,11 +656,10 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
                 const double sj = rsn[bj];
                 if (sj == 0.0) continue;
                 const int pj = pp[bj], qj = qq[bj];
-                const double cj = rc[bj];
-                const T uj = ru[bj];
-                const T qp = Q[row + pj * ld], qq_ = Q[row + qj * ld];
-                Q[row + pj * ld] = s_sub(s_rscale(cj, qp), s_mul(s_rscale(sj, s_conj(uj)), qq_));
-                Q[row + qj * ld] = s_add(s_mul(s_rscale(sj, uj), qp), s_rscale(cj, qq_));
+                T qp = Q[row + pj * ld], qv = Q[row + qj * ld];
+                jac_qrot<T>(qp, qv, rc[bj], sj, ru[bj]);
+                Q[row + pj * ld] = qp;
+                Q[row + qj * ld] = qv;
             }
             __syncthreads();
         }
@@ -664,6 +685,200 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
         for (int row = 0; row < s; ++row) Qout[row + (int64_t)rank * s] = Q[row + i * ld];
     }
     if (tid == 0 && info) info[0] = sweep;
+}
+
+// ---------------------------------------------------------------------------------------
+// The same Jacobi over a grid of CTAs, for matrices whose working copies do not fit in one CTA's
+// shared memory (complex s > 82, real s > 118). The working copies stay in global memory (L2), and
+// one round's updates, which touch every entry of A and Q, are split over the CTAs: CTA b forms a
+// contiguous share of the 2x2 blocks (bi <= bj) and of the (row, pair) entries of Q, then all CTAs
+// meet at a grid barrier. Every CTA computes all the round's angles itself from the same entries,
+// so the rotations, the convergence test and the number of sweeps agree in every CTA without
+// further communication. Global reads and writes of the working copies bypass L1 (ld/st .cg):
+// another SM may have written them since the last barrier. The grid is launched cooperatively
+// (all CTAs resident); the barrier's spin is bounded all the same, and on a timeout the kernel
+// stops, writes -1 to info[0] and NaN eigenvalues.
+// ---------------------------------------------------------------------------------------
+constexpr int kJacGridThreads = 256;
+constexpr long long kJacBarrierSpins = 1ll << 26;  // ~ seconds with the back-off below
+
+// Grid barrier over `nblocks` CTAs on two words: bar[0] counts arrivals, bar[1] is the generation.
+// Returns false when the wait gave up (and sets bar[2]).
+__device__ __forceinline__ bool jac_grid_barrier(unsigned* bar, unsigned nblocks, unsigned& gen) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        __threadfence();
+        if (atomicAdd(&bar[0], 1u) == nblocks - 1) {
+            atomicExch(&bar[0], 0u);
+            __threadfence();
+            atomicExch(&bar[1], gen + 1);
+        } else {
+            long long spins = 0;
+            while (atomicAdd(&bar[1], 0u) == gen) {
+                if (++spins > kJacBarrierSpins || atomicAdd(&bar[2], 0u) != 0u) {
+                    atomicExch(&bar[2], 1u);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = ok && atomicAdd(&bar[2], 0u) == 0;
+    }
+    __syncthreads();
+    ++gen;
+    return s_ok != 0;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kJacGridThreads)
+jacobi_grid_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __restrict__ evals, int* info,
+                   T* work, int max_sweeps) {
+    const int sp = s + (s & 1);
+    const int npair = sp / 2;
+    const int ld = sp + 1;
+    T* A = work;
+    T* Q = A + (size_t)sp * ld;
+    unsigned* bar = reinterpret_cast<unsigned*>(info + 1);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* rc = (double*)smem_raw;
+    double* rsn = rc + npair;
+    T* ru = (T*)(rsn + npair);
+    int* pp = (int*)(ru + npair);
+    int* qq = pp + npair;
+    __shared__ int s_rot;
+    __shared__ unsigned long long s_maxsn;
+    __shared__ double red[32];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int G = gridDim.x, b = blockIdx.x;
+    unsigned gen = 0;
+    bool ok = true;
+    // working copies: CTA b initialises its share of the entries
+    {
+        const int64_t tot = (int64_t)sp * sp;
+        for (int64_t e = (int64_t)b * nt + tid; e < tot; e += (int64_t)G * nt) {
+            const int i = (int)(e % sp), j = (int)(e / sp);
+            __stcg(A + i + (int64_t)j * ld, (i < s && j < s) ? Ain[i + (int64_t)j * s] : s_zero(T()));
+            __stcg(Q + i + (int64_t)j * ld, s_from<T>(i == j ? 1.0 : 0.0, 0.0));
+        }
+    }
+    // the Frobenius norm of the input, in the same order in every CTA
+    double f = 0.0;
+    for (int e = tid; e < s * s; e += nt) f += s_abs2(Ain[e]);
+    f = block_sum(f, red);
+    const double abs_tol = 1e-17 * sqrt(f);
+    const double rel_tol = 1e-15;
+    const int M = sp - 1;
+    const int64_t nblk = (int64_t)npair * (npair + 1) / 2;         // 2x2 blocks with bi <= bj
+    const int64_t blk0 = nblk * b / G, blk1 = nblk * (b + 1) / G;  // this CTA's share
+    const int64_t nq = (int64_t)s * npair;                         // (row, pair) entries of Q
+    const int64_t q0 = nq * b / G, q1 = nq * (b + 1) / G;
+    ok = jac_grid_barrier(bar, G, gen);
+    int sweep = 0;
+    for (; ok && sweep < max_sweeps; ++sweep) {
+        if (tid == 0) {
+            s_rot = 0;
+            s_maxsn = 0ull;
+        }
+        __syncthreads();
+        for (int r = 0; r < M && ok; ++r) {
+            unsigned long long snbits = 0ull;
+            for (int i = tid; i < npair; i += nt) {
+                int p, q;
+                rr_pair<T>(r, i, M, sp, p, q);
+                double c = 1.0, sn = 0.0;
+                T u = s_from<T>(1.0, 0.0);
+                if (q < s) {
+                    jac_angle<T>(__ldcg(A + p + (int64_t)q * ld), s_real(__ldcg(A + p + (int64_t)p * ld)),
+                                 s_real(__ldcg(A + q + (int64_t)q * ld)), abs_tol, rel_tol, c, sn, u);
+                    snbits = max(snbits, (unsigned long long)__double_as_longlong(fabs(sn)));
+                }
+                rc[i] = c;
+                rsn[i] = sn;
+                ru[i] = u;
+                pp[i] = p;
+                qq[i] = q;
+            }
+            if (tid < ((npair + 31) & ~31)) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) snbits = max(snbits, __shfl_xor_sync(0xffffffffu, snbits, o));
+                if ((tid & 31) == 0 && snbits) {
+                    atomicMax(&s_maxsn, snbits);
+                    s_rot = 1;
+                }
+            }
+            __syncthreads();
+            // this CTA's 2x2 blocks: linear index e over bj-major upper triangle (bi <= bj)
+            for (int64_t e = blk0 + tid; e < blk1; e += nt) {
+                // bj = largest with bj (bj + 1) / 2 <= e
+                int bj = (int)((sqrt(8.0 * (double)e + 1.0) - 1.0) * 0.5);
+                while ((int64_t)(bj + 1) * (bj + 2) / 2 <= e) ++bj;
+                while ((int64_t)bj * (bj + 1) / 2 > e) --bj;
+                const int bi = (int)(e - (int64_t)bj * (bj + 1) / 2);
+                const double si = rsn[bi], sj = rsn[bj];
+                if (si == 0.0 && sj == 0.0) continue;
+                const int pi = pp[bi], qi = qq[bi], pj = pp[bj], qj = qq[bj];
+                T* a0 = A + pi + (int64_t)pj * ld;
+                T* a1 = A + qi + (int64_t)pj * ld;
+                T* a2 = A + pi + (int64_t)qj * ld;
+                T* a3 = A + qi + (int64_t)qj * ld;
+                T a_pp = __ldcg(a0), a_qp = __ldcg(a1), a_pq = __ldcg(a2), a_qq = __ldcg(a3);
+                jac_block<T>(a_pp, a_qp, a_pq, a_qq, rc[bi], si, ru[bi], rc[bj], sj, ru[bj], bi == bj);
+                __stcg(a0, a_pp);
+                __stcg(a1, a_qp);
+                __stcg(a2, a_pq);
+                __stcg(a3, a_qq);
+                if (bi != bj) {
+                    __stcg(A + pj + (int64_t)pi * ld, s_conj(a_pp));
+                    __stcg(A + pj + (int64_t)qi * ld, s_conj(a_qp));
+                    __stcg(A + qj + (int64_t)pi * ld, s_conj(a_pq));
+                    __stcg(A + qj + (int64_t)qi * ld, s_conj(a_qq));
+                }
+            }
+            // this CTA's (row, pair) entries of Q <- Q G_j, rows fastest (coalesced columns)
+            for (int64_t e = q0 + tid; e < q1; e += nt) {
+                const int bj = (int)(e / s), row = (int)(e - (int64_t)bj * s);
+                const double sj = rsn[bj];
+                if (sj == 0.0) continue;
+                T* qpp = Q + row + (int64_t)pp[bj] * ld;
+                T* qqp = Q + row + (int64_t)qq[bj] * ld;
+                T qp = __ldcg(qpp), qv = __ldcg(qqp);
+                jac_qrot<T>(qp, qv, rc[bj], sj, ru[bj]);
+                __stcg(qpp, qp);
+                __stcg(qqp, qv);
+            }
+            ok = jac_grid_barrier(bar, G, gen);
+        }
+        const int rot = s_rot;
+        const double maxsn = __longlong_as_double((long long)s_maxsn);
+        __syncthreads();
+        if (!ok) break;
+        if (!rot || maxsn < 1e-9) {
+            if (rot) ++sweep;
+            break;
+        }
+    }
+    if (!ok) {
+        for (int i = b * nt + tid; i < s; i += G * nt) evals[i] = __longlong_as_double(0x7ff8000000000000ll);
+        if (b == 0 && tid == 0 && info) info[0] = -1;
+        return;
+    }
+    // ascending order (rank sort, ties by index); CTA b writes the columns i = b, b + G, ...
+    for (int i = b; i < s; i += G) {
+        const double li = s_real(__ldcg(A + i + (int64_t)i * ld));
+        int rank = 0;
+        for (int j = tid; j < s; j += nt) {
+            const double lj = s_real(__ldcg(A + j + (int64_t)j * ld));
+            if (lj < li || (lj == li && j < i)) ++rank;
+        }
+        rank = (int)block_sum((double)rank, red);
+        if (tid == 0) evals[rank] = li;
+        for (int row = tid; row < s; row += nt) Qout[row + (int64_t)rank * s] = __ldcg(Q + row + (int64_t)i * ld);
+    }
+    if (b == 0 && tid == 0 && info) info[0] = sweep;
 }
 
 size_t small_eigh_work_bytes(rc_ctx* ctx, int dtype, int64_t s) {
@@ -692,6 +907,21 @@ rc_status small_eigh_work(rc_ctx* ctx, int dtype, int64_t s, void* A, void* Q, d
     const size_t dyn = fit ? head + mats : head;
     if (!fit && !work) return rc_fail(ctx, RC_ERR_INVALID, "small_eigh: work memory required");
     const int sweeps = 60;
+    // working copies in global memory: the grid form over up to 32 CTAs (RCB200_JACOBI_CTAS; 1 keeps
+    // the one-CTA kernel), launched cooperatively, with its barrier words in info[1..3]
+    const int ctas = std::max(1, std::min(ctx->jacobi_ctas > 0 ? ctx->jacobi_ctas : 32, ctx->sm_count));
+    if (!fit && ctas > 1 && info) {
+        RC_CU(ctx, cudaMemsetAsync(info + 1, 0, 3 * sizeof(int), ctx->stream));
+        int si = (int)s;
+        int sw = sweeps;
+        void* args[] = {&si, &A, &Q, &evals, &info, &work, &sw};
+        const void* kern = dtype == RC_COMPLEX128 ? (const void*)jacobi_grid_kernel<double2>
+                                                  : (const void*)jacobi_grid_kernel<double>;
+        RC_CU(ctx, cudaLaunchCooperativeKernel(kern, dim3((unsigned)ctas), dim3(kJacGridThreads), args, dyn,
+                                               ctx->stream));
+        ctx->launches++;
+        return RC_OK;
+    }
     if (dtype == RC_COMPLEX128) {
         if (dyn > 48 * 1024)
             RC_CU(ctx, allow_max_smem(ctx, jacobi_kernel<double2>));

@@ -181,8 +181,8 @@ struct CsrValue<P, std::void_t<typename P::value_t>> {
 // Launch the staged step when the operator and the blocks allow it; false leaves the step to the
 // per-row gather kernels.
 template <class Pol, class TS, class TC, int W, bool SRC, class TM>
-static bool try_staged(rc_ctx* ctx, const Pol& pol, const StageOffsets* so, int64_t n, int nseg, int64_t ld,
-                       const TM* x, const TM* z, TM* y, TC a, TC b, TC g, const TM* src, const float* sig) {
+static bool try_staged_real(rc_ctx* ctx, const Pol& pol, const StageOffsets* so, int64_t n, int nseg, int64_t ld,
+                            const TM* x, const TM* z, TM* y, TC a, TC b, TC g, const TM* src, const float* sig) {
     if (!so || !ctx->staged || so->n == 0 || nseg > kStagedThreads) return false;
     auto al16 = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
     if (!al16(x) || (z && !al16(z)) || !al16(y) || (SRC && !al16(src))) return false;
@@ -225,6 +225,16 @@ static bool try_staged(rc_ctx* ctx, const Pol& pol, const StageOffsets* so, int6
     ctx->launches++;
     ctx->staged_launches++;
     return true;
+}
+
+template <class Pol, class TS, class TC, int W, bool SRC, class TM>
+static bool try_staged(rc_ctx* ctx, const Pol& pol, const StageOffsets* so, int64_t n, int nseg, int64_t ld,
+                       const TM* x, const TM* z, TM* y, TC a, TC b, TC g, const TM* src, const float* sig) {
+    if constexpr (SRC && IsComplex<TC>::value) {
+        return false;  // the staged kernel has no complex correction step
+    } else {
+        return try_staged_real<Pol, TS, TC, W, SRC, TM>(ctx, pol, so, n, nseg, ld, x, z, y, a, b, g, src, sig);
+    }
 }
 
 template <class Pol, class TS, class TC, int W, class IX, bool SRC, class TM = TS>
@@ -272,12 +282,13 @@ __global__ void corr_coef_kernel(int64_t s, int64_t ld, int64_t m, double a, dou
     }
 }
 
-template <class TM>
+template <class TM, class TV>
 __global__ void __launch_bounds__(256)
-corr_to_cm_kernel(int64_t n, int64_t s, const TM* __restrict__ E, int64_t ld, double* __restrict__ Vc, int64_t ldv,
+corr_to_cm_kernel(int64_t n, int64_t s, const TM* __restrict__ E, int64_t ld, TV* __restrict__ Vc, int64_t ldv,
                   const double* __restrict__ coef, double beta) {
-    __shared__ float tile[32][33];
-    corr_to_cm_tile<TM>(n, s, E, ld, Vc, ldv, coef, beta, (int64_t)blockIdx.x * 32, (int64_t)blockIdx.y * 32, tile);
+    __shared__ CorrTile<TM> tile[32][33];
+    corr_to_cm_tile<TM, TV>(n, s, E, ld, Vc, ldv, coef, beta, (int64_t)blockIdx.x * 32, (int64_t)blockIdx.y * 32,
+                            tile);
 }
 
 
@@ -345,17 +356,17 @@ static rc_status run_rm_filter(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, 
     return RC_OK;
 }
 
-// The correction filter (real operators; blocks stored as TM = rc_corr_t, bfloat16 by default,
-// FP32 arithmetic). V holds Ritz vectors v_c with Ritz values lam_c, and R = A V - V diag(lam)
-// (row-major, leading dimension ld). With x_k = c_k v + a e_k (c_k the scalar recurrence at
-// lam_c) the recurrence of run_rm_filter becomes
+// The correction filter (blocks stored as TM: rc_corr_t for real operators, rc_corr2_t for complex
+// Hermitian ones, bfloat16 by default; FP32 / c64 arithmetic). V holds Ritz vectors v_c with Ritz
+// values lam_c (real), and R = A V - V diag(lam) (row-major, leading dimension ld). With
+// x_k = c_k v + a e_k (c_k the real scalar recurrence at lam_c) the recurrence of run_rm_filter becomes
 //   e_0 = 0, e_1 = R, e_k = a A e_{k-1} + b e_{k-1} - e_{k-2} + c_{k-1} R,
 // and the result x_m/(m+1) = coef_c v_c + a e_m/(m+1) is formed in FP64. e_k is small (of the size
 // of the residual), so its rounding perturbs the filtered block by the storage rounding times the
 // residual instead of times the block: the subspace keeps converging past the FP32 floor of the
 // plain FP32 filter. e_2 -> A, e_3 -> B (e_1 = R is read as x_{k-2}), then e_k over e_{k-2}.
-template <class Pol, class TS, class TC, int W, class IX, class TM>
-static rc_status run_rm_corr(rc_ctx* ctx, const Pol& pol, int64_t n, double* V, int64_t ldv, int64_t s,
+template <class Pol, class TS, class TC, int W, class IX, class TM, class TV>
+static rc_status run_rm_corr(rc_ctx* ctx, const Pol& pol, int64_t n, TV* V, int64_t ldv, int64_t s,
                              int64_t degree, double a, double b, const TM* R, const float* sig, const double* coef,
                              TM* A, TM* B, int64_t ld, int64_t band, const StageOffsets* so) {
     const int64_t pf_z = ctx->pf_rows;
@@ -379,7 +390,8 @@ static rc_status run_rm_corr(rc_ctx* ctx, const Pol& pol, int64_t n, double* V, 
     step_mark(ctx);
     const TM* em = degree == 1 ? R : (degree % 2 == 0 ? A : B);
     const dim3 tgrid((unsigned)((n + 31) / 32), (unsigned)((s + 31) / 32)), tblk(32, 8);
-    corr_to_cm_kernel<TM><<<tgrid, tblk, 0, ctx->stream>>>(n, s, em, ld, V, ldv, coef, a / (double)(degree + 1));
+    corr_to_cm_kernel<TM, TV><<<tgrid, tblk, 0, ctx->stream>>>(n, s, em, ld, V, ldv, coef,
+                                                               a / (double)(degree + 1));
     ctx->launches++;
     RC_CU(ctx, cudaGetLastError());
     return RC_OK;
@@ -442,60 +454,83 @@ static rc_status rm_filter_dispatch(rc_ctx* ctx, rc_op* op, void* V, int64_t ldv
                                                          so);
 }
 
-template <class Pol>
-static rc_status rm_corr_select(rc_ctx* ctx, const Pol& pol, int64_t n, double* V, int64_t ldv, int64_t s,
-                                int64_t degree, double a, double b, const rc_corr_t* R, const float* sig,
-                                const double* coef, rc_corr_t* A, rc_corr_t* B, int64_t ld, int64_t band,
+template <class Pol, class TS, class TM, class TV>
+static rc_status rm_corr_select(rc_ctx* ctx, const Pol& pol, int64_t n, TV* V, int64_t ldv, int64_t s,
+                                int64_t degree, double a, double b, const TM* R, const float* sig,
+                                const double* coef, TM* A, TM* B, int64_t ld, int64_t band,
                                 const StageOffsets* so) {
     if ((n + 1) * ld < ((int64_t)1 << 32))
-        return run_rm_corr<Pol, float, float, 1, uint32_t, rc_corr_t>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig,
-                                                                      coef, A, B, ld, band, so);
-    return run_rm_corr<Pol, float, float, 1, int64_t, rc_corr_t>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef,
-                                                                 A, B, ld, band, so);
+        return run_rm_corr<Pol, TS, TS, 1, uint32_t, TM, TV>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B,
+                                                             ld, band, so);
+    return run_rm_corr<Pol, TS, TS, 1, int64_t, TM, TV>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld,
+                                                        band, so);
 }
 
+// Real operators (CSR, 5/7/27-point stencils) and complex Hermitian ones (CSR, 5/7-point stencils
+// with Peierls phases), blocks of up to 256 columns.
 bool rm_corr_supported(const rc_op* op, int64_t s) {
-    return op->dtype == RC_REAL64 && op->kind != 2 && s >= 1 && s <= 96 &&
-           (op->kind == 0 || op->skind == 5 || op->skind == 7 || op->skind == 27);
+    if (op->kind == 2 || s < 1 || s > kCorrMaxCols) return false;
+    if (op->dtype == RC_REAL64) return op->kind == 0 || op->skind == 5 || op->skind == 7 || op->skind == 27;
+    return op->dtype == RC_COMPLEX128 && (op->kind == 0 || op->skind == 5 || op->skind == 7);
 }
 
-rc_status rm_filter_corr(rc_ctx* ctx, rc_op* op, double* V, int64_t ldv, int64_t s, int64_t degree, double a,
-                         double b, const double* lam_dev, const rc_corr_t* R, void* bufA, void* bufB) {
+template <class TS, class TM, class TV>
+static rc_status rm_corr_dispatch(rc_ctx* ctx, rc_op* op, TV* V, int64_t ldv, int64_t s, int64_t degree, double a,
+                                  double b, const TM* R, const float* sig, const double* coef, TM* A, TM* B,
+                                  int64_t ld) {
+    const int64_t n = op->n;
+    const int64_t band = op->kind == 0 ? op->band : (op->skind == 5 ? op->nx : op->nx * op->ny);
+    StageOffsets so_v;
+    const StageOffsets* so = stage_offsets(op, &so_v) ? &so_v : nullptr;
+    if (op->kind == 0) {
+        CsrRows<TS, TS> pol{op->rowptr, op->colind, (const TS*)op->vals32};
+        return rm_corr_select<CsrRows<TS, TS>, TS>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band,
+                                                   so);
+    }
+    const double theta = 2.0 * 3.14159265358979323846 * op->flux;
+    if constexpr (!IsComplex<TS>::value) {
+        if (op->skind == 27) {
+            StencilRows<float, TS, 27> pol{op->nx, op->ny, op->nz, op->diag32, op->offdiag, theta};
+            return rm_corr_select<StencilRows<float, TS, 27>, TS>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef,
+                                                                  A, B, ld, band, so);
+        }
+    }
+    if (op->skind == 7) {
+        StencilRows<float, TS, 7> pol{op->nx, op->ny, op->nz, op->diag32, op->offdiag, theta};
+        pol.ph = (const TS*)op->phase32;
+        return rm_corr_select<StencilRows<float, TS, 7>, TS>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A,
+                                                             B, ld, band, so);
+    }
+    StencilRows<float, TS, 5> pol{op->nx, op->ny, op->nz, op->diag32, op->offdiag, theta};
+    pol.ph = (const TS*)op->phase32;
+    return rm_corr_select<StencilRows<float, TS, 5>, TS>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B,
+                                                         ld, band, so);
+}
+
+rc_status rm_filter_corr(rc_ctx* ctx, rc_op* op, void* V, int64_t ldv, int64_t s, int64_t degree, double a,
+                         double b, const double* lam_dev, const void* R, void* bufA, void* bufB) {
     if (!rm_corr_supported(op, s)) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "correction filter: unsupported operator");
     if (degree < 1) return RC_OK;
     RC_TRY(ensure_fp32(ctx, op));
-    const int64_t ld = rm_leading_dim(RC_REAL64, P32, s);
+    const bool cplx = op->dtype == RC_COMPLEX128;
+    const int64_t ld = corr_leading_dim(op->dtype, s);
     void* tab = nullptr;
     RC_TRY(rc_slot(ctx, S_CORR, corr_table_bytes(degree, ld), &tab));
     float* sig = (float*)tab;
     double* coef = (double*)((char*)tab + corr_table_coef_offset(degree, ld));
     RC_TRY(corr_coefficients(ctx, s, ld, degree, a, b, lam_dev, sig, coef));
-    if (ctx->serve) {  // under the request server: one job of a batched launch
+    if (ctx->serve && !cplx) {  // under the request server: one job of a batched launch
         bool handled = false;
-        RC_TRY(serve_filter_corr(ctx, op, V, ldv, s, degree, a, b, R, sig, coef, bufA, bufB, &handled));
+        RC_TRY(serve_filter_corr(ctx, op, (double*)V, ldv, s, degree, a, b, (const rc_corr_t*)R, sig, coef, bufA,
+                                 bufB, &handled));
         if (handled) return RC_OK;
     }
-    const int64_t n = op->n;
-    const int64_t band = op->kind == 0 ? op->band : (op->skind == 5 ? op->nx : op->nx * op->ny);
-    rc_corr_t* A = (rc_corr_t*)bufA;
-    rc_corr_t* B = (rc_corr_t*)bufB;
-    StageOffsets so_v;
-    const StageOffsets* so = stage_offsets(op, &so_v) ? &so_v : nullptr;
-    if (op->kind == 0) {
-        CsrRows<float, float> pol{op->rowptr, op->colind, (const float*)op->vals32};
-        return rm_corr_select(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band, so);
-    }
-    const double theta = 0.0;
-    if (op->skind == 27) {
-        StencilRows<float, float, 27> pol{op->nx, op->ny, op->nz, op->diag32, op->offdiag, theta};
-        return rm_corr_select(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band, so);
-    }
-    if (op->skind == 7) {
-        StencilRows<float, float, 7> pol{op->nx, op->ny, op->nz, op->diag32, op->offdiag, theta};
-        return rm_corr_select(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band, so);
-    }
-    StencilRows<float, float, 5> pol{op->nx, op->ny, op->nz, op->diag32, op->offdiag, theta};
-    return rm_corr_select(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band, so);
+    if (cplx)
+        return rm_corr_dispatch<float2, rc_corr2_t, double2>(ctx, op, (double2*)V, ldv, s, degree, a, b,
+                                                            (const rc_corr2_t*)R, sig, coef, (rc_corr2_t*)bufA,
+                                                            (rc_corr2_t*)bufB, ld);
+    return rm_corr_dispatch<float, rc_corr_t, double>(ctx, op, (double*)V, ldv, s, degree, a, b, (const rc_corr_t*)R,
+                                                      sig, coef, (rc_corr_t*)bufA, (rc_corr_t*)bufB, ld);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -594,11 +629,15 @@ rc_status corr_coefficients(rc_ctx* ctx, int64_t s, int64_t ld, int64_t degree, 
     return RC_OK;
 }
 
-rc_status to_row_major_f64(rc_ctx* ctx, int64_t n, int64_t s, const double* V, int64_t ldv, double* Yrm,
-                           int64_t ld) {
+rc_status to_row_major(rc_ctx* ctx, int dtype, int64_t n, int64_t s, const void* V, int64_t ldv, void* Yrm,
+                       int64_t ld) {
     if ((s + 31) / 32 > 65535) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "row-major copy: too many columns");
     const dim3 tgrid((unsigned)((n + 31) / 32), (unsigned)((s + 31) / 32)), tblk(32, 8);
-    to_rm_kernel<double, double><<<tgrid, tblk, 0, ctx->stream>>>(n, s, V, ldv, Yrm, ld);
+    if (dtype == RC_COMPLEX128)
+        to_rm_kernel<double2, double2><<<tgrid, tblk, 0, ctx->stream>>>(n, s, (const double2*)V, ldv, (double2*)Yrm,
+                                                                        ld);
+    else
+        to_rm_kernel<double, double><<<tgrid, tblk, 0, ctx->stream>>>(n, s, (const double*)V, ldv, (double*)Yrm, ld);
     ctx->launches++;
     RC_CU(ctx, cudaGetLastError());
     return RC_OK;

@@ -20,11 +20,16 @@ enum { P64 = 0, P32 = 1 };
 #ifndef RC_CORR_BF16
 #define RC_CORR_BF16 1
 #endif
+// Complex Hermitian operators store real and imaginary parts that way (rc_corr2_t).
 #if RC_CORR_BF16
 typedef __nv_bfloat16 rc_corr_t;
+typedef __nv_bfloat162 rc_corr2_t;
 #else
 typedef float rc_corr_t;
+typedef float2 rc_corr2_t;
 #endif
+// Widest block of the correction filter and of the residual-block kernel.
+constexpr int64_t kCorrMaxCols = 256;
 
 struct DevBuf {
     void* ptr = nullptr;
@@ -67,6 +72,9 @@ struct rc_ctx {
     // stencil-structured operators: 1, or 0 (default: the per-row gather kernels, measured faster
     // on the 128^3 workloads), from RCB200_STAGED.
     int staged = 0;
+    // CTAs of the Jacobi eigensolve when its working copies live in global memory (0 = 32; 1 = the
+    // one-CTA kernel), from RCB200_JACOBI_CTAS.
+    int jacobi_ctas = 0;
     int64_t staged_launches = 0;
     // staged step shape: rows per chunk (multiple of 4) and pipeline stages; 0 = the largest that
     // fit. RCB200_STAGED_ROWS, RCB200_STAGED_STAGES.
@@ -191,15 +199,19 @@ rc_status serve_filter(rc_ctx* ctx, rc_op* op, void* V, int64_t ld, int64_t s, i
 rc_status serve_filter_corr(rc_ctx* ctx, rc_op* op, double* V, int64_t ldv, int64_t s, int64_t degree, double a,
                             double b, const rc_corr_t* R, const float* sig, const double* coef, void* bufA,
                             void* bufB, bool* handled);
-// Correction filter (rc_filter_rm.cu), the MIXED precision refinement: V (FP64 column-major,
+// Correction filter (rc_filter_rm.cu), the MIXED precision refinement: V (FP64 / c128 column-major,
 // leading dimension ldv) holds Ritz vectors with Ritz values lam_dev (device) and R (row-major
-// rc_corr_t, leading dimension rm_leading_dim(RC_REAL64, P32, s)) their residual block A V - V diag(lam);
-// V <- P_m(A')V with FP32 storage of the (small) deviation from the scalar recurrence. bufA and
-// bufB: two row-major FP32 blocks of the same size as R.
+// rc_corr_t, or rc_corr2_t for complex operators, leading dimension corr_leading_dim(dtype, s))
+// their residual block A V - V diag(lam); V <- P_m(A')V with bfloat16 (or FP32) storage of the
+// (small) deviation from the scalar recurrence. bufA and bufB: two row-major blocks of the same
+// size as R.
 bool rm_corr_supported(const rc_op* op, int64_t s);
-rc_status rm_filter_corr(rc_ctx* ctx, rc_op* op, double* V, int64_t ldv, int64_t s, int64_t degree, double a,
-                         double b, const double* lam_dev, const rc_corr_t* R, void* bufA, void* bufB);
+rc_status rm_filter_corr(rc_ctx* ctx, rc_op* op, void* V, int64_t ldv, int64_t s, int64_t degree, double a,
+                         double b, const double* lam_dev, const void* R, void* bufA, void* bufB);
 int64_t rm_leading_dim(int dtype, int prec, int64_t s);
+// Leading dimension (elements) and element bytes of the correction filter's row-major blocks.
+inline int64_t corr_leading_dim(int dtype, int64_t s) { return rm_leading_dim(dtype, P32, s); }
+inline size_t corr_elem_bytes(int dtype) { return dtype == RC_COMPLEX128 ? sizeof(rc_corr2_t) : sizeof(rc_corr_t); }
 // One degree step y = alpha A x + beta x + gamma z on row-major blocks (leading dimension ld, a
 // multiple of 32 bytes of elements), storage and arithmetic by prec (RC_PREC_FP64 / RC_PREC_MIXED);
 // alpha, beta, gamma are (re, im) pairs, z may be null. The filter's own step kernels.
@@ -217,9 +229,10 @@ inline size_t corr_table_bytes(int64_t degree, int64_t ld) {
 }
 rc_status corr_coefficients(rc_ctx* ctx, int64_t s, int64_t ld, int64_t degree, double a, double b,
                             const double* lam_dev, float* sig, double* coef);
-// Row-major FP64 copy Yrm (leading dimension ld) of the column-major n x s block V.
-rc_status to_row_major_f64(rc_ctx* ctx, int64_t n, int64_t s, const double* V, int64_t ldv, double* Yrm,
-                           int64_t ld);
+// Row-major FP64 (c128 for RC_COMPLEX128) copy Yrm (leading dimension ld) of the column-major n x s
+// block V.
+rc_status to_row_major(rc_ctx* ctx, int dtype, int64_t n, int64_t s, const void* V, int64_t ldv, void* Yrm,
+                       int64_t ld);
 // Build the FP32 (c64) copy of an operator's values/diagonal used by the MIXED filter.
 rc_status ensure_fp32(rc_ctx* ctx, rc_op* op);
 // Degree-step timing (ctx->step_timing): record an event on the context stream; step_flush
@@ -265,13 +278,14 @@ rc_status xt2(rc_ctx* ctx, int64_t n, int64_t k, int64_t nc, const double* X, in
               int64_t ldt, double* Y, int64_t ldy, const double* W, int64_t ldw, const double* lam, int64_t res_count,
               double* res, float* R32 = nullptr, int64_t ldr = 0, double* Yrm = nullptr, int64_t ldyr = 0);
 
-// Residual block of Ritz vectors on native real operators (rc_resid.cu): R = A Y - Y diag(lam)
-// from the row-major FP64 copy Yrm of Y (leading dimension rm_leading_dim(RC_REAL64, P64, s)),
-// its column norms ||R_c|| for c < res_count into res (device), and with R32 the row-major FP32
-// copy of R (leading dimension rm_leading_dim(RC_REAL64, P32, s)). One pass over Yrm.
+// Residual block of Ritz vectors on native operators (rc_resid.cu; real, or complex CSR and 5/7-point
+// stencils; s <= kCorrMaxCols): R = A Y - Y diag(lam) from the row-major FP64 (c128) copy Yrm of Y
+// (leading dimension rm_leading_dim(dtype, P64, s)), its column norms ||R_c|| for c < res_count into
+// res (device), and with R the row-major copy of R in the correction filter's storage (rc_corr_t or
+// rc_corr2_t, leading dimension corr_leading_dim(dtype, s)). One pass over Yrm.
 bool resid_supported(const rc_op* op, int64_t s);
-rc_status resid_block(rc_ctx* ctx, const rc_op* op, const double* Yrm, int64_t ld, int64_t s, const double* lam,
-                      int64_t res_count, double* res, rc_corr_t* R32, int64_t ldr);
+rc_status resid_block(rc_ctx* ctx, const rc_op* op, const void* Yrm, int64_t ld, int64_t s, const double* lam,
+                      int64_t res_count, double* res, void* R, int64_t ldr);
 
 // Cholesky factor of Gram G (s x s) with diagonal scaling, shift on breakdown;
 // writes Tout = D^-1 R^-1 (upper). flags (device int[4]): [0] shifted, [1] failed, [2] zero column.

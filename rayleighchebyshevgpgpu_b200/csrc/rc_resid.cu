@@ -3,29 +3,47 @@
 // The reference forms tmp = A*V with a second SpMM and then runs its residuals kernel
 // (RayleighChebyshevLMCuda.h:2235, :2274-2280; cuda_kernels.cu:307-382). Here the sparse product,
 // the subtraction, the column norms ||R_c|| (c < res_count) and, for the correction filter, the
-// row-major bfloat16 (rc_corr_t) copy of R are one kernel over the row-major FP64 copy of Y that the Ritz GEMM
-// writes beside the column-major one (xt2): the filter's degree-step arithmetic (rc_rmstep.cuh
-// layout: 16-byte slices, consecutive row groups per CTA), so a neighbour row is one contiguous
-// run and the far neighbours (i +- band) are L2 hits. Nothing n x s is written in FP64.
+// row-major bfloat16 copy of R (rc_corr_t, or rc_corr2_t for complex operators) are one kernel over
+// a row-major FP64 (c128) copy of Y: the filter's degree-step arithmetic (rc_rmstep.cuh layout:
+// 16-byte slices, consecutive row groups per CTA), so a neighbour row is one contiguous run and the
+// far neighbours (i +- band) are L2 hits. Nothing n x s is written in FP64.
 // Column norms: each thread sums the squares of its own columns over its rows, the threads of a
 // CTA are combined in shared memory in a fixed order, and the per-CTA partials are summed in a
 // fixed order by resid_norm_reduce_kernel (deterministic).
 #include <algorithm>
+#include <type_traits>
 #include "rc_common.cuh"
 #include "rc_internal.h"
 #include "rc_rmstep.cuh"
 
 namespace rcb {
 
-// 4 resident CTAs per SM (64 registers): the residual epilogue keeps per-column sums and Ritz
-// values in registers, which spill at the filter steps' 40.
-template <class Pol, int W, class IX>
+// Two FP32 values of the residual block at p: two real columns, or the real and imaginary part of
+// one complex column.
+__device__ __forceinline__ void corr_store2(void* p, float a, float b) {
+#if RC_CORR_BF16
+    *reinterpret_cast<__nv_bfloat162*>(p) = __floats2bfloat162_rn(a, b);
+#else
+    *reinterpret_cast<float2*>(p) = make_float2(a, b);
+#endif
+}
+__device__ __forceinline__ double resid_sub(double lm, double y, double acc) { return fma(-lm, y, acc); }
+__device__ __forceinline__ double2 resid_sub(double lm, double2 y, double2 acc) {
+    return make_double2(fma(-lm, y.x, acc.x), fma(-lm, y.y, acc.y));
+}
+
+// 4 resident CTAs per SM (64 registers): the residual epilogue keeps per-column sums in registers,
+// which spill at the filter steps' 40 (the Ritz values are re-read from L1 per row). T = double
+// (real) or double2 (complex).
+template <class Pol, class T, int W, class IX>
 __global__ void __launch_bounds__(kRmThreads, 4)
-resid_rm_kernel(Pol op, int64_t n, int64_t s, int nseg, int64_t ld, int groups, const double* __restrict__ Y,
-                const double* __restrict__ lam, int res_count, double* __restrict__ part, rc_corr_t* __restrict__ R32,
+resid_rm_kernel(Pol op, int64_t n, int64_t s, int nseg, int64_t ld, int groups, const T* __restrict__ Y,
+                const double* __restrict__ lam, int res_count, double* __restrict__ part, void* __restrict__ Rout,
                 int64_t ldr) {
-    constexpr int V = Pack16<double>::V;  // 2 columns per 16-byte slice
-    extern __shared__ double red[];        // [rows_per_iter][ld]
+    constexpr int V = Pack16<T>::V;  // 2 real or 1 complex column per 16-byte slice
+    using TR = typename std::conditional<IsComplex<T>::value, rc_corr2_t, rc_corr_t>::type;
+    TR* R = reinterpret_cast<TR*>(Rout);
+    extern __shared__ double red[];  // [rows_per_iter][ld]
     const int rows_per_iter = blockDim.x / nseg;
     const int rloc = threadIdx.x / nseg;
     const bool active = rloc < rows_per_iter;
@@ -33,15 +51,8 @@ resid_rm_kernel(Pol op, int64_t n, int64_t s, int nseg, int64_t ld, int groups, 
     const IX wstride = (IX)nseg * (IX)V;
     const IX ldy = (IX)ld;
     double sq[W * V];
-    double lm[W * V];
 #pragma unroll
-    for (int w = 0; w < W; ++w)
-#pragma unroll
-        for (int v = 0; v < V; ++v) {
-            const int64_t c = (int64_t)(off + w * wstride + v);
-            sq[w * V + v] = 0.0;
-            lm[w * V + v] = (active && c < s) ? lam[c] : 0.0;
-        }
+    for (int v = 0; v < W * V; ++v) sq[v] = 0.0;
     if (active) {
         const int64_t stride = rows_per_iter;
         int64_t i = (int64_t)blockIdx.x * groups * rows_per_iter + rloc;
@@ -56,38 +67,37 @@ resid_rm_kernel(Pol op, int64_t n, int64_t s, int nseg, int64_t ld, int groups, 
             typename Pol::Pre p2;
             if (i + stride < i_end) op.fetch2(i + stride, p1);
             if (i + 2 * stride < i_end) op.fetch1(i + 2 * stride, p2);
-            double acc[W * V];
+            T acc[W * V];
 #pragma unroll
-            for (int v = 0; v < W * V; ++v) acc[v] = 0.0;
-            op.row(i, p0, [&](int64_t j, double a) {
-                const double* yj = Y + ((IX)j * ldy + off);
+            for (int v = 0; v < W * V; ++v) acc[v] = s_zero(T());
+            op.row(i, p0, [&](int64_t j, T a) {
+                const T* yj = Y + ((IX)j * ldy + off);
 #pragma unroll
                 for (int w = 0; w < W; ++w) {
-                    const Pack16<double> q = ld16_ro(yj + w * wstride);
+                    const Pack16<T> q = ld16_ro(yj + w * wstride);
 #pragma unroll
-                    for (int v = 0; v < V; ++v) acc[w * V + v] = fma(a, q.v[v], acc[w * V + v]);
+                    for (int v = 0; v < V; ++v) acc[w * V + v] = s_fma(a, q.v[v], acc[w * V + v]);
                 }
             });
 #pragma unroll
             for (int w = 0; w < W; ++w) {
                 const IX o = (IX)i * ldy + off + w * wstride;
-                const Pack16<double> yi = ld16_ro(Y + o);
-                float rv[V];
+                const Pack16<T> yi = ld16_ro(Y + o);
+                float rv[2];
 #pragma unroll
                 for (int v = 0; v < V; ++v) {
                     const int64_t c = (int64_t)(off + w * wstride + v);
-                    const double d = c < s ? fma(-lm[w * V + v], yi.v[v], acc[w * V + v]) : 0.0;
-                    sq[w * V + v] = fma(d, d, sq[w * V + v]);
-                    rv[v] = (float)d;
+                    const T d = c < s ? resid_sub(__ldg(lam + c), yi.v[v], acc[w * V + v]) : s_zero(T());
+                    if constexpr (IsComplex<T>::value) {
+                        sq[w * V + v] = fma(d.y, d.y, fma(d.x, d.x, sq[w * V + v]));
+                        rv[0] = (float)d.x;
+                        rv[1] = (float)d.y;
+                    } else {
+                        sq[w * V + v] = fma(d, d, sq[w * V + v]);
+                        rv[v] = (float)d;
+                    }
                 }
-                if (R32) {
-                    const int64_t c0 = (int64_t)(off + w * wstride);
-#if RC_CORR_BF16
-                    *reinterpret_cast<__nv_bfloat162*>(R32 + i * ldr + c0) = __floats2bfloat162_rn(rv[0], rv[1]);
-#else
-                    *reinterpret_cast<float2*>(R32 + i * ldr + c0) = make_float2(rv[0], rv[1]);
-#endif
-                }
+                if (R) corr_store2(R + i * ldr + (int64_t)(off + w * wstride), rv[0], rv[1]);
             }
             p0 = p1;
             p1 = p2;
@@ -120,14 +130,15 @@ __global__ void resid_norm_reduce_kernel(int64_t nparts, int res_count, const do
 }
 
 bool resid_supported(const rc_op* op, int64_t s) {
-    return op->dtype == RC_REAL64 && s >= 1 && s <= 96 &&
-           (op->kind == 0 || (op->kind == 1 && (op->skind == 5 || op->skind == 7 || op->skind == 27)));
+    if (s < 1 || s > kCorrMaxCols || op->kind == 2) return false;
+    if (op->dtype == RC_REAL64) return op->kind == 0 || op->skind == 5 || op->skind == 7 || op->skind == 27;
+    return op->dtype == RC_COMPLEX128 && (op->kind == 0 || op->skind == 5 || op->skind == 7);
 }
 
-template <class Pol, int W, class IX>
-static rc_status resid_launch(rc_ctx* ctx, const Pol& pol, int64_t n, int64_t s, const double* Y, int64_t ld,
-                              const double* lam, int64_t res_count, double* res, rc_corr_t* R32, int64_t ldr) {
-    constexpr int V = Pack16<double>::V;
+template <class Pol, class T, int W, class IX>
+static rc_status resid_launch(rc_ctx* ctx, const Pol& pol, int64_t n, int64_t s, const T* Y, int64_t ld,
+                              const double* lam, int64_t res_count, double* res, void* R, int64_t ldr) {
+    constexpr int V = Pack16<T>::V;
     if (ld % (V * W) != 0) return rc_fail(ctx, RC_ERR_INVALID, "residual block: leading dimension not padded");
     const int nseg = (int)(ld / (V * W));
     if (nseg > kRmThreads) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "residual block: block too wide");
@@ -142,8 +153,8 @@ static rc_status resid_launch(rc_ctx* ctx, const Pol& pol, int64_t n, int64_t s,
         part = (double*)pp;
     }
     const size_t smem = res_count > 0 ? (size_t)rows_per_iter * ld * sizeof(double) : 0;
-    resid_rm_kernel<Pol, W, IX><<<(unsigned)grid, kRmThreads, smem, ctx->stream>>>(
-        pol, n, s, nseg, ld, groups, Y, lam, (int)res_count, part, R32, ldr);
+    resid_rm_kernel<Pol, T, W, IX><<<(unsigned)grid, kRmThreads, smem, ctx->stream>>>(
+        pol, n, s, nseg, ld, groups, Y, lam, (int)res_count, part, R, ldr);
     ctx->launches++;
     RC_CU(ctx, cudaGetLastError());
     if (res_count > 0) {
@@ -154,35 +165,89 @@ static rc_status resid_launch(rc_ctx* ctx, const Pol& pol, int64_t n, int64_t s,
     return RC_OK;
 }
 
-template <class Pol, int W>
-static rc_status resid_ix(rc_ctx* ctx, const Pol& pol, int64_t n, int64_t s, const double* Y, int64_t ld,
-                          const double* lam, int64_t res_count, double* res, rc_corr_t* R32, int64_t ldr) {
-    if ((n + 1) * std::max(ld, ldr) < ((int64_t)1 << 32))
-        return resid_launch<Pol, W, uint32_t>(ctx, pol, n, s, Y, ld, lam, res_count, res, R32, ldr);
-    return resid_launch<Pol, W, int64_t>(ctx, pol, n, s, Y, ld, lam, res_count, res, R32, ldr);
+// Slices per thread: the measured choices for real blocks of up to 96 columns (two for CSR, one for
+// stencils); otherwise the count (1 or 2 real, up to 4 complex: more spill) that leaves the fewest
+// of a CTA's threads idle.
+template <class T>
+static int resid_slices(int64_t ld, int64_t s, bool csr) {
+    constexpr int V = Pack16<T>::V;
+    if (!IsComplex<T>::value && s <= 96) return csr ? 2 : 1;
+    int best = 0, best_idle = kRmThreads + 1;
+    for (int w = 1; w <= (IsComplex<T>::value ? 4 : 2); ++w) {
+        if (ld % (V * w) != 0 || ld / (V * w) > kRmThreads) continue;
+        const int idle = kRmThreads % (int)(ld / (V * w));
+        if (idle < best_idle) {
+            best = w;
+            best_idle = idle;
+        }
+    }
+    return best;
 }
 
-rc_status resid_block(rc_ctx* ctx, const rc_op* op, const double* Yrm, int64_t ld, int64_t s, const double* lam,
-                      int64_t res_count, double* res, rc_corr_t* R32, int64_t ldr) {
-    if (!resid_supported(op, s)) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "residual block: unsupported operator");
-    if (res_count < 0 || res_count > s || ld != rm_leading_dim(RC_REAL64, P64, s) ||
-        (R32 && ldr != rm_leading_dim(RC_REAL64, P32, s)))
-        return rc_fail(ctx, RC_ERR_INVALID, "residual block: bad sizes");
+template <class Pol, class T>
+static rc_status resid_ix(rc_ctx* ctx, const Pol& pol, int64_t n, int64_t s, const T* Y, int64_t ld,
+                          const double* lam, int64_t res_count, double* res, void* R, int64_t ldr) {
+    const int w = resid_slices<T>(ld, s, Pol::kIsCsr);
+    const bool small = (n + 1) * std::max(ld, ldr) < ((int64_t)1 << 32);
+    switch (w) {
+        case 1:
+            return small ? resid_launch<Pol, T, 1, uint32_t>(ctx, pol, n, s, Y, ld, lam, res_count, res, R, ldr)
+                         : resid_launch<Pol, T, 1, int64_t>(ctx, pol, n, s, Y, ld, lam, res_count, res, R, ldr);
+        case 2:
+            return small ? resid_launch<Pol, T, 2, uint32_t>(ctx, pol, n, s, Y, ld, lam, res_count, res, R, ldr)
+                         : resid_launch<Pol, T, 2, int64_t>(ctx, pol, n, s, Y, ld, lam, res_count, res, R, ldr);
+        default:
+            break;
+    }
+    if constexpr (IsComplex<T>::value) {
+        switch (w) {
+            case 3:
+                return small ? resid_launch<Pol, T, 3, uint32_t>(ctx, pol, n, s, Y, ld, lam, res_count, res, R, ldr)
+                             : resid_launch<Pol, T, 3, int64_t>(ctx, pol, n, s, Y, ld, lam, res_count, res, R, ldr);
+            case 4:
+                return small ? resid_launch<Pol, T, 4, uint32_t>(ctx, pol, n, s, Y, ld, lam, res_count, res, R, ldr)
+                             : resid_launch<Pol, T, 4, int64_t>(ctx, pol, n, s, Y, ld, lam, res_count, res, R, ldr);
+            default:
+                break;
+        }
+    }
+    return rc_fail(ctx, RC_ERR_UNSUPPORTED, "residual block: block too wide");
+}
+
+template <class T>
+static rc_status resid_dispatch(rc_ctx* ctx, const rc_op* op, const T* Y, int64_t ld, int64_t s, const double* lam,
+                                int64_t res_count, double* res, void* R, int64_t ldr) {
     const int64_t n = op->n;
     if (op->kind == 0) {
-        CsrRows<double, double> pol{op->rowptr, op->colind, (const double*)op->vals64};
-        return resid_ix<CsrRows<double, double>, 2>(ctx, pol, n, s, Yrm, ld, lam, res_count, res, R32, ldr);
+        CsrRows<T, T> pol{op->rowptr, op->colind, (const T*)op->vals64};
+        return resid_ix<CsrRows<T, T>, T>(ctx, pol, n, s, Y, ld, lam, res_count, res, R, ldr);
     }
-    if (op->skind == 27) {
-        StencilRows<double, double, 27> pol{op->nx, op->ny, op->nz, op->diag64, op->offdiag, 0.0};
-        return resid_ix<StencilRows<double, double, 27>, 1>(ctx, pol, n, s, Yrm, ld, lam, res_count, res, R32, ldr);
+    const double theta = 2.0 * 3.14159265358979323846 * op->flux;
+    if constexpr (!IsComplex<T>::value) {
+        if (op->skind == 27) {
+            StencilRows<double, T, 27> pol{op->nx, op->ny, op->nz, op->diag64, op->offdiag, theta};
+            return resid_ix<StencilRows<double, T, 27>, T>(ctx, pol, n, s, Y, ld, lam, res_count, res, R, ldr);
+        }
     }
     if (op->skind == 7) {
-        StencilRows<double, double, 7> pol{op->nx, op->ny, op->nz, op->diag64, op->offdiag, 0.0};
-        return resid_ix<StencilRows<double, double, 7>, 1>(ctx, pol, n, s, Yrm, ld, lam, res_count, res, R32, ldr);
+        StencilRows<double, T, 7> pol{op->nx, op->ny, op->nz, op->diag64, op->offdiag, theta};
+        pol.ph = (const T*)op->phase64;
+        return resid_ix<StencilRows<double, T, 7>, T>(ctx, pol, n, s, Y, ld, lam, res_count, res, R, ldr);
     }
-    StencilRows<double, double, 5> pol{op->nx, op->ny, op->nz, op->diag64, op->offdiag, 0.0};
-    return resid_ix<StencilRows<double, double, 5>, 1>(ctx, pol, n, s, Yrm, ld, lam, res_count, res, R32, ldr);
+    StencilRows<double, T, 5> pol{op->nx, op->ny, op->nz, op->diag64, op->offdiag, theta};
+    pol.ph = (const T*)op->phase64;
+    return resid_ix<StencilRows<double, T, 5>, T>(ctx, pol, n, s, Y, ld, lam, res_count, res, R, ldr);
+}
+
+rc_status resid_block(rc_ctx* ctx, const rc_op* op, const void* Yrm, int64_t ld, int64_t s, const double* lam,
+                      int64_t res_count, double* res, void* R, int64_t ldr) {
+    if (!resid_supported(op, s)) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "residual block: unsupported operator");
+    if (res_count < 0 || res_count > s || ld != rm_leading_dim(op->dtype, P64, s) ||
+        (R && ldr != corr_leading_dim(op->dtype, s)))
+        return rc_fail(ctx, RC_ERR_INVALID, "residual block: bad sizes");
+    if (op->dtype == RC_COMPLEX128)
+        return resid_dispatch<double2>(ctx, op, (const double2*)Yrm, ld, s, lam, res_count, res, R, ldr);
+    return resid_dispatch<double>(ctx, op, (const double*)Yrm, ld, s, lam, res_count, res, R, ldr);
 }
 
 }  // namespace rcb

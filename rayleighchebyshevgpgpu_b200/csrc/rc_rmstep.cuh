@@ -40,8 +40,9 @@ __device__ __forceinline__ void st16(TS* p, const Pack16<TS>& v) {
 }
 
 // A 16-byte slice of a block stored as TM, unpacked to the storage type TS of the step arithmetic:
-// TM == TS (16/sizeof(TS) values), or TM bfloat16 with TS float (8 values; the correction
-// filter's bfloat16 blocks), rounded to nearest even on store.
+// TM == TS (16/sizeof(TS) values), TM bfloat16 with TS float (8 values; the correction filter's
+// real blocks) or TM a bfloat16 pair with TS float2 (4 complex values, real and imaginary part
+// each a bfloat16; its complex blocks), rounded to nearest even on store.
 template <class TS, class TM = TS>
 struct Slice {
     static constexpr int V = 16 / sizeof(TM);
@@ -60,6 +61,12 @@ __device__ __forceinline__ Slice<TS, TM> slice_from(const uint4& u) {
     Slice<TS, TM> r;
     if constexpr (std::is_same<TM, TS>::value) {
         memcpy(&r, &u, 16);
+    } else if constexpr (std::is_same<TM, __nv_bfloat162>::value) {
+        static_assert(std::is_same<TS, float2>::value, "complex bfloat16 blocks feed c64 steps");
+        r.v[0] = make_float2(bf_lo(u.x), bf_hi(u.x));
+        r.v[1] = make_float2(bf_lo(u.y), bf_hi(u.y));
+        r.v[2] = make_float2(bf_lo(u.z), bf_hi(u.z));
+        r.v[3] = make_float2(bf_lo(u.w), bf_hi(u.w));
     } else {
         static_assert(std::is_same<TS, float>::value && std::is_same<TM, __nv_bfloat16>::value,
                       "bfloat16 blocks feed FP32 steps");
@@ -87,6 +94,11 @@ __device__ __forceinline__ void stv(TM* p, const Slice<TS, TM>& v) {
     uint4 u;
     if constexpr (std::is_same<TM, TS>::value) {
         memcpy(&u, &v, 16);
+    } else if constexpr (std::is_same<TM, __nv_bfloat162>::value) {
+        u.x = bf2_pack(v.v[0].x, v.v[0].y);
+        u.y = bf2_pack(v.v[1].x, v.v[1].y);
+        u.z = bf2_pack(v.v[2].x, v.v[2].y);
+        u.w = bf2_pack(v.v[3].x, v.v[3].y);
     } else {
         u.x = bf2_pack(v.v[0], v.v[1]);
         u.y = bf2_pack(v.v[2], v.v[3]);
@@ -119,6 +131,8 @@ __device__ __forceinline__ void fmul2(float a0, float a1, float x0, float x1, fl
 
 __device__ __forceinline__ float elem_f(float v) { return v; }
 __device__ __forceinline__ float elem_f(__nv_bfloat16 v) { return __bfloat162float(v); }
+__device__ __forceinline__ float2 elem_f(float2 v) { return v; }
+__device__ __forceinline__ float2 elem_f(__nv_bfloat162 v) { return __bfloat1622float2(v); }
 
 constexpr int kRmThreads = 256;
 // Resident CTAs per SM the register budget must allow: 8 (32 registers) for FP32 storage, 6 (40
@@ -187,9 +201,12 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
     const IX wstride = (IX)nseg * (IX)V;
     const IX ldx = (IX)ld;
     const int64_t stride = rows_per_iter;
-    // source coefficients: held in registers, or (bfloat16 blocks, 8 columns per thread, where
-    // registers bound the resident CTAs) re-read from L1 per row
-    constexpr bool kSigReg = sizeof(TM) != 2;
+    // source coefficients: held in registers, or (bfloat16 blocks, 8 columns per thread, and complex
+    // blocks, where registers bound the resident CTAs) re-read from L1 per row
+    constexpr bool kSigReg = sizeof(TM) != 2 && !IsComplex<TC>::value;
+    // complex FP32 steps of the correction filter: every coefficient is real, so the epilogue
+    // works on (re, im) pairs with real scalars (ffma2, fmul2)
+    constexpr bool kCplxSrc = SRC && std::is_same<TC, float2>::value;
     // bfloat16 blocks (TS = TC = float): the FP32 arithmetic in packed pairs (ffma2, fmul2)
     constexpr bool kPacked = sizeof(TM) == 2;
     TC sg[SRC && kSigReg ? W * V : 1];
@@ -258,6 +275,19 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
                     ffma2(sg2.x, sg2.y, si.v[v], si.v[v + 1], r0, r1);
                     out.v[v] = r0;
                     out.v[v + 1] = r1;
+                }
+            } else if constexpr (kCplxSrc) {
+                const Slice<TS, TM> si = ldv_ro<TS, TM>(src + o);
+                const Slice<TS, TM> zi = z ? ldv<TS, TM>(z + o) : Slice<TS, TM>{};
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    const float sgv = __ldg(sig + off + w * wstride + v);
+                    float r0, r1;
+                    fmul2(alpha.x, alpha.x, acc[w * V + v].x, acc[w * V + v].y, r0, r1);
+                    ffma2(beta.x, beta.x, xi.v[v].x, xi.v[v].y, r0, r1);
+                    if (z) ffma2(gamma.x, gamma.x, zi.v[v].x, zi.v[v].y, r0, r1);
+                    ffma2(sgv, sgv, si.v[v].x, si.v[v].y, r0, r1);
+                    out.v[v] = make_float2(r0, r1);
                 }
             } else if (SRC) {
                 const Slice<TS, TM> si = ldv_ro<TS, TM>(src + o);
@@ -455,24 +485,33 @@ __device__ __forceinline__ void to_cm_tile(int64_t n, int64_t s, const TS* __res
 }
 
 // Last step of the correction filter: V[i + c*ldv] = coef[c] * V[i + c*ldv] + beta * E[i*ld + c]
-// (x_m = c_m(lambda_c) v_c + a e_m, scaled by 1/(m+1)); one 32x32 tile, threads 32 x 8.
+// (x_m = c_m(lambda_c) v_c + a e_m, scaled by 1/(m+1)); one 32x32 tile, threads 32 x 8. Real
+// blocks (TM bfloat16 or float, V double) or complex ones (TM a bfloat16 pair or float2, V double2;
+// real and imaginary parts each formed as in the real case).
 template <class TM>
+using CorrTile = decltype(elem_f(TM()));
+__device__ __forceinline__ double corr_fma(double c, double v, double b, float e) { return fma(c, v, b * (double)e); }
+__device__ __forceinline__ double2 corr_fma(double c, double2 v, double b, float2 e) {
+    return make_double2(fma(c, v.x, b * (double)e.x), fma(c, v.y, b * (double)e.y));
+}
+template <class TM, class TV>
 __device__ __forceinline__ void corr_to_cm_tile(int64_t n, int64_t s, const TM* __restrict__ E, int64_t ld,
-                                                double* __restrict__ Vc, int64_t ldv, const double* __restrict__ coef,
-                                                double beta, int64_t r0, int64_t c0, float (&tile)[32][33]) {
+                                                TV* __restrict__ Vc, int64_t ldv, const double* __restrict__ coef,
+                                                double beta, int64_t r0, int64_t c0, CorrTile<TM> (&tile)[32][33]) {
     const int tx = threadIdx.x, ty = threadIdx.y;
+    using TT = CorrTile<TM>;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         const int64_t r = r0 + ty + 8 * j, c = c0 + tx;
-        tile[ty + 8 * j][tx] = (r < n && c < s) ? elem_f(E[r * ld + c]) : 0.0f;
+        tile[ty + 8 * j][tx] = (r < n && c < s) ? elem_f(E[r * ld + c]) : s_zero(TT());
     }
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
         const int64_t c = c0 + ty + 8 * j, r = r0 + tx;
         if (r < n && c < s) {
-            double* vp = Vc + r + c * ldv;
-            *vp = fma(coef[c], *vp, beta * (double)tile[tx][ty + 8 * j]);
+            TV* vp = Vc + r + c * ldv;
+            *vp = corr_fma(coef[c], *vp, beta, tile[tx][ty + 8 * j]);
         }
     }
 }

@@ -154,12 +154,13 @@ int64_t solve_footprint(const rc_op* op, const rc_solve_params& p, int sm_count)
     t += round_2m(4 * sq * sq * esz + 1024) + round_2m(2 * (sq + 1) * (sq + 1) * esz + 4096);  // cholqr, Jacobi
     if (op->kind == 2) t += round_2m(n * ss * esz);                   // callback step scratch
     if (rcb::resid_supported(op, ss))                                 // row-major copy of the Ritz vectors
-        t += round_2m(n * rcb::rm_leading_dim(op->dtype, P64, ss) * 8);
+        t += round_2m(n * rcb::rm_leading_dim(op->dtype, P64, ss) * esz);
     if (p.precision == RC_PREC_MIXED && p.mixed_refine == 0 && rcb::rm_corr_supported(op, ss)) {
-        // correction filter: the residual block (rc_corr_t) and the coefficient table
-        const int64_t ld32 = rcb::rm_leading_dim(op->dtype, P32, ss);
+        // correction filter: the residual block (rc_corr_t / rc_corr2_t) and the coefficient table
+        const int64_t ld32 = rcb::corr_leading_dim(op->dtype, ss);
         const int64_t dmax = p.poly_degree_max > 0 ? p.poly_degree_max : 200;
-        t += round_2m(n * ld32 * (int64_t)sizeof(rc_corr_t)) + round_2m((dmax + 1) * ld32 * 4 + ld32 * 8 + 512);
+        t += round_2m(n * ld32 * (int64_t)rcb::corr_elem_bytes(op->dtype)) +
+             round_2m((dmax + 1) * ld32 * 4 + ld32 * 8 + 512);
     }
     return t;
 }

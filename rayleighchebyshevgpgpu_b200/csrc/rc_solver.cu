@@ -15,10 +15,10 @@
 //   * Ritz vectors V*Q are not renormalised (V and Q are orthonormal);
 //   * after an outer pass only the stale tail columns are refreshed (the CPU LM refreshes the
 //     buffer range, RayleighChebyshevLM.h:1086-1092; the GPU reference the whole block, :1176-1179);
-//   * MIXED precision: the first filter application runs in FP32 (there is no residual block
-//     yet), then the correction filter (bfloat16 storage, FP32 arithmetic) on the residual block
-//     of the Ritz vectors (rc_filter_rm.cu), which converges like the FP64 filter. Operators
-//     without it run the FP32/c64 filter until the residuals reach mixed_switch_tol (1e-6) or
+//   * MIXED precision: the first filter application runs in FP32 / c64 (there is no residual
+//     block yet), then the correction filter (bfloat16 storage, FP32 / c64 arithmetic) on the
+//     residual block of the Ritz vectors (rc_filter_rm.cu), which converges like the FP64 filter.
+//     Operators without it (callback operators, blocks wider than kCorrMaxCols) run the FP32/c64 filter until the residuals reach mixed_switch_tol (1e-6) or
 //     stall (never stopping in that phase), then the FP64 filter; a set mixed_switch_tol also
 //     delays the correction filter to that residual. The FP64 filter also takes over when the
 //     correction filter stalls.
@@ -64,10 +64,10 @@ private:
     rc_status randomize_cols(void* X, int64_t c0, int64_t c1);
     rc_status deflate(void* X, int64_t s);
     rc_status ortho(int64_t s);
-    rc_status rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool read_back, rc_corr_t* R32 = nullptr);
-    rc_status rr_fused(int64_t s, int64_t res_count, bool* ok, rc_corr_t* R32 = nullptr);
-    rc_status r32_block(int64_t s, rc_corr_t** out);
-    rc_status ritz_and_residuals(XtArgs a, int64_t s, int64_t res_count, rc_corr_t* R32);
+    rc_status rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool read_back, void* R32 = nullptr);
+    rc_status rr_fused(int64_t s, int64_t res_count, bool* ok, void* R32 = nullptr);
+    rc_status r32_block(int64_t s, void** out);
+    rc_status ritz_and_residuals(XtArgs a, int64_t s, int64_t res_count, void* R32);
     rc_status lanczos(int which, double tol, double* lmin, double* lmax);
     void tic(int ph);
     void toc(int ph);
@@ -92,7 +92,8 @@ private:
     int64_t fused_ok_ = 0, fused_fallback_ = 0;
     double* hbuf_ = nullptr;
     int64_t ss_cap_ = 0;
-    // MIXED correction filter: the residual block of the current Ritz vectors (row-major rc_corr_t),
+    // MIXED correction filter: the residual block of the current Ritz vectors (row-major, in the
+    // correction filter's storage: rc_corr_t, or rc_corr2_t for complex operators),
     // valid while haveR_ (written by the last Rayleigh-Ritz step, consumed by the next filter)
     bool haveR_ = false;
     bool rWritten_ = false;  // set by ritz_and_residuals when it wrote the residual block
@@ -227,25 +228,32 @@ rc_status Solver::ortho(int64_t s) {
 // Rayleigh-Ritz on orthonormal X (n x s): AX = A X, H = X^H AX, H = Q L Q^H,
 // X <- X Q, AX <- AX Q, residuals of the first res_count columns; results read to the host.
 // Ritz vectors Y = X Q (a.Y) and the residuals of their first res_count columns (dres_), plus
-// the FP32 residual block when R32 is given. Native real operators with s <= 96: Y by the GEMM,
-// which also writes a row-major copy, then R = A Y - Y diag(lam) in one pass over that copy
-// (rc_resid.cu). Otherwise (complex or callback operators, wider blocks): the dual GEMM (A X) Q
+// the correction filter's residual block when R32 is given. Native operators (real, or complex CSR
+// and 5/7-point stencils) with s <= kCorrMaxCols: Y by the GEMM and a row-major FP64 (c128) copy of
+// it (written by the real GEMM itself for s <= 96, else by a layout change), then
+// R = A Y - Y diag(lam) in one pass over that copy (rc_resid.cu): a sparse product costs less than
+// the second dense product W Q. Otherwise (callback operators, wider blocks): the dual GEMM (A X) Q
 // with the residual norms reduced on the fly.
-rc_status Solver::ritz_and_residuals(XtArgs a, int64_t s, int64_t res_count, rc_corr_t* R32) {
+rc_status Solver::ritz_and_residuals(XtArgs a, int64_t s, int64_t res_count, void* R32) {
     rWritten_ = false;
-    if (resid_supported(op_, s) && xt2_supported(dtype_, a.k, a.nc)) {
-        const int64_t ldrm = rm_leading_dim(RC_REAL64, P64, s);
+    if (resid_supported(op_, s)) {
+        const int64_t ldrm = rm_leading_dim(dtype_, P64, s);
         void* yrm = nullptr;
-        RC_TRY(rc_slot(ctx_, S_YRM, (size_t)n_ * ldrm * sizeof(double), &yrm));
+        RC_TRY(rc_slot(ctx_, S_YRM, (size_t)n_ * ldrm * esz_, &yrm));
         a.X2 = nullptr;
         a.Y2 = nullptr;
         a.lam = nullptr;
         a.res_count = 0;
-        a.Yrm = (double*)yrm;
-        a.ldyr = ldrm;
-        RC_TRY(xt(ctx_, dtype_, a));
-        RC_TRY(resid_block(ctx_, op_, (const double*)yrm, ldrm, s, dlam_, res_count, dres_, R32,
-                           R32 ? rm_leading_dim(RC_REAL64, P32, s) : 0));
+        if (dtype_ == RC_REAL64 && xt2_supported(dtype_, a.k, a.nc)) {
+            a.Yrm = (double*)yrm;
+            a.ldyr = ldrm;
+            RC_TRY(xt(ctx_, dtype_, a));
+        } else {
+            RC_TRY(xt(ctx_, dtype_, a));
+            RC_TRY(to_row_major(ctx_, dtype_, n_, s, a.Y, a.ldy, yrm, ldrm));
+        }
+        RC_TRY(resid_block(ctx_, op_, yrm, ldrm, s, dlam_, res_count, dres_, R32,
+                           R32 ? corr_leading_dim(dtype_, s) : 0));
         rWritten_ = R32 != nullptr;
         return RC_OK;
     }
@@ -253,24 +261,14 @@ rc_status Solver::ritz_and_residuals(XtArgs a, int64_t s, int64_t res_count, rc_
     a.lam = dlam_;
     a.res_count = res_count;
     a.res = dres_;
-    if constexpr (std::is_same<rc_corr_t, float>::value) {  // the dual GEMM writes FP32 residual blocks only
-        if (R32) {
-            a.R32 = reinterpret_cast<float*>(R32);
-            a.ldr = rm_leading_dim(RC_REAL64, P32, s);
-            rWritten_ = true;
-        }
-    }
     return xt(ctx_, dtype_, a);
 }
 
-rc_status Solver::r32_block(int64_t s, rc_corr_t** out) {
-    void* p = nullptr;
-    RC_TRY(rc_slot(ctx_, S_R32, (size_t)n_ * rm_leading_dim(RC_REAL64, P32, s) * sizeof(rc_corr_t), &p));
-    *out = (rc_corr_t*)p;
-    return RC_OK;
+rc_status Solver::r32_block(int64_t s, void** out) {
+    return rc_slot(ctx_, S_R32, (size_t)n_ * corr_leading_dim(dtype_, s) * corr_elem_bytes(dtype_), out);
 }
 
-rc_status Solver::rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool read_back, rc_corr_t* R32) {
+rc_status Solver::rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool read_back, void* R32) {
     StepArgs st;
     st.s = s;
     st.x = X; st.xp = P64; st.ldx = n_;
@@ -307,7 +305,7 @@ rc_status Solver::rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool rea
 // problem. Accepted only when the scaled Gram matrix is well conditioned (smallest Cholesky pivot
 // >= 1e-3, no shift needed); otherwise *ok = false, V_ still holds V_f and the caller
 // orthonormalises and repeats the Rayleigh-Ritz step.
-rc_status Solver::rr_fused(int64_t s, int64_t res_count, bool* ok, rc_corr_t* R32) {
+rc_status Solver::rr_fused(int64_t s, int64_t res_count, bool* ok, void* R32) {
     StepArgs st;
     st.s = s;
     st.x = V_; st.xp = P64; st.ldx = n_;
@@ -509,10 +507,10 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
                 if (phase == PH_CORR32 && haveR_) {
                     // the correction filter: V_ holds the Ritz vectors, dlam_ their values and the
                     // R32 slot their residual block; its two work blocks (FP32 or bfloat16) fit in T1_
-                    rc_corr_t* R32 = nullptr;
+                    void* R32 = nullptr;
                     RC_TRY(r32_block(subspaceSize, &R32));
                     const size_t rmb =
-                        (size_t)n_ * rm_leading_dim(RC_REAL64, P32, subspaceSize) * sizeof(rc_corr_t);
+                        (size_t)n_ * corr_leading_dim(dtype_, subspaceSize) * corr_elem_bytes(dtype_);
                     const size_t blk = (size_t)n_ * subspaceSize * esz_;
                     void* bufA = T1_;
                     void* bufB = (char*)T1_ + ((rmb + 255) / 256) * 256;
@@ -529,8 +527,8 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
                             steps += st2;
                             continue;
                         }
-                        RC_TRY(rm_filter_corr(ctx_, op_, (double*)V_, n_, subspaceSize, starDegree, fa, fb, dlam_,
-                                              R32, bufA, bufB));
+                        RC_TRY(rm_filter_corr(ctx_, op_, V_, n_, subspaceSize, starDegree, fa, fb, dlam_, R32, bufA,
+                                              bufB));
                         steps += starDegree;
                         corr_steps_ += starDegree;
                     }
@@ -556,7 +554,7 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
             bool fused = false;
             // the residual block for the next correction filter, once the residuals approach the
             // switch tolerance
-            rc_corr_t* R32 = nullptr;
+            void* R32 = nullptr;
             const double prevResidual = residualHistory.empty() ? 1e300 : residualHistory.back();
             if (corrOk && phase != PH_FP64 && (phase == PH_CORR32 || prevResidual < 1e3 * switchTol))
                 RC_TRY(r32_block(subspaceSize, &R32));
@@ -906,7 +904,7 @@ rc_status Solver::run(const void* v0, double* evals_out, void* evecs_out, double
         r.time_filter_steps_ms = ctx_->step_ms - step_ms0_;
         r.correction_iterations = corr_iters_;
         r.correction_degree_steps = corr_steps_;
-        r.correction_element_bytes = (int64_t)sizeof(rc_corr_t);
+        r.correction_element_bytes = (int64_t)corr_elem_bytes(dtype_);
         std::memcpy(info, &r, std::min(sz, sizeof(r)));
     }
     return RC_OK;

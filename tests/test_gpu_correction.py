@@ -30,17 +30,27 @@ _CASES = {
     "st7": (7, (14, 13, 12)),
     "st27": (27, (12, 11, 10)),
 }
+# complex Hermitian tight-binding operators with Peierls phases on the y-bonds (flux 1/17 and 0.11)
+_CCASES = {
+    "ccsr7": ((13, 12, 11), 1.0 / 17.0),
+    "cst7": ((13, 12, 11), 1.0 / 17.0),
+    "cst5": ((43, 39), 0.11),
+}
 _cache = {}
 
 
 def _problem(name):
     if name not in _cache:
-        kind, dims = _CASES[name]
-        n = int(np.prod(dims))
-        rng = np.random.default_rng(kind * 7 + len(dims))
-        d0 = {5: 4.0, 7: 6.0, 27: 1.0}[kind]
-        diag = d0 + rng.uniform(0.0, 3.0 if kind != 27 else 2.0, n)
-        Q = problems.Problem(name, dims, kind, diag, -1.0 / 26.0 if kind == 27 else -1.0)
+        if name in _CCASES:
+            dims, flux = _CCASES[name]
+            Q = problems.small_laplacian(dims, seed=len(dims) + 40, complex_=True, flux=flux)
+        else:
+            kind, dims = _CASES[name]
+            n = int(np.prod(dims))
+            rng = np.random.default_rng(kind * 7 + len(dims))
+            d0 = {5: 4.0, 7: 6.0, 27: 1.0}[kind]
+            diag = d0 + rng.uniform(0.0, 3.0 if kind != 27 else 2.0, n)
+            Q = problems.Problem(name, dims, kind, diag, -1.0 / 26.0 if kind == 27 else -1.0)
         A = O.csr_matrix(*Q.csr())
         w, U = np.linalg.eigh(A.toarray())
         _cache[name] = (Q, A, w, U)
@@ -48,11 +58,14 @@ def _problem(name):
 
 
 def _ritz_pairs(A, U, s, d, seed):
-    """Ritz pairs of a perturbed invariant subspace: residual about d."""
+    """Ritz pairs of a perturbed invariant subspace: residual about d (complex U: complex noise)."""
     rng = np.random.default_rng(seed)
-    V, _ = np.linalg.qr(U[:, :s] + d * rng.standard_normal((U.shape[0], s)))
-    H = V.T @ (A @ V)
-    lam, Qs = np.linalg.eigh(0.5 * (H + H.T))
+    noise = rng.standard_normal((U.shape[0], s))
+    if np.iscomplexobj(U):
+        noise = noise + 1j * rng.standard_normal((U.shape[0], s))
+    V, _ = np.linalg.qr(U[:, :s] + d * noise)
+    H = V.conj().T @ (A @ V)
+    lam, Qs = np.linalg.eigh(0.5 * (H + H.conj().T))
     Y = V @ Qs
     rn = np.linalg.norm(A @ Y - Y * lam) / np.linalg.norm(Y)
     return Y, lam, rn
@@ -66,7 +79,7 @@ def _coefficients(w, s, m):
 
 
 def _op(ctx, Q, name):
-    return R.operator_from_problem(ctx, Q, "csr" if name.startswith("csr") else "stencil")
+    return R.operator_from_problem(ctx, Q, "csr" if "csr" in name else "stencil")
 
 
 def _gpu(ctx, op, Y, s, lam, m, g1, g2):
@@ -92,6 +105,37 @@ def _check(A, Y, lam, rn, m, g1, g2, got):
 def test_correction_filter_matches_oracle(ctx, name, s):
     Q, A, w, U = _problem(name)
     m = 9
+    Y, lam, rn = _ritz_pairs(A, U, s, 1e-5, seed=s)
+    g1, g2 = _coefficients(w, s, m)
+    op = _op(ctx, Q, name)
+    got = _gpu(ctx, op, Y, s, lam, m, g1, g2)
+    _check(A, Y, lam, rn, m, g1, g2, got)
+    op.close()
+
+
+@pytest.mark.parametrize("name", list(_CCASES))
+@pytest.mark.parametrize("s", [4, 24, 96, 192])
+def test_complex_correction_filter_matches_oracle(ctx, name, s):
+    """Complex Hermitian operators: complex bfloat16 blocks (real and imaginary part each a bfloat16),
+    c64 arithmetic, real Ritz values and coefficients, up to the 192 columns of the 96^3 complex
+    tight-binding workload."""
+    Q, A, w, U = _problem(name)
+    m = 9
+    Y, lam, rn = _ritz_pairs(A, U, s, 1e-5, seed=s + 3)
+    g1, g2 = _coefficients(w, s, m)
+    op = _op(ctx, Q, name)
+    got = _gpu(ctx, op, Y, s, lam, m, g1, g2)
+    _check(A, Y, lam, rn, m, g1, g2, got)
+    op.close()
+
+
+@pytest.mark.parametrize("name", ["csr7", "st7", "st27"])
+@pytest.mark.parametrize("s", [130, 256])
+def test_wide_correction_filter_matches_oracle(ctx, name, s):
+    """Real blocks wider than 96 columns: the row-major FP64 copy of V comes from a layout change
+    and the residual block kernel takes one 16-byte slice per thread or two."""
+    Q, A, w, U = _problem(name)
+    m = 7
     Y, lam, rn = _ritz_pairs(A, U, s, 1e-5, seed=s)
     g1, g2 = _coefficients(w, s, m)
     op = _op(ctx, Q, name)
@@ -129,11 +173,12 @@ def test_correction_error_shrinks_with_the_residual(ctx):
 
 def test_batched_correction_equals_single_block_bitwise(ctx):
     """Two different jobs (CSR s = 24, degree 9; 7-point stencil s = 48, degree 13) in one batched
-    launch per step, plus a 27-point job that runs on the single-block kernels in the same call:
-    every block equals its rc_filter_correction result bit for bit and matches the oracle."""
+    launch per step, plus a 27-point job and a complex job that run on the single-block kernels in
+    the same call: every block equals its rc_filter_correction result bit for bit and matches the
+    oracle."""
     import torch
     jobs, singles, refs = [], [], []
-    for name, s, m, seed in (("csr7", 24, 9, 1), ("st7", 48, 13, 2), ("st27", 16, 7, 3)):
+    for name, s, m, seed in (("csr7", 24, 9, 1), ("st7", 48, 13, 2), ("st27", 16, 7, 3), ("cst7", 20, 8, 4)):
         Q, A, w, U = _problem(name)
         Y, lam, rn = _ritz_pairs(A, U, s, 1e-5, seed=seed)
         g1, g2 = _coefficients(w, s, m)
@@ -152,11 +197,13 @@ def test_batched_correction_equals_single_block_bitwise(ctx):
 
 
 def test_correction_filter_rejects_unsupported(ctx):
+    """Blocks wider than 256 columns are refused (RC_ERR_UNSUPPORTED), before any work."""
     import torch
-    Q = problems.small_laplacian((6, 6, 6), seed=1, complex_=True, flux=0.1)
+    Q = problems.small_laplacian((8, 8, 8), seed=1, complex_=True, flux=0.1)
     op = R.operator_from_problem(ctx, Q, "csr")
-    Vd = torch.zeros((4, Q.n), dtype=torch.complex128, device="cuda")
+    s = 257
+    Vd = torch.zeros((s, Q.n), dtype=torch.complex128, device="cuda")
     with pytest.raises(R.capi.RCError) as e:
-        R.filter_correction(ctx, op, Vd, 4, np.zeros(4), 3, 0.1, 1.0)
+        R.filter_correction(ctx, op, Vd, s, np.zeros(s), 3, 0.1, 1.0)
     assert e.value.status == 8  # RC_ERR_UNSUPPORTED
     op.close()

@@ -147,8 +147,11 @@ def test_cholqr_block_widths(ctx, s):
     assert (np.linalg.norm(resid, axis=0) / np.linalg.norm(V, axis=0)).max() < 1e-10
 
 
-@pytest.mark.parametrize("s,complex_", [(24, False), (96, False), (150, False), (40, True), (130, True), (7, False)])
+@pytest.mark.parametrize("s,complex_", [(24, False), (96, False), (150, False), (40, True), (130, True), (7, False),
+                                        (192, True), (255, True), (256, False)])
 def test_small_eigh_matches_lapack(ctx, s, complex_):
+    """One-CTA Jacobi in shared memory (real s <= 118, complex s <= 82) and the grid form with the
+    working copies in global memory (the wider cases)."""
     rng = np.random.default_rng(s)
     H = rng.standard_normal((s, s))
     if complex_:
@@ -173,6 +176,38 @@ def test_small_eigh_degenerate_cluster(ctx):
     ev, Qm = R.small_eigh(ctx, H)
     np.testing.assert_allclose(ev, np.sort(d), atol=1e-13)
     assert np.abs(Qm.T @ Qm - np.eye(s)).max() < 1e-12
+
+
+@pytest.mark.parametrize("complex_", [False, True])
+def test_grid_jacobi_matches_one_cta_kernel(complex_):
+    """The grid Jacobi (32 CTAs, cooperative launch) and the one-CTA kernel on the same global-memory
+    working copies (RCB200_JACOBI_CTAS=1) apply the same rotations: the eigenvalues agree to
+    rounding and both match LAPACK on a matrix with a degenerate cluster."""
+    s = 160 if complex_ else 200
+    rng = np.random.default_rng(17)
+    X = rng.standard_normal((s, s)) + (1j * rng.standard_normal((s, s)) if complex_ else 0)
+    U, _ = np.linalg.qr(X)
+    d = np.concatenate([np.full(12, 1.0), np.full(12, 1.0 + 1e-13), np.linspace(2, 5, s - 24)])
+    H = (U * d) @ U.conj().T
+    H = 0.5 * (H + H.conj().T)
+    out = []
+    for ctas in ("0", "1"):
+        old = os.environ.get("RCB200_JACOBI_CTAS")
+        os.environ["RCB200_JACOBI_CTAS"] = ctas
+        try:
+            c = R.Context(0)
+        finally:
+            if old is None:
+                os.environ.pop("RCB200_JACOBI_CTAS", None)
+            else:
+                os.environ["RCB200_JACOBI_CTAS"] = old
+        ev, Qm = R.small_eigh(c, H)
+        c.close()
+        np.testing.assert_allclose(ev, np.sort(d), atol=1e-13)
+        assert np.abs(Qm.conj().T @ Qm - np.eye(s)).max() < 1e-12
+        assert np.abs(H @ Qm - Qm * ev).max() < 1e-12 * s
+        out.append(ev)
+    np.testing.assert_allclose(out[0], out[1], atol=1e-14)
 
 
 def test_rayleigh_ritz_matches_dense(ctx):

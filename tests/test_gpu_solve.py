@@ -94,6 +94,38 @@ def test_mixed_correction_filter_matches_fp64(ctx, kind, dims, k):
         op.close()
 
 
+@pytest.mark.parametrize("case", ["complex7", "complex5", "wide5"])
+def test_mixed_correction_filter_complex_and_wide_blocks(ctx, case):
+    """The correction filter on complex Hermitian operators (complex bfloat16 blocks, c64 arithmetic)
+    and on real blocks wider than 96 columns (k = 96, s = 144): no FP64 degree step, the FP64 path's
+    eigenvalues and dense LAPACK's (zheevr / dsyevr)."""
+    if case == "complex7":
+        Q = problems.small_laplacian((12, 11, 10), seed=21, complex_=True, flux=1.0 / 17.0)
+        k, tol = 32, 1e-9
+    elif case == "complex5":
+        Q = problems.small_laplacian((48, 44), seed=22, complex_=True, flux=0.11)
+        k, tol = 24, 1e-9
+    else:
+        Q = problems.small_laplacian((60, 50), seed=23, vmax=3.0)
+        k, tol = 96, 1e-10
+    A = O.csr_matrix(*Q.csr())
+    dense = O.dense_lowest(A, k)
+    incr, buf = problems.block_sizes(k)
+    start = Q.start_block(incr + buf)
+    for form in ("csr", "stencil"):
+        op = R.operator_from_problem(ctx, Q, form)
+        f64 = _solve(ctx, op, Q, k, tol, "fp64", start=start, incr=incr, buffer=buf)
+        mix = _solve(ctx, op, Q, k, tol, "mixed", start=start, incr=incr, buffer=buf)
+        assert mix.info["correction_iterations"] > 0, mix.info
+        assert mix.info["fp64_degree_steps"] == 0, mix.info
+        np.testing.assert_allclose(mix.evals, f64.evals, rtol=tol)
+        np.testing.assert_allclose(mix.evals, dense, rtol=tol, atol=1e-13)
+        X = mix.evecs.T
+        r = np.linalg.norm(A @ X - X * mix.evals, axis=0) / np.maximum(np.abs(mix.evals), 0.1)
+        assert r.max() <= 1.5 * tol, r.max()
+        op.close()
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_multipass_deflation_incr_smaller_than_k(ctx, precision):
     Q = problems.small_laplacian((24, 24), seed=5)
