@@ -91,6 +91,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-count", type=int, default=64,
                     help="requests of the configuration-4 serving stream run after the timed solves (0: skip)")
+    ap.add_argument("--other-configs", default="3,5",
+                    help="configurations solved once each in mixed precision and in FP64 after the headline, "
+                         "reported under other_workloads (empty: skip)")
     return ap.parse_args()
 
 
@@ -526,6 +529,15 @@ def run_ours(args):
         "gpu_launches": int(launches),
         "clocks": clk,
     }
+    # ---- configurations 3 and 5, one mixed and one FP64 solve each, N = 1 only ----
+    if world == 1 and args.other_configs:
+        others = {}
+        for c in [int(x) for x in args.other_configs.split(",") if x.strip()]:
+            try:
+                others[f"config{c}"] = other_workload(c, ctx, stream)
+            except Exception as e:  # reported, never required for the headline
+                others[f"config{c}"] = {"unavailable": str(e)}
+        line["other_workloads"] = others
     # ---- serving (configuration 4, the first --serve-count requests of the stream), N = 1 only ----
     if world == 1 and args.serve_count > 0:
         from rayleighchebyshevgpgpu_b200 import serve_bench
@@ -545,6 +557,67 @@ def run_ours(args):
     ctx.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+OTHER_NAMES = {
+    3: "config3: 3D tight-binding 96^3, Peierls flux 1/17 on y-bonds, U[-1,1) potential, complex Hermitian "
+       "7-point stencil, lowest 128 eigenpairs, tol 1e-9 RESIDUAL_ONLY",
+    5: "config5: 3D 27-point stencil 256^3, off-diagonal -1/26, diagonal 1 + U[0,2) potential, lowest 32 "
+       "eigenpairs, tol 1e-10 RESIDUAL_ONLY",
+}
+
+
+def other_workload(config: int, ctx, stream) -> dict:
+    """One configuration beside the headline: a warm-up solve, then one mixed and one FP64 solve from
+    the same start block (CUDA events on the solver stream), the eigenvalues of the two compared, and
+    every residual recomputed with the stencil written out in plain torch (verify.stencil_residuals)."""
+    import torch
+
+    from rayleighchebyshevgpgpu_b200 import problems
+    from rayleighchebyshevgpgpu_b200 import runtime as R
+    from rayleighchebyshevgpgpu_b200.verify import stencil_residuals
+
+    P = problems.config3() if config == 3 else problems.config5()
+    incr, buf = problems.block_sizes(P.k)
+    s = incr + buf
+    op = R.operator_from_problem(ctx, P, "stencil")
+    v0 = torch.from_numpy(P.start_block(s)).cuda()
+    evecs = torch.empty((P.k, P.n), dtype=v0.dtype, device="cuda")
+
+    def run(prec, iters=0):
+        p = R.make_params(P.k, P.tol, incr=incr, buffer=buf, precision=prec, stop="RESIDUAL_ONLY", phase_timing=1)
+        p.v0_cols = s
+        if iters:
+            p.max_inner_loop = iters
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        res = R.solve(ctx, op, p, v0=v0, host=False, evecs_out=evecs)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return res, e0.elapsed_time(e1)
+
+    run("mixed", iters=4)  # warm-up: operator copies, scratch slots, kernel modules
+    out = {"workload": OTHER_NAMES[config], "n": P.n, "k": P.k, "subspace": s, "operator_form": "stencil",
+           "start_block": f"N(0,1) seed {P.start_seed}"}
+    solves = {}
+    for prec in ("mixed", "fp64"):
+        res, ms = run(prec)
+        rel = stencil_residuals(P, evecs[:P.k], res.evals)
+        info = res.info
+        solves[prec] = (res, ms)
+        out[prec] = {"tts_ms": ms, "eigenpairs_per_s": P.k / (ms * 1e-3), "found": int(info["found"]),
+                     "max_rel_residual_independent": float(rel.max()),
+                     "solve_info": {k: info[k] for k in ("inner_iterations", "degree_steps", "fp64_degree_steps",
+                                                         "correction_iterations", "time_filter_ms",
+                                                         "time_eigenvalue_ms", "time_ortho_ms", "time_lanczos_ms")}}
+    (rm, tm), (r64, t64) = solves["mixed"], solves["fp64"]
+    out["speedup_mixed_vs_fp64"] = t64 / tm
+    out["max_rel_eig_diff_mixed_vs_fp64"] = float(np.max(np.abs(rm.evals - r64.evals) / np.abs(r64.evals)))
+    del v0, evecs
+    op.close()
+    torch.cuda.empty_cache()
+    return out
 
 
 def main():

@@ -292,6 +292,29 @@ corr_to_cm_kernel(int64_t n, int64_t s, const TM* __restrict__ E, int64_t ld, TV
 }
 
 
+// The same combination into a row-major FP64 block: Vf[i*ldf + c] = coef[c] * Yrm[i*ldy + c] +
+// beta * E[i*lde + c] for c < s (zero in the padding columns s..ldf), with Yrm the row-major copy of
+// V (the values corr_to_cm_kernel forms, with the same arithmetic). Real blocks; one 16-byte pair of
+// columns per thread, grid-stride, coalesced on every block.
+template <class TM>
+__global__ void __launch_bounds__(256)
+corr_to_rm_kernel(int64_t n, int64_t s, const double* __restrict__ Yrm, int64_t ldy, const TM* __restrict__ E,
+                  int64_t lde, double* __restrict__ Vf, int64_t ldf, const double* __restrict__ coef, double beta) {
+    const int64_t pairs = ldf / 2;
+    const int64_t total = n * pairs;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = e / pairs, c = 2 * (e - i * pairs);
+        double2 out = make_double2(0.0, 0.0);
+        if (c < s) {
+            const double2 y = *reinterpret_cast<const double2*>(Yrm + i * ldy + c);
+            const float e0 = elem_f(E[i * lde + c]);
+            out.x = fma(coef[c], y.x, beta * (double)e0);
+            if (c + 1 < s) out.y = fma(coef[c + 1], y.y, beta * (double)elem_f(E[i * lde + c + 1]));
+        }
+        *reinterpret_cast<double2*>(Vf + i * ldf + c) = out;
+    }
+}
+
 template <class TV, class TS>
 __global__ void __launch_bounds__(256)
 to_rm_kernel(int64_t n, int64_t s, const TV* __restrict__ Vc, int64_t ldv, TS* __restrict__ Rr, int64_t ld) {
@@ -365,10 +388,19 @@ static rc_status run_rm_filter(rc_ctx* ctx, const Pol& pol, int64_t n, void* V, 
 // of the residual), so its rounding perturbs the filtered block by the storage rounding times the
 // residual instead of times the block: the subspace keeps converging past the FP32 floor of the
 // plain FP32 filter. e_2 -> A, e_3 -> B (e_1 = R is read as x_{k-2}), then e_k over e_{k-2}.
+// Where a correction-filter application leaves its result: V (column-major), or, with vf set, the
+// row-major FP64 block vf formed from the row-major copy yrm of V.
+struct CorrRmOut {
+    const double* yrm = nullptr;
+    int64_t ldy = 0;
+    double* vf = nullptr;
+    int64_t ldf = 0;
+};
+
 template <class Pol, class TS, class TC, int W, class IX, class TM, class TV>
 static rc_status run_rm_corr(rc_ctx* ctx, const Pol& pol, int64_t n, TV* V, int64_t ldv, int64_t s,
                              int64_t degree, double a, double b, const TM* R, const float* sig, const double* coef,
-                             TM* A, TM* B, int64_t ld, int64_t band, const StageOffsets* so) {
+                             TM* A, TM* B, int64_t ld, int64_t band, const StageOffsets* so, const CorrRmOut& ro) {
     const int64_t pf_z = ctx->pf_rows;
     const int64_t pf_x = pf_z > 0 ? pf_z + band : 0;
     constexpr int VEC = Slice<TS, TM>::V;  // 8 values per 16-byte slice for bfloat16 blocks
@@ -389,9 +421,20 @@ static rc_status run_rm_corr(rc_ctx* ctx, const Pol& pol, int64_t n, TV* V, int6
     RC_CU(ctx, cudaGetLastError());
     step_mark(ctx);
     const TM* em = degree == 1 ? R : (degree % 2 == 0 ? A : B);
-    const dim3 tgrid((unsigned)((n + 31) / 32), (unsigned)((s + 31) / 32)), tblk(32, 8);
-    corr_to_cm_kernel<TM, TV><<<tgrid, tblk, 0, ctx->stream>>>(n, s, em, ld, V, ldv, coef,
-                                                               a / (double)(degree + 1));
+    if (ro.vf) {
+        if constexpr (IsComplex<TC>::value) {
+            return rc_fail(ctx, RC_ERR_UNSUPPORTED, "correction filter: row-major result for real blocks only");
+        } else {
+            const int64_t total = n * (ro.ldf / 2);
+            const unsigned grid = (unsigned)std::min<int64_t>((total + 255) / 256, (int64_t)ctx->sm_count * 16);
+            corr_to_rm_kernel<TM><<<grid, 256, 0, ctx->stream>>>(n, s, ro.yrm, ro.ldy, em, ld, ro.vf, ro.ldf, coef,
+                                                                 a / (double)(degree + 1));
+        }
+    } else {
+        const dim3 tgrid((unsigned)((n + 31) / 32), (unsigned)((s + 31) / 32)), tblk(32, 8);
+        corr_to_cm_kernel<TM, TV><<<tgrid, tblk, 0, ctx->stream>>>(n, s, em, ld, V, ldv, coef,
+                                                                   a / (double)(degree + 1));
+    }
     ctx->launches++;
     RC_CU(ctx, cudaGetLastError());
     return RC_OK;
@@ -458,12 +501,12 @@ template <class Pol, class TS, class TM, class TV>
 static rc_status rm_corr_select(rc_ctx* ctx, const Pol& pol, int64_t n, TV* V, int64_t ldv, int64_t s,
                                 int64_t degree, double a, double b, const TM* R, const float* sig,
                                 const double* coef, TM* A, TM* B, int64_t ld, int64_t band,
-                                const StageOffsets* so) {
+                                const StageOffsets* so, const CorrRmOut& ro) {
     if ((n + 1) * ld < ((int64_t)1 << 32))
         return run_rm_corr<Pol, TS, TS, 1, uint32_t, TM, TV>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B,
-                                                             ld, band, so);
+                                                             ld, band, so, ro);
     return run_rm_corr<Pol, TS, TS, 1, int64_t, TM, TV>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld,
-                                                        band, so);
+                                                        band, so, ro);
 }
 
 // Real operators (CSR, 5/7/27-point stencils) and complex Hermitian ones (CSR, 5/7-point stencils
@@ -477,7 +520,7 @@ bool rm_corr_supported(const rc_op* op, int64_t s) {
 template <class TS, class TM, class TV>
 static rc_status rm_corr_dispatch(rc_ctx* ctx, rc_op* op, TV* V, int64_t ldv, int64_t s, int64_t degree, double a,
                                   double b, const TM* R, const float* sig, const double* coef, TM* A, TM* B,
-                                  int64_t ld) {
+                                  int64_t ld, const CorrRmOut& ro) {
     const int64_t n = op->n;
     const int64_t band = op->kind == 0 ? op->band : (op->skind == 5 ? op->nx : op->nx * op->ny);
     StageOffsets so_v;
@@ -485,31 +528,34 @@ static rc_status rm_corr_dispatch(rc_ctx* ctx, rc_op* op, TV* V, int64_t ldv, in
     if (op->kind == 0) {
         CsrRows<TS, TS> pol{op->rowptr, op->colind, (const TS*)op->vals32};
         return rm_corr_select<CsrRows<TS, TS>, TS>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B, ld, band,
-                                                   so);
+                                                   so, ro);
     }
     const double theta = 2.0 * 3.14159265358979323846 * op->flux;
     if constexpr (!IsComplex<TS>::value) {
         if (op->skind == 27) {
             StencilRows<float, TS, 27> pol{op->nx, op->ny, op->nz, op->diag32, op->offdiag, theta};
             return rm_corr_select<StencilRows<float, TS, 27>, TS>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef,
-                                                                  A, B, ld, band, so);
+                                                                  A, B, ld, band, so, ro);
         }
     }
     if (op->skind == 7) {
         StencilRows<float, TS, 7> pol{op->nx, op->ny, op->nz, op->diag32, op->offdiag, theta};
         pol.ph = (const TS*)op->phase32;
         return rm_corr_select<StencilRows<float, TS, 7>, TS>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A,
-                                                             B, ld, band, so);
+                                                             B, ld, band, so, ro);
     }
     StencilRows<float, TS, 5> pol{op->nx, op->ny, op->nz, op->diag32, op->offdiag, theta};
     pol.ph = (const TS*)op->phase32;
     return rm_corr_select<StencilRows<float, TS, 5>, TS>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B,
-                                                         ld, band, so);
+                                                         ld, band, so, ro);
 }
 
 rc_status rm_filter_corr(rc_ctx* ctx, rc_op* op, void* V, int64_t ldv, int64_t s, int64_t degree, double a,
-                         double b, const double* lam_dev, const void* R, void* bufA, void* bufB) {
+                         double b, const double* lam_dev, const void* R, void* bufA, void* bufB, const double* Yrm,
+                         int64_t ldy, double* Vf, int64_t ldf) {
     if (!rm_corr_supported(op, s)) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "correction filter: unsupported operator");
+    if (Vf && (op->dtype != RC_REAL64 || ctx->serve || !Yrm || ldy < s || ldf < s || ldy % 2 || ldf % 2))
+        return rc_fail(ctx, RC_ERR_INVALID, "correction filter: bad row-major result arguments");
     if (degree < 1) return RC_OK;
     RC_TRY(ensure_fp32(ctx, op));
     const bool cplx = op->dtype == RC_COMPLEX128;
@@ -525,12 +571,17 @@ rc_status rm_filter_corr(rc_ctx* ctx, rc_op* op, void* V, int64_t ldv, int64_t s
                                  bufB, &handled));
         if (handled) return RC_OK;
     }
+    CorrRmOut ro;
+    ro.yrm = Yrm;
+    ro.ldy = ldy;
+    ro.vf = Vf;
+    ro.ldf = ldf;
     if (cplx)
         return rm_corr_dispatch<float2, rc_corr2_t, double2>(ctx, op, (double2*)V, ldv, s, degree, a, b,
                                                             (const rc_corr2_t*)R, sig, coef, (rc_corr2_t*)bufA,
-                                                            (rc_corr2_t*)bufB, ld);
+                                                            (rc_corr2_t*)bufB, ld, ro);
     return rm_corr_dispatch<float, rc_corr_t, double>(ctx, op, (double*)V, ldv, s, degree, a, b, (const rc_corr_t*)R,
-                                                      sig, coef, (rc_corr_t*)bufA, (rc_corr_t*)bufB, ld);
+                                                      sig, coef, (rc_corr_t*)bufA, (rc_corr_t*)bufB, ld, ro);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -638,6 +689,21 @@ rc_status to_row_major(rc_ctx* ctx, int dtype, int64_t n, int64_t s, const void*
                                                                         ld);
     else
         to_rm_kernel<double, double><<<tgrid, tblk, 0, ctx->stream>>>(n, s, (const double*)V, ldv, (double*)Yrm, ld);
+    ctx->launches++;
+    RC_CU(ctx, cudaGetLastError());
+    return RC_OK;
+}
+
+rc_status to_col_major(rc_ctx* ctx, int dtype, int64_t n, int64_t s, const void* Yrm, int64_t ld, void* V,
+                       int64_t ldv) {
+    if ((s + 31) / 32 > 65535) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "column-major copy: too many columns");
+    const dim3 tgrid((unsigned)((n + 31) / 32), (unsigned)((s + 31) / 32)), tblk(32, 8);
+    if (dtype == RC_COMPLEX128)
+        to_cm_kernel<double2, double2><<<tgrid, tblk, 0, ctx->stream>>>(n, s, (const double2*)Yrm, ld, (double2*)V,
+                                                                        ldv, 1.0);
+    else
+        to_cm_kernel<double, double><<<tgrid, tblk, 0, ctx->stream>>>(n, s, (const double*)Yrm, ld, (double*)V, ldv,
+                                                                      1.0);
     ctx->launches++;
     RC_CU(ctx, cudaGetLastError());
     return RC_OK;

@@ -71,26 +71,54 @@ __device__ __forceinline__ void load_cols_async(double* tile, int rp, const doub
     }
 }
 
+// Copy rows [r0, r0 + RT) of columns [0, ncols) of a row-major block (leading dimension ld, even,
+// rows 16-byte aligned) into a shared tile laid out row by row with `rp` doubles per row, in
+// 16-byte pairs (an odd last column is copied with its neighbour zero-filled; rows past r_end read
+// as zero).
+template <int RT>
+__device__ __forceinline__ void load_rows_async(double* tile, int rp, const double* __restrict__ src, int64_t ld,
+                                                int ncols, int64_t r0, int64_t r_end, int tid, int nthreads) {
+    const int pairs = (ncols + 1) / 2;
+    for (int e = tid; e < RT * pairs; e += nthreads) {
+        const int rr = e / pairs, c = 2 * (e - rr * pairs);
+        const int64_t r = r0 + rr;
+        const int bytes = r < r_end ? (c + 1 < ncols ? 16 : 8) : 0;
+        cp_async16(tile + rr * rp + c, bytes ? src + r * ld + c : src, bytes);
+    }
+}
+
 // ---------------------------------------------------------------------------------------
 // gram2
 // ---------------------------------------------------------------------------------------
 constexpr int GM_KT = 32;          // rows per K-tile
 constexpr int GM_KP = GM_KT + 4;   // doubles per column in shared memory (= 4 mod 16: conflict-free fragments)
+// Shared-memory operand tile of gram_mma_kernel: column-major inputs are held column by column
+// (GM_KP doubles per column), row-major inputs row by row (32 SB + 4 doubles per row, also = 4 mod
+// 16); element (row rr, column c) lies at c * CS + rr * RS.
+template <int SB, bool RM>
+struct GmTile {
+    static constexpr int RP = 32 * SB + 4;
+    static constexpr int SIZE = RM ? GM_KT * RP : 32 * SB * GM_KP;
+    static constexpr int CS = RM ? 1 : GM_KP;
+    static constexpr int RS = RM ? RP : 1;
+};
 
 template <int SB, int NY>
 constexpr int gm_threads() {
     return 32 * NY * SB * (SB + 1) / 2;
 }
 
-template <int SB, int NY, bool V16>
+template <int SB, int NY, bool V16, bool RM = false>
 __global__ void __launch_bounds__(gm_threads<SB, NY>(), 1)
 gram_mma_kernel(int64_t n, int m, const double* __restrict__ X, int64_t ldx, const double* __restrict__ Y0,
                 int64_t ldy0, const double* __restrict__ Y1, int64_t ldy1, double* __restrict__ part, int64_t rows) {
+    using TL = GmTile<SB, RM>;
     constexpr int NT = gm_threads<SB, NY>();
     constexpr int NP = SB * (SB + 1) / 2;
     constexpr int SC = 32 * SB;                 // padded columns
     constexpr int OPS = 1 + NY;                 // operands per stage
-    constexpr int STAGE = OPS * SC * GM_KP;     // doubles per stage
+    constexpr int OPSZ = TL::SIZE;              // doubles per operand tile
+    constexpr int STAGE = OPS * OPSZ;           // doubles per stage
     extern __shared__ __align__(16) double gms[];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, q = lane & 3;
@@ -103,8 +131,16 @@ gram_mma_kernel(int64_t n, int m, const double* __restrict__ X, int64_t ldx, con
     const int bj = bi + pidx;
     const int64_t r_begin = (int64_t)blockIdx.x * rows;
     const int64_t r_end = min(n, r_begin + rows);
-    // zero the padding columns m..SC of every operand of both stages once (never copied into)
-    {
+    // zero the padding columns m..SC of every operand of both stages once (never copied into, or
+    // zero-filled by the copies)
+    if constexpr (RM) {
+        const int per = GM_KT * (SC - m);
+        for (int e = tid; e < 2 * OPS * per; e += NT) {
+            const int op = e / per, f = e - op * per;
+            const int rr = f / (SC - m), c = m + (f - rr * (SC - m));
+            gms[op * OPSZ + rr * TL::RP + c] = 0.0;
+        }
+    } else {
         const int per = (SC - m) * GM_KP;
         for (int e = tid; e < 2 * OPS * per; e += NT) {
             const int st = e / per, f = e - st * per;
@@ -120,9 +156,15 @@ gram_mma_kernel(int64_t n, int m, const double* __restrict__ X, int64_t ldx, con
     auto issue = [&](int64_t t) {
         double* st = gms + (t & 1) * STAGE;
         const int64_t r0 = r_begin + t * GM_KT;
-        load_cols_async<GM_KT, V16>(st, GM_KP, X, ldx, m, r0, r_end, tid, NT);
-        load_cols_async<GM_KT, V16>(st + SC * GM_KP, GM_KP, Y0, ldy0, m, r0, r_end, tid, NT);
-        if (NY == 2) load_cols_async<GM_KT, V16>(st + 2 * SC * GM_KP, GM_KP, Y1, ldy1, m, r0, r_end, tid, NT);
+        if constexpr (RM) {
+            load_rows_async<GM_KT>(st, TL::RP, X, ldx, m, r0, r_end, tid, NT);
+            load_rows_async<GM_KT>(st + OPSZ, TL::RP, Y0, ldy0, m, r0, r_end, tid, NT);
+            if (NY == 2) load_rows_async<GM_KT>(st + 2 * OPSZ, TL::RP, Y1, ldy1, m, r0, r_end, tid, NT);
+        } else {
+            load_cols_async<GM_KT, V16>(st, GM_KP, X, ldx, m, r0, r_end, tid, NT);
+            load_cols_async<GM_KT, V16>(st + SC * GM_KP, GM_KP, Y0, ldy0, m, r0, r_end, tid, NT);
+            if (NY == 2) load_cols_async<GM_KT, V16>(st + 2 * SC * GM_KP, GM_KP, Y1, ldy1, m, r0, r_end, tid, NT);
+        }
     };
     // two stages, one barrier per K-tile: after the barrier every warp has finished tile t-1, so
     // the copies of tile t+1 go into its stage while tile t is multiplied
@@ -133,15 +175,15 @@ gram_mma_kernel(int64_t n, int m, const double* __restrict__ X, int64_t ldx, con
         __syncthreads();
         if (t + 1 < ntiles) issue(t + 1);
         cp_async_commit();
-        const double* xs = gms + (t & 1) * STAGE + (bi * 32 + g) * GM_KP + q;
-        const double* ys = gms + (t & 1) * STAGE + (1 + y) * SC * GM_KP + (bj * 32 + g) * GM_KP + q;
+        const double* xs = gms + (t & 1) * STAGE + (bi * 32 + g) * TL::CS + q * TL::RS;
+        const double* ys = gms + (t & 1) * STAGE + (1 + y) * OPSZ + (bj * 32 + g) * TL::CS + q * TL::RS;
 #pragma unroll
         for (int k0 = 0; k0 < GM_KT; k0 += 4) {
             double a[4], b[4];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = xs[i * 8 * GM_KP + k0];
+            for (int i = 0; i < 4; ++i) a[i] = xs[i * 8 * TL::CS + k0 * TL::RS];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = ys[j * 8 * GM_KP + k0];
+            for (int j = 0; j < 4; ++j) b[j] = ys[j * 8 * TL::CS + k0 * TL::RS];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -181,21 +223,22 @@ __global__ void gram2_reduce_kernel(int m, int64_t nchunks, int ny, const double
 
 bool gram2_supported(int dtype, int64_t m) { return dtype == RC_REAL64 && m >= 1 && m <= 96; }
 
-template <int SB, int NY, bool V16>
+template <int SB, int NY, bool V16, bool RM>
 static rc_status gram_mma_launch(rc_ctx* ctx, int64_t n, int64_t m, const double* X, int64_t ldx, const double* Y0,
                                  int64_t ldy0, const double* Y1, int64_t ldy1, double* part, int64_t nchunks,
                                  int64_t rows) {
     constexpr int NT = gm_threads<SB, NY>();
-    const size_t smem = (size_t)2 * (1 + NY) * 32 * SB * GM_KP * sizeof(double);
-    RC_CU(ctx, allow_max_smem(ctx, gram_mma_kernel<SB, NY, V16>));
-    gram_mma_kernel<SB, NY, V16><<<(unsigned)nchunks, NT, smem, ctx->stream>>>(n, (int)m, X, ldx, Y0, ldy0, Y1,
-                                                                               ldy1, part, rows);
+    const size_t smem = (size_t)2 * (1 + NY) * GmTile<SB, RM>::SIZE * sizeof(double);
+    RC_CU(ctx, allow_max_smem(ctx, gram_mma_kernel<SB, NY, V16, RM>));
+    gram_mma_kernel<SB, NY, V16, RM><<<(unsigned)nchunks, NT, smem, ctx->stream>>>(n, (int)m, X, ldx, Y0, ldy0, Y1,
+                                                                                   ldy1, part, rows);
     return RC_OK;
 }
 
 // C0 = X^T Y0 and (if Y1) C1 = X^T Y1, square m x m symmetric results (upper computed, mirrored).
+// rm: the blocks are row-major (leading dimensions even, rows 16-byte aligned).
 rc_status gram2(rc_ctx* ctx, int64_t n, int64_t m, const double* X, int64_t ldx, const double* Y0, int64_t ldy0,
-                double* C0, const double* Y1, int64_t ldy1, double* C1) {
+                double* C0, const double* Y1, int64_t ldy1, double* C1, bool rm) {
     const int ny = Y1 ? 2 : 1;
     const int sb = (int)((m + 31) / 32);
     // one CTA per SM for the widest blocks; narrower blocks run several CTAs per SM
@@ -206,15 +249,18 @@ rc_status gram2(rc_ctx* ctx, int64_t n, int64_t m, const double* X, int64_t ldx,
     nchunks = (n + rows - 1) / rows;
     void* part = nullptr;
     RC_TRY(rc_slot(ctx, S_PART, (size_t)ny * nchunks * m * m * sizeof(double), &part));
-    // 16-byte copies need 16-byte aligned columns
+    // 16-byte copies need 16-byte aligned columns (rows, for row-major blocks)
     const bool v16 = ((uintptr_t)X % 16 == 0) && ((uintptr_t)Y0 % 16 == 0) && (ldx % 2 == 0) && (ldy0 % 2 == 0) &&
                      (!Y1 || (((uintptr_t)Y1 % 16 == 0) && (ldy1 % 2 == 0)));
+    if (rm && (!v16 || ldx < m || ldy0 < m || (Y1 && ldy1 < m)))
+        return rc_fail(ctx, RC_ERR_INVALID, "gram2: row-major blocks need even leading dimensions >= m, 16-byte aligned");
     const double* y1 = Y1 ? Y1 : Y0;
     const int64_t l1 = Y1 ? ldy1 : ldy0;
     double* pp = (double*)part;
 #define RC_GM(SBV, NYV)                                                                                           \
-    (v16 ? gram_mma_launch<SBV, NYV, true>(ctx, n, m, X, ldx, Y0, ldy0, y1, l1, pp, nchunks, rows)                \
-         : gram_mma_launch<SBV, NYV, false>(ctx, n, m, X, ldx, Y0, ldy0, y1, l1, pp, nchunks, rows))
+    (rm ? gram_mma_launch<SBV, NYV, true, true>(ctx, n, m, X, ldx, Y0, ldy0, y1, l1, pp, nchunks, rows)           \
+        : v16 ? gram_mma_launch<SBV, NYV, true, false>(ctx, n, m, X, ldx, Y0, ldy0, y1, l1, pp, nchunks, rows)    \
+              : gram_mma_launch<SBV, NYV, false, false>(ctx, n, m, X, ldx, Y0, ldy0, y1, l1, pp, nchunks, rows))
     rc_status st;
     if (ny == 2) st = sb == 1 ? RC_GM(1, 2) : (sb == 2 ? RC_GM(2, 2) : RC_GM(3, 2));
     else st = sb == 1 ? RC_GM(1, 1) : (sb == 2 ? RC_GM(2, 1) : RC_GM(3, 1));
@@ -378,7 +424,9 @@ xt_mma_kernel(int64_t n, int k, int nc, const double* __restrict__ X, int64_t ld
 constexpr int XP_RT = 64;
 constexpr int XP_RP = XP_RT + 4;  // = 4 mod 16
 
-template <int NH, bool V16>
+// X row-major (RM): the 64-row tiles are held row by row with kpt doubles per row (= 4 mod 16),
+// element (row r, column kk) at r * RS + kk * CS in both layouts.
+template <int NH, bool V16, bool RM = false>
 __global__ void __launch_bounds__(128 * NH, 1)
 xt_mma_plain_kernel(int64_t n, int k, int nc, const double* __restrict__ X, int64_t ldx,
                     const double* __restrict__ Tm, int64_t ldt, double* __restrict__ Y, int64_t ldy,
@@ -388,8 +436,9 @@ xt_mma_plain_kernel(int64_t n, int k, int nc, const double* __restrict__ X, int6
     const int k4 = (k + 3) / 4 * 4;
     extern __shared__ __align__(16) double xps[];
     double* Ts = xps;                            // [NH*48][kpt]
-    double* tiles = Ts + (size_t)NH * 48 * kpt;  // [2][k4][XP_RP]
-    const int stage = k4 * XP_RP;
+    double* tiles = Ts + (size_t)NH * 48 * kpt;  // [2][k4][XP_RP], or [2][XP_RT][kpt] when RM
+    const int stage = RM ? XP_RT * kpt : k4 * XP_RP;
+    const int CS = RM ? 1 : XP_RP, RS = RM ? kpt : 1;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, q = lane & 3;
     const int slab = warp & 3, half = warp >> 2;
@@ -398,25 +447,35 @@ xt_mma_plain_kernel(int64_t n, int k, int nc, const double* __restrict__ X, int6
         const int c = e / kpt, kk = e - c * kpt;
         Ts[e] = (c < nc && kk < k) ? Tm[kk + (int64_t)c * ldt] : 0.0;
     }
-    {
+    if constexpr (RM) {  // padding columns k..k4 of every row of both stages
+        const int w = k4 - k;
+        for (int e = tid; e < 2 * XP_RT * w; e += NT) {
+            const int row = e / w;  // stage-major: row in [0, 2 * XP_RT)
+            tiles[row * kpt + k + (e - row * w)] = 0.0;
+        }
+    } else {
         const int per = (k4 - k) * XP_RP;
         for (int e = tid; e < 2 * per; e += NT) {
             const int st = e / per, f = e - st * per;
             tiles[st * stage + k * XP_RP + f] = 0.0;
         }
     }
+    auto load = [&](double* dst, int64_t r0) {
+        if constexpr (RM) load_rows_async<XP_RT>(dst, kpt, X, ldx, k, r0, n, tid, NT);
+        else load_cols_async<XP_RT, V16>(dst, XP_RP, X, ldx, k, r0, n, tid, NT);
+    };
     const int64_t ntiles = (n + XP_RT - 1) / XP_RT;
     int buf = 0;
     int64_t t = blockIdx.x;
-    if (t < ntiles) load_cols_async<XP_RT, V16>(tiles, XP_RP, X, ldx, k, t * XP_RT, n, tid, NT);
+    if (t < ntiles) load(tiles, t * XP_RT);
     cp_async_commit();
     for (; t < ntiles; t += gridDim.x) {
         cp_async_wait0();
         __syncthreads();
         const int64_t tn = t + gridDim.x;
-        if (tn < ntiles) load_cols_async<XP_RT, V16>(tiles + (buf ^ 1) * stage, XP_RP, X, ldx, k, tn * XP_RT, n, tid, NT);
+        if (tn < ntiles) load(tiles + (buf ^ 1) * stage, tn * XP_RT);
         cp_async_commit();
-        const double* xs = tiles + buf * stage + slab * 16 + g + q * XP_RP;
+        const double* xs = tiles + buf * stage + (slab * 16 + g) * RS + q * CS;
         const double* ts = Ts + (cbase + g) * kpt + q;
         double acc[2][XM_CT][2];
 #pragma unroll
@@ -425,7 +484,7 @@ xt_mma_plain_kernel(int64_t n, int k, int nc, const double* __restrict__ X, int6
             for (int j = 0; j < XM_CT; ++j) acc[m][j][0] = acc[m][j][1] = 0.0;
 #pragma unroll 2
         for (int k0 = 0; k0 < k4; k0 += 4) {
-            const double a0 = xs[k0 * XP_RP], a1 = xs[k0 * XP_RP + 8];
+            const double a0 = xs[k0 * CS], a1 = xs[k0 * CS + 8 * RS];
             double b[XM_CT];
 #pragma unroll
             for (int j = 0; j < XM_CT; ++j) b[j] = ts[j * 8 * kpt + k0];
@@ -547,6 +606,34 @@ rc_status xt2(rc_ctx* ctx, int64_t n, int64_t k, int64_t nc, const double* X, in
         ctx->launches++;
         RC_CU(ctx, cudaGetLastError());
     }
+    return RC_OK;
+}
+
+// Y = X T for a row-major X (leading dimension ldx, even, >= k, rows 16-byte aligned): Y column-major
+// (ldy) and, when Yrm is given, a row-major copy (ldyr, even).
+rc_status xt2_rm(rc_ctx* ctx, int64_t n, int64_t k, int64_t nc, const double* X, int64_t ldx, const double* T,
+                 int64_t ldt, double* Y, int64_t ldy, double* Yrm, int64_t ldyr) {
+    if (!xt2_supported(RC_REAL64, k, nc)) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "xt2_rm: k, nc <= 96 only");
+    if ((uintptr_t)X % 16 != 0 || ldx % 2 != 0 || ldx < k)
+        return rc_fail(ctx, RC_ERR_INVALID, "xt2_rm: row-major X needs an even leading dimension >= k, 16-byte aligned");
+    if (Yrm && (ldyr % 2 != 0 || (uintptr_t)Yrm % 16 != 0))
+        return rc_fail(ctx, RC_ERR_INVALID, "xt2_rm: the row-major copy needs an even leading dimension");
+    const int nh = nc <= 48 ? 1 : 2;
+    const int64_t pt = (n + XP_RT - 1) / XP_RT;
+    const unsigned pg = (unsigned)std::max<int64_t>(1, std::min<int64_t>(pt, ctx->sm_count));
+    const int kpt = xm_kpt((int)k);
+    const size_t psm = ((size_t)nh * 48 * kpt + (size_t)2 * XP_RT * kpt) * sizeof(double);
+    if (nh == 1) {
+        RC_CU(ctx, allow_max_smem(ctx, xt_mma_plain_kernel<1, true, true>));
+        xt_mma_plain_kernel<1, true, true><<<pg, 128, psm, ctx->stream>>>(n, (int)k, (int)nc, X, ldx, T, ldt, Y,
+                                                                          ldy, Yrm, ldyr);
+    } else {
+        RC_CU(ctx, allow_max_smem(ctx, xt_mma_plain_kernel<2, true, true>));
+        xt_mma_plain_kernel<2, true, true><<<pg, 256, psm, ctx->stream>>>(n, (int)k, (int)nc, X, ldx, T, ldt, Y,
+                                                                          ldy, Yrm, ldyr);
+    }
+    ctx->launches++;
+    RC_CU(ctx, cudaGetLastError());
     return RC_OK;
 }
 

@@ -75,6 +75,9 @@ struct rc_ctx {
     // CTAs of the Jacobi eigensolve when its working copies live in global memory (0 = 32; 1 = the
     // one-CTA kernel), from RCB200_JACOBI_CTAS.
     int jacobi_ctas = 0;
+    // Rayleigh-Ritz of the correction filter's output on row-major blocks (the filtered block and
+    // W = A V formed row-major, no transposes): 1 (default) or 0, from RCB200_RM_RR.
+    int rm_rr = 1;
     int64_t staged_launches = 0;
     // staged step shape: rows per chunk (multiple of 4) and pipeline stages; 0 = the largest that
     // fit. RCB200_STAGED_ROWS, RCB200_STAGED_STAGES.
@@ -96,7 +99,7 @@ struct rc_ctx {
 
 enum Slot {
     S_V = 0, S_W, S_T1, S_T2, S_FOUND, S_PART, S_SMALL, S_LANCZOS, S_RPART, S_IO, S_CB, S_EIG, S_FA, S_FB,
-    S_R32, S_CORR, S_YRM, S_BATCH, S_COUNT
+    S_R32, S_CORR, S_YRM, S_BATCH, S_VFRM, S_WRM, S_COUNT
 };
 
 struct rc_op {
@@ -206,8 +209,12 @@ rc_status serve_filter_corr(rc_ctx* ctx, rc_op* op, double* V, int64_t ldv, int6
 // (small) deviation from the scalar recurrence. bufA and bufB: two row-major blocks of the same
 // size as R.
 bool rm_corr_supported(const rc_op* op, int64_t s);
+// With Vf (real operators, not under the request server): the result goes to the row-major FP64 block
+// Vf (leading dimension ldf, even) instead of V, formed from Yrm, the row-major copy of V (leading
+// dimension ldy), and V is left unchanged.
 rc_status rm_filter_corr(rc_ctx* ctx, rc_op* op, void* V, int64_t ldv, int64_t s, int64_t degree, double a,
-                         double b, const double* lam_dev, const void* R, void* bufA, void* bufB);
+                         double b, const double* lam_dev, const void* R, void* bufA, void* bufB,
+                         const double* Yrm = nullptr, int64_t ldy = 0, double* Vf = nullptr, int64_t ldf = 0);
 int64_t rm_leading_dim(int dtype, int prec, int64_t s);
 // Leading dimension (elements) and element bytes of the correction filter's row-major blocks.
 inline int64_t corr_leading_dim(int dtype, int64_t s) { return rm_leading_dim(dtype, P32, s); }
@@ -233,6 +240,9 @@ rc_status corr_coefficients(rc_ctx* ctx, int64_t s, int64_t ld, int64_t degree, 
 // block V.
 rc_status to_row_major(rc_ctx* ctx, int dtype, int64_t n, int64_t s, const void* V, int64_t ldv, void* Yrm,
                        int64_t ld);
+// The reverse: column-major V (leading dimension ldv) from the row-major Yrm (leading dimension ld).
+rc_status to_col_major(rc_ctx* ctx, int dtype, int64_t n, int64_t s, const void* Yrm, int64_t ld, void* V,
+                       int64_t ldv);
 // Build the FP32 (c64) copy of an operator's values/diagonal used by the MIXED filter.
 rc_status ensure_fp32(rc_ctx* ctx, rc_op* op);
 // Degree-step timing (ctx->step_timing): record an event on the context stream; step_flush
@@ -272,8 +282,11 @@ rc_status xt(rc_ctx* ctx, int dtype, const XtArgs& a);
 // the residual block W T - Y diag(lam) in row-major FP32 when R32 is given.
 bool gram2_supported(int dtype, int64_t m);
 rc_status gram2(rc_ctx* ctx, int64_t n, int64_t m, const double* X, int64_t ldx, const double* Y0, int64_t ldy0,
-                double* C0, const double* Y1, int64_t ldy1, double* C1);
+                double* C0, const double* Y1, int64_t ldy1, double* C1, bool rm = false);
 bool xt2_supported(int dtype, int64_t k, int64_t nc);
+// Y = X T with X row-major (leading dimension ldx): Y column-major and, with Yrm, row-major.
+rc_status xt2_rm(rc_ctx* ctx, int64_t n, int64_t k, int64_t nc, const double* X, int64_t ldx, const double* T,
+                 int64_t ldt, double* Y, int64_t ldy, double* Yrm, int64_t ldyr);
 rc_status xt2(rc_ctx* ctx, int64_t n, int64_t k, int64_t nc, const double* X, int64_t ldx, const double* T,
               int64_t ldt, double* Y, int64_t ldy, const double* W, int64_t ldw, const double* lam, int64_t res_count,
               double* res, float* R32 = nullptr, int64_t ldr = 0, double* Yrm = nullptr, int64_t ldyr = 0);

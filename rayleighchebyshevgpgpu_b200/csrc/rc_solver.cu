@@ -97,6 +97,10 @@ private:
     // valid while haveR_ (written by the last Rayleigh-Ritz step, consumed by the next filter)
     bool haveR_ = false;
     bool rWritten_ = false;  // set by ritz_and_residuals when it wrote the residual block
+    // the correction filter left the filtered block row-major in the S_VFRM slot (V_ still holds the
+    // Ritz vectors it started from); rr_fused then works on row-major blocks
+    bool vfRm_ = false;
+    bool rm_rr_ok(int64_t s, int64_t reps) const;
     int64_t corr_iters_ = 0, corr_steps_ = 0;
 
     std::vector<double> eigValues_, eigVecResiduals_, VtAVeigValue_, subspaceResiduals_;
@@ -264,6 +268,14 @@ rc_status Solver::ritz_and_residuals(XtArgs a, int64_t s, int64_t res_count, voi
     return xt(ctx_, dtype_, a);
 }
 
+// The row-major Rayleigh-Ritz step after a correction filter: real native operators with blocks the
+// DMMA kernels take (s <= 96), one filter application per iteration, no found vectors to deflate
+// against (the deflation works on column-major blocks), outside the request server.
+bool Solver::rm_rr_ok(int64_t s, int64_t reps) const {
+    return ctx_->rm_rr && dtype_ == RC_REAL64 && !ctx_->serve && P_.orth_mode == 0 && reps == 1 && foundSize_ == 0 &&
+           gram2_supported(dtype_, s) && xt2_supported(dtype_, s, s) && resid_supported(op_, s);
+}
+
 rc_status Solver::r32_block(int64_t s, void** out) {
     return rc_slot(ctx_, S_R32, (size_t)n_ * corr_leading_dim(dtype_, s) * corr_elem_bytes(dtype_), out);
 }
@@ -306,18 +318,32 @@ rc_status Solver::rr(void*& X, void*& AX, int64_t s, int64_t res_count, bool rea
 // >= 1e-3, no shift needed); otherwise *ok = false, V_ still holds V_f and the caller
 // orthonormalises and repeats the Rayleigh-Ritz step.
 rc_status Solver::rr_fused(int64_t s, int64_t res_count, bool* ok, void* R32) {
-    StepArgs st;
-    st.s = s;
-    st.x = V_; st.xp = P64; st.ldx = n_;
-    st.y = W_; st.yp = P64; st.ldy = n_;
-    st.cp = P64;
-    RC_TRY(op_step(ctx_, op_, st));
-    if (gram2_supported(dtype_, s)) {
-        RC_TRY(gram2(ctx_, n_, s, (const double*)V_, n_, (const double*)V_, n_, (double*)G_, (const double*)W_, n_,
-                     (double*)H_));
+    const bool rm = vfRm_;
+    vfRm_ = false;
+    const int64_t ldrm = rm_leading_dim(RC_REAL64, P64, s);
+    void *vf = nullptr, *wrm = nullptr;
+    if (rm) {
+        // row-major: V_f from the correction filter, W = A V_f by the filter's FP64 step kernel
+        RC_TRY(rc_slot(ctx_, S_VFRM, (size_t)n_ * ldrm * sizeof(double), &vf));
+        RC_TRY(rc_slot(ctx_, S_WRM, (size_t)n_ * ldrm * sizeof(double), &wrm));
+        const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+        RC_TRY(rm_step(ctx_, op_, vf, nullptr, wrm, ldrm, s, one, zero, zero, RC_PREC_FP64));
+        RC_TRY(gram2(ctx_, n_, s, (const double*)vf, ldrm, (const double*)vf, ldrm, (double*)G_, (const double*)wrm,
+                     ldrm, (double*)H_, true));
     } else {
-        RC_TRY(gram(ctx_, dtype_, n_, s, s, V_, n_, V_, n_, G_, true));
-        RC_TRY(gram(ctx_, dtype_, n_, s, s, V_, n_, W_, n_, H_, true));
+        StepArgs st;
+        st.s = s;
+        st.x = V_; st.xp = P64; st.ldx = n_;
+        st.y = W_; st.yp = P64; st.ldy = n_;
+        st.cp = P64;
+        RC_TRY(op_step(ctx_, op_, st));
+        if (gram2_supported(dtype_, s)) {
+            RC_TRY(gram2(ctx_, n_, s, (const double*)V_, n_, (const double*)V_, n_, (double*)G_, (const double*)W_,
+                         n_, (double*)H_));
+        } else {
+            RC_TRY(gram(ctx_, dtype_, n_, s, s, V_, n_, V_, n_, G_, true));
+            RC_TRY(gram(ctx_, dtype_, n_, s, s, V_, n_, W_, n_, H_, true));
+        }
     }
     RC_CU(ctx_, cudaMemsetAsync(dflags_, 0, 4 * sizeof(int), ctx_->stream));
     RC_TRY(chol_factor(ctx_, dtype_, s, n_, G_, Tt_, dflags_, dpiv_));
@@ -326,13 +352,24 @@ rc_status Solver::rr_fused(int64_t s, int64_t res_count, bool* ok, void* R32) {
     RC_TRY(hermitize(ctx_, dtype_, s, Cc_));
     RC_TRY(small_eigh(ctx_, dtype_, s, Cc_, M1_, dlam_, dinfo_));  // Y into M1
     RC_TRY(small_gemm(ctx_, dtype_, s, Tt_, false, M1_, Q_));  // Q = T Y
-    XtArgs a;
-    a.n = n_; a.k = s; a.nc = s;
-    a.X = V_; a.ldx = n_;
-    a.T = Q_; a.ldt = s;
-    a.Y = T1_; a.ldy = n_;
-    a.X2 = W_; a.ldx2 = n_;
-    RC_TRY(ritz_and_residuals(a, s, res_count, R32));
+    if (rm) {
+        // Ritz vectors V_f Q, column-major into T1_ and row-major beside them, then the residuals
+        void* yrm = nullptr;
+        RC_TRY(rc_slot(ctx_, S_YRM, (size_t)n_ * ldrm * sizeof(double), &yrm));
+        RC_TRY(xt2_rm(ctx_, n_, s, s, (const double*)vf, ldrm, (const double*)Q_, s, (double*)T1_, n_, (double*)yrm,
+                      ldrm));
+        RC_TRY(resid_block(ctx_, op_, yrm, ldrm, s, dlam_, res_count, dres_, R32,
+                           R32 ? corr_leading_dim(dtype_, s) : 0));
+        rWritten_ = R32 != nullptr;
+    } else {
+        XtArgs a;
+        a.n = n_; a.k = s; a.nc = s;
+        a.X = V_; a.ldx = n_;
+        a.T = Q_; a.ldt = s;
+        a.Y = T1_; a.ldy = n_;
+        a.X2 = W_; a.ldx2 = n_;
+        RC_TRY(ritz_and_residuals(a, s, res_count, R32));
+    }
     RC_CU(ctx_, cudaMemcpyAsync(hbuf_, dlam_, s * sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
     if (res_count > 0)
         RC_CU(ctx_, cudaMemcpyAsync(hbuf_ + s, dres_, res_count * sizeof(double), cudaMemcpyDeviceToHost,
@@ -346,6 +383,9 @@ rc_status Solver::rr_fused(int64_t s, int64_t res_count, bool* ok, void* R32) {
     *ok = !(fl[0] || fl[1] || fl[2]) && piv >= 1e-3 && std::isfinite(piv);
     if (!*ok) {
         ++fused_fallback_;
+        rWritten_ = false;
+        // the caller orthonormalises V_f: bring it to V_ when it was formed row-major
+        if (rm) RC_TRY(to_col_major(ctx_, dtype_, n_, s, vf, ldrm, V_, n_));
         return RC_OK;
     }
     ++fused_ok_;
@@ -527,8 +567,21 @@ rc_status Solver::base(double minEigValue, double lambdaMax, double maxEigValue,
                             steps += st2;
                             continue;
                         }
-                        RC_TRY(rm_filter_corr(ctx_, op_, V_, n_, subspaceSize, starDegree, fa, fb, dlam_, R32, bufA,
-                                              bufB));
+                        if (rm_rr_ok(subspaceSize, filterRepetitionCount)) {
+                            // the filtered block row-major, from the row-major copy of the Ritz
+                            // vectors that the last Rayleigh-Ritz step wrote beside V_
+                            const int64_t ldrm = rm_leading_dim(RC_REAL64, P64, subspaceSize);
+                            void* yrm = nullptr;
+                            void* vf = nullptr;
+                            RC_TRY(rc_slot(ctx_, S_YRM, (size_t)n_ * ldrm * sizeof(double), &yrm));
+                            RC_TRY(rc_slot(ctx_, S_VFRM, (size_t)n_ * ldrm * sizeof(double), &vf));
+                            RC_TRY(rm_filter_corr(ctx_, op_, V_, n_, subspaceSize, starDegree, fa, fb, dlam_, R32,
+                                                  bufA, bufB, (const double*)yrm, ldrm, (double*)vf, ldrm));
+                            vfRm_ = true;
+                        } else {
+                            RC_TRY(rm_filter_corr(ctx_, op_, V_, n_, subspaceSize, starDegree, fa, fb, dlam_, R32,
+                                                  bufA, bufB));
+                        }
                         steps += starDegree;
                         corr_steps_ += starDegree;
                     }

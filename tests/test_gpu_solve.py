@@ -126,6 +126,48 @@ def test_mixed_correction_filter_complex_and_wide_blocks(ctx, case):
         op.close()
 
 
+@pytest.mark.parametrize("kind,dims,k", [(7, (18, 17, 16), 24), (27, (14, 13, 12), 16), (5, (70, 66), 40)])
+def test_row_major_rayleigh_ritz_matches_column_major(kind, dims, k):
+    """After a correction filter the Rayleigh-Ritz step runs on row-major blocks (filtered block and
+    W = A V row-major, Gram and Ritz-vector DMMA kernels reading rows); RCB200_RM_RR=0 keeps every
+    block column-major. The two differ only in the rounding of W = A V: the same iterations, the same
+    eigenvalues to 1e-12, both at the requested residual and equal to dense LAPACK."""
+    import os
+    n = int(np.prod(dims))
+    diag = (4.0 if kind == 5 else (6.0 if kind == 7 else 1.0)) + np.random.default_rng(kind + 50).uniform(0, 3, n)
+    Q = problems.Problem(f"rmrr{kind}", dims, kind, diag, -1.0 / 26.0 if kind == 27 else -1.0, k=k)
+    A = O.csr_matrix(*Q.csr())
+    dense = O.dense_lowest(A, k)
+    incr, buf = problems.block_sizes(k)
+    start = Q.start_block(incr + buf)
+    out = {}
+    for flag in ("1", "0"):
+        old = os.environ.get("RCB200_RM_RR")
+        os.environ["RCB200_RM_RR"] = flag
+        try:
+            c = R.Context(0)
+        finally:
+            if old is None:
+                os.environ.pop("RCB200_RM_RR", None)
+            else:
+                os.environ["RCB200_RM_RR"] = old
+        for form in ("csr", "stencil"):
+            op = R.operator_from_problem(c, Q, form)
+            res = _solve(c, op, Q, k, 1e-10, "mixed", start=start)
+            assert res.info["correction_iterations"] > 0 and res.info["fp64_degree_steps"] == 0
+            X = res.evecs.T
+            r = np.linalg.norm(A @ X - X * res.evals, axis=0) / np.maximum(np.abs(res.evals), 0.1)
+            assert r.max() <= 1.5e-10, r.max()
+            np.testing.assert_allclose(res.evals, dense, rtol=1e-10, atol=1e-13)
+            out[(flag, form)] = res
+            op.close()
+        c.close()
+    for form in ("csr", "stencil"):
+        a, b = out[("1", form)], out[("0", form)]
+        np.testing.assert_allclose(a.evals, b.evals, rtol=1e-12)
+        assert abs(a.info["inner_iterations"] - b.info["inner_iterations"]) <= 1
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_multipass_deflation_incr_smaller_than_k(ctx, precision):
     Q = problems.small_laplacian((24, 24), seed=5)

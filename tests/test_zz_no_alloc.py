@@ -54,6 +54,27 @@ def test_noalloc_matches_allocating_entry_point_two_calls(ctx):
         assert np.abs(overlap - 1.0).max() < 1e-9
 
 
+def test_noalloc_allocates_no_device_memory(ctx):
+    """After one set-up call, further calls change neither the context's device memory (its
+    scratch slots and operator copies) nor the device's free memory; the grid-form Jacobi that a
+    block of this width takes (working copies in global memory) runs on the library's array."""
+    import torch
+    L = _capi.lib()
+    rng = np.random.default_rng(7)
+    H1, H2 = _hermitian(rng, 128, False), _hermitian(rng, 110, True)
+    assert _call(L.rc_small_eigh_noalloc, ctx, H1)[0] == 0  # set-up call
+    torch.cuda.synchronize()
+    slots0 = ctx.device_bytes()
+    free0 = torch.cuda.mem_get_info()[0]
+    for H in (H1, H2, H1):
+        st, ev, Q = _call(L.rc_small_eigh_noalloc, ctx, H)
+        assert st == 0, ctx.last_error()
+        assert np.abs(ev - np.linalg.eigvalsh(H)).max() < 1e-13 * np.abs(ev).max() * H.shape[0]
+    torch.cuda.synchronize()
+    assert ctx.device_bytes() == slots0
+    assert torch.cuda.mem_get_info()[0] == free0
+
+
 def test_noalloc_rejects_sizes_beyond_its_array(ctx):
     L = _capi.lib()
     H = _hermitian(np.random.default_rng(1), 129, False)
