@@ -44,10 +44,13 @@ rm_step_src_kernel(Pol op, int64_t n, int nseg, int64_t ld, int groups, const TM
 }
 
 // The 27-point steps with the box sum reused along x (rm_step_rows27).
-// 4 resident CTAs per SM: the three cross-section sums need more than the 40 registers of the
-// per-row steps.
+// RC_RM27_MIN_BLOCKS resident CTAs per SM (default 4, 64 registers): the three cross-section sums
+// need more than the 40 registers of the per-row steps.
+#ifndef RC_RM27_MIN_BLOCKS
+#define RC_RM27_MIN_BLOCKS 4
+#endif
 template <class TD, class TS, class TC, int W, class IX, bool SRC, class TM>
-__global__ void __launch_bounds__(kRmThreads, sizeof(TM) == 2 ? 3 : 4)
+__global__ void __launch_bounds__(kRmThreads, RC_RM27_MIN_BLOCKS)
 rm_step27_kernel(StencilRows<TD, TC, 27> op, int64_t n, int nseg, int64_t ld, const TM* __restrict__ x, const TM* z,
                  TM* y, TC alpha, TC beta, TC gamma, int64_t pf_z, int64_t pf_x, const TM* __restrict__ src,
                  const float* __restrict__ sig) {

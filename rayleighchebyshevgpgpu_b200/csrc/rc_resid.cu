@@ -32,6 +32,82 @@ __device__ __forceinline__ double2 resid_sub(double lm, double2 y, double2 acc) 
     return make_double2(fma(-lm, y.x, acc.x), fma(-lm, y.y, acc.y));
 }
 
+// The 27-point form (real): each thread walks kRun27 consecutive rows and keeps the 3x3
+// cross-section sums of rows i-1, i and i+1 (rm_step_rows27's scheme), so a row gathers 9
+// neighbours instead of 27: (A y)_i = (diag_i - offd) y_i + offd (Q(i-1) + Q(i) + Q(i+1)).
+// Thread (r, seg) of CTA b takes rows (b*rows_per_iter + r)*kRun27 .. + kRun27.
+template <int W, class IX>
+__device__ __forceinline__ void resid_rows27(const StencilRows<double, double, 27>& op, int64_t n, int64_t s,
+                                             int64_t ld, int rows_per_iter, int rloc, IX off, IX wstride,
+                                             const double* __restrict__ Y, const double* __restrict__ lam,
+                                             double (&sq)[W * 2], rc_corr_t* R, int64_t ldr) {
+    constexpr int V = 2;
+    const IX ldy = (IX)ld;
+    const int64_t nx = op.nx, ny = op.ny, nz = op.nz, sy = nx, sz = nx * ny;
+    const double woff = op.offd;
+    const int64_t i0 = ((int64_t)blockIdx.x * rows_per_iter + rloc) * (int64_t)kRun27;
+    const int64_t i1 = min(n, i0 + kRun27);
+    auto cross = [&](int64_t j, bool vym, bool vyp, bool vzm, bool vzp, double (&q)[W * V]) {
+#pragma unroll
+        for (int v = 0; v < W * V; ++v) q[v] = 0.0;
+#pragma unroll
+        for (int dz = -1; dz <= 1; ++dz) {
+            const bool vz = dz < 0 ? vzm : (dz > 0 ? vzp : true);
+#pragma unroll
+            for (int dy = -1; dy <= 1; ++dy) {
+                const bool vy = dy < 0 ? vym : (dy > 0 ? vyp : true);
+                if (vz && vy) {
+                    const double* yj = Y + ((IX)(j + dy * sy + dz * sz) * ldy + off);
+#pragma unroll
+                    for (int w = 0; w < W; ++w) {
+                        const Pack16<double> pk = ld16_ro(yj + w * wstride);
+#pragma unroll
+                        for (int v = 0; v < V; ++v) q[w * V + v] += pk.v[v];
+                    }
+                }
+            }
+        }
+    };
+    double qm[W * V], q0[W * V], qp[W * V];
+    for (int64_t i = i0; i < i1; ++i) {
+        const int64_t ix = i % nx, t = i / nx, iy = t % ny, iz = t / ny;
+        const bool vym = iy > 0, vyp = iy + 1 < ny, vzm = iz > 0, vzp = iz + 1 < nz;
+        if (i == i0 || ix == 0) {  // (re)start the window at the run's first row or a new x-line
+            if (ix > 0) cross(i - 1, vym, vyp, vzm, vzp, qm);
+            else
+#pragma unroll
+                for (int v = 0; v < W * V; ++v) qm[v] = 0.0;
+            cross(i, vym, vyp, vzm, vzp, q0);
+        }
+        if (ix + 1 < nx) cross(i + 1, vym, vyp, vzm, vzp, qp);
+        else
+#pragma unroll
+            for (int v = 0; v < W * V; ++v) qp[v] = 0.0;
+        const double dmw = op.diag[i] - woff;
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            const IX o = (IX)i * ldy + off + w * wstride;
+            const Pack16<double> yi = ld16_ro(Y + o);
+            float rv[V];
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                const int e = w * V + v;
+                const int64_t c = (int64_t)(off + w * wstride + v);
+                const double ay = fma(woff, (qm[e] + q0[e]) + qp[e], dmw * yi.v[v]);
+                const double d = c < s ? fma(-__ldg(lam + c), yi.v[v], ay) : 0.0;
+                sq[e] = fma(d, d, sq[e]);
+                rv[v] = (float)d;
+            }
+            if (R) corr_store2(R + i * ldr + (int64_t)(off + w * wstride), rv[0], rv[1]);
+        }
+#pragma unroll
+        for (int v = 0; v < W * V; ++v) {
+            qm[v] = q0[v];
+            q0[v] = qp[v];
+        }
+    }
+}
+
 // 4 resident CTAs per SM (64 registers): the residual epilogue keeps per-column sums in registers,
 // which spill at the filter steps' 40 (the Ritz values are re-read from L1 per row). T = double
 // (real) or double2 (complex).
@@ -53,7 +129,11 @@ resid_rm_kernel(Pol op, int64_t n, int64_t s, int nseg, int64_t ld, int groups, 
     double sq[W * V];
 #pragma unroll
     for (int v = 0; v < W * V; ++v) sq[v] = 0.0;
-    if (active) {
+    if constexpr (IsStencil27<Pol>::value) {
+        if (active)
+            resid_rows27<W, IX>(op, n, s, ld, rows_per_iter, rloc, off, wstride, Y, lam, sq,
+                                reinterpret_cast<rc_corr_t*>(Rout), ldr);
+    } else if (active) {
         const int64_t stride = rows_per_iter;
         int64_t i = (int64_t)blockIdx.x * groups * rows_per_iter + rloc;
         const int64_t i_end = min(n, ((int64_t)blockIdx.x + 1) * groups * rows_per_iter);
@@ -143,7 +223,8 @@ static rc_status resid_launch(rc_ctx* ctx, const Pol& pol, int64_t n, int64_t s,
     const int nseg = (int)(ld / (V * W));
     if (nseg > kRmThreads) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "residual block: block too wide");
     const int rows_per_iter = kRmThreads / nseg;
-    const int groups = 8;  // 80+ rows per CTA: fewer per-CTA column-sum epilogues and partials
+    // 80+ rows per CTA: fewer per-CTA column-sum epilogues and partials (27-point: kRun27 rows a thread)
+    const int groups = IsStencil27<Pol>::value ? kRun27 : 8;
     const int64_t rows_per_cta = (int64_t)groups * rows_per_iter;
     const int64_t grid = (n + rows_per_cta - 1) / rows_per_cta;
     double* part = nullptr;

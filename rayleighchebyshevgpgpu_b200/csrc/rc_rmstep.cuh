@@ -345,8 +345,11 @@ __device__ __forceinline__ void rm_step_rows27(const StencilRows<TD, TC, 27>& op
     const IX off = (IX)(threadIdx.x - rloc * nseg) * (IX)V;
     const IX wstride = (IX)nseg * (IX)V;
     const IX ldx = (IX)ld;
-    TC sg[SRC ? W * V : 1];
-    if (SRC) {
+    // source coefficients in registers, or (bfloat16 blocks, where registers bound the resident CTAs)
+    // re-read from L1 per row
+    constexpr bool kSigReg = sizeof(TM) != 2;
+    TC sg[SRC && kSigReg ? W * V : 1];
+    if (SRC && kSigReg) {
 #pragma unroll
         for (int w = 0; w < W; ++w)
 #pragma unroll
@@ -420,7 +423,11 @@ __device__ __forceinline__ void rm_step_rows27(const StencilRows<TD, TC, 27>& op
                 TC r = s_mul(alpha, ax);
                 r = s_fma(beta, xv, r);
                 if (z) r = s_fma(gamma, s_cvt<TC>(zi.v[v]), r);
-                if (SRC) r = s_fma(sg[e], s_cvt<TC>(si.v[v]), r);
+                if (SRC) {
+                    const TC sgv = kSigReg ? sg[kSigReg ? e : 0]
+                                           : s_from<TC>((double)__ldg(sig + off + w * wstride + v), 0.0);
+                    r = s_fma(sgv, s_cvt<TC>(si.v[v]), r);
+                }
                 out.v[v] = s_cvt<TS>(r);
             }
             stv<TS, TM>(y + o, out);
