@@ -289,9 +289,11 @@ typedef struct rc_solve_params {
                                       ill-conditioned; 1: always CholeskyQR2 then Rayleigh-Ritz */
     int mixed_refine;              /* MIXED, after the switch tolerance: 0 (default) the correction filter
                                       (the recurrence applied to the residual block A V - V diag(lam) of
-                                      the Ritz vectors, stored in bfloat16 with FP32 arithmetic, whose
-                                      rounding error shrinks with the residual; real operators, subspace
-                                      <= 96; FP64 filter otherwise or when it stalls); 1 the FP64 filter */
+                                      the Ritz vectors, stored in bfloat16 with FP32 / c64 arithmetic,
+                                      whose rounding error shrinks with the residual; CSR and 5/7-point
+                                      stencil operators, real or complex, and real 27-point stencils,
+                                      subspace <= 256; FP64 filter otherwise or when it stalls); 1 the
+                                      FP64 filter */
 } rc_solve_params;
 
 typedef struct rc_solve_info {
@@ -326,7 +328,8 @@ typedef struct rc_solve_info {
     int64_t correction_iterations; /* MIXED: inner iterations that ran the correction filter */
     int64_t correction_degree_steps; /* of degree_steps, those of the correction filter */
     int64_t correction_element_bytes; /* bytes per stored element of the correction filter's residual
-                                         and recurrence blocks: 2 (bfloat16) or 4 (FP32) */
+                                         and recurrence blocks: 2 (bfloat16) or 4 (FP32) for real
+                                         operators, twice that for complex ones */
 } rc_solve_info;
 
 void rc_solve_params_default(rc_solve_params* p);
