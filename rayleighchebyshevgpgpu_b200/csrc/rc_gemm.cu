@@ -71,16 +71,29 @@ __device__ __forceinline__ void load_cols_async(double* tile, int rp, const doub
     }
 }
 
+// A thread's share of the row-major tile copies below: column pair lp of rows lr0, lr0 + lrs, ...
+// (threads past lrs * pairs copy nothing). Set up once per kernel, so the copies of every tile need no
+// division by the runtime column count. Needs pairs = (ncols + 1) / 2 <= nthreads (true for the
+// blocks of at most 96 columns and the CTAs of at least 32 threads per 32 columns here).
+struct RowCopyMap {
+    int lp, lr0, lrs;
+    __device__ __forceinline__ RowCopyMap(int ncols, int tid, int nthreads) {
+        const int pairs = (ncols + 1) / 2;
+        lrs = nthreads / pairs;
+        lp = tid % pairs;
+        lr0 = tid < lrs * pairs ? tid / pairs : 1 << 30;
+    }
+};
+
 // Copy rows [r0, r0 + RT) of columns [0, ncols) of a row-major block (leading dimension ld, even,
 // rows 16-byte aligned) into a shared tile laid out row by row with `rp` doubles per row, in
 // 16-byte pairs (an odd last column is copied with its neighbour zero-filled; rows past r_end read
 // as zero).
 template <int RT>
 __device__ __forceinline__ void load_rows_async(double* tile, int rp, const double* __restrict__ src, int64_t ld,
-                                                int ncols, int64_t r0, int64_t r_end, int tid, int nthreads) {
-    const int pairs = (ncols + 1) / 2;
-    for (int e = tid; e < RT * pairs; e += nthreads) {
-        const int rr = e / pairs, c = 2 * (e - rr * pairs);
+                                                int ncols, int64_t r0, int64_t r_end, const RowCopyMap& cm) {
+    const int c = 2 * cm.lp;
+    for (int rr = cm.lr0; rr < RT; rr += cm.lrs) {
         const int64_t r = r0 + rr;
         const int bytes = r < r_end ? (c + 1 < ncols ? 16 : 8) : 0;
         cp_async16(tile + rr * rp + c, bytes ? src + r * ld + c : src, bytes);
@@ -153,13 +166,14 @@ gram_mma_kernel(int64_t n, int m, const double* __restrict__ X, int64_t ldx, con
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
     const int64_t ntiles = r_end > r_begin ? (r_end - r_begin + GM_KT - 1) / GM_KT : 0;
+    const RowCopyMap rcm(m, tid, NT);
     auto issue = [&](int64_t t) {
         double* st = gms + (t & 1) * STAGE;
         const int64_t r0 = r_begin + t * GM_KT;
         if constexpr (RM) {
-            load_rows_async<GM_KT>(st, TL::RP, X, ldx, m, r0, r_end, tid, NT);
-            load_rows_async<GM_KT>(st + OPSZ, TL::RP, Y0, ldy0, m, r0, r_end, tid, NT);
-            if (NY == 2) load_rows_async<GM_KT>(st + 2 * OPSZ, TL::RP, Y1, ldy1, m, r0, r_end, tid, NT);
+            load_rows_async<GM_KT>(st, TL::RP, X, ldx, m, r0, r_end, rcm);
+            load_rows_async<GM_KT>(st + OPSZ, TL::RP, Y0, ldy0, m, r0, r_end, rcm);
+            if (NY == 2) load_rows_async<GM_KT>(st + 2 * OPSZ, TL::RP, Y1, ldy1, m, r0, r_end, rcm);
         } else {
             load_cols_async<GM_KT, V16>(st, GM_KP, X, ldx, m, r0, r_end, tid, NT);
             load_cols_async<GM_KT, V16>(st + SC * GM_KP, GM_KP, Y0, ldy0, m, r0, r_end, tid, NT);
@@ -460,8 +474,9 @@ xt_mma_plain_kernel(int64_t n, int k, int nc, const double* __restrict__ X, int6
             tiles[st * stage + k * XP_RP + f] = 0.0;
         }
     }
+    const RowCopyMap rcm(k, tid, NT);
     auto load = [&](double* dst, int64_t r0) {
-        if constexpr (RM) load_rows_async<XP_RT>(dst, kpt, X, ldx, k, r0, n, tid, NT);
+        if constexpr (RM) load_rows_async<XP_RT>(dst, kpt, X, ldx, k, r0, n, rcm);
         else load_cols_async<XP_RT, V16>(dst, XP_RP, X, ldx, k, r0, n, tid, NT);
     };
     const int64_t ntiles = (n + XP_RT - 1) / XP_RT;
