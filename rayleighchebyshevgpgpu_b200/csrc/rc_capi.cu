@@ -285,6 +285,9 @@ rc_status rc_op_stencil_create(rc_ctx* ctx, int dtype, int kind, int64_t nx, int
     if (kind == RC_STENCIL_5PT_2D && nz != 1) return rc_fail(ctx, RC_ERR_INVALID, "5-point stencil needs nz == 1");
     if (kind == RC_STENCIL_27PT_3D && dtype == RC_COMPLEX128)
         return rc_fail(ctx, RC_ERR_UNSUPPORTED, "27-point stencil is real only");
+    // the kernels divide row indices by nx and ny with a multiply-high (RowDiv): grids below 2^32 points
+    if (nx > INT32_MAX || ny > INT32_MAX || nz > INT32_MAX || (double)nx * (double)ny * (double)nz >= 4294967296.0)
+        return rc_fail(ctx, RC_ERR_UNSUPPORTED, "stencil grids must have fewer than 2^32 points");
     rc_op* op = new (std::nothrow) rc_op();
     if (!op) return RC_ERR_NOMEM;
     op->ctx = ctx;

@@ -95,6 +95,19 @@ template <> RC_HD float s_from<float>(double re, double) { return (float)re; }
 template <> RC_HD double2 s_from<double2>(double re, double im) { return make_double2(re, im); }
 template <> RC_HD float2 s_from<float2>(double re, double im) { return make_float2((float)re, (float)im); }
 
+// ---- division of row indices by a fixed grid extent ----------------------------------
+// floor(i / d) for 0 <= i < 2^32 and 1 <= d < 2^32 as the high 64 bits of i * m, m = ceil(2^64 / d):
+// with m d = 2^64 + e, 0 <= e < d, the product is i/d + i e / (d 2^64) and i e < 2^64, so the
+// floor is exact. One 64-bit multiply-high instead of a 64-bit division per row.
+struct RowDiv {
+    uint64_t m = 0;  // 0 for d == 1
+    RC_HD RowDiv() {}
+    RC_HD explicit RowDiv(int64_t d) : m(d > 1 ? ~0ull / (uint64_t)d + 1 : 0) {}
+    __device__ __forceinline__ int64_t div(int64_t i) const {
+        return m ? (int64_t)__umul64hi((uint64_t)i, m) : i;
+    }
+};
+
 // ---- reductions ----------------------------------------------------------------------
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll

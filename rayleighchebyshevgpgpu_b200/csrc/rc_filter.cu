@@ -161,16 +161,16 @@ template <> __device__ __forceinline__ float2 phase_val<float2>(double t, bool c
 
 template <class TD, class TX, class TZ, class TY, class TC, int KIND, int CB>
 __global__ void __launch_bounds__(kStepThreads)
-stencil_step_kernel(int64_t nx, int64_t ny, int64_t nz, int64_t s, const TD* __restrict__ diag, real_t<TC> offd,
-                    double theta, const TX* __restrict__ x, int64_t ldx, const TZ* z, int64_t ldz, TY* y,
-                    int64_t ldy, TC alpha, TC beta, TC gamma, real_t<TC> scale) {
+stencil_step_kernel(int64_t nx, int64_t ny, int64_t nz, RowDiv dnx, RowDiv dny, int64_t s,
+                    const TD* __restrict__ diag, real_t<TC> offd, double theta, const TX* __restrict__ x, int64_t ldx,
+                    const TZ* z, int64_t ldz, TY* y, int64_t ldy, TC alpha, TC beta, TC gamma, real_t<TC> scale) {
     const int64_t n = nx * ny * nz;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const int64_t ix = i % nx;
-    const int64_t t = i / nx;
-    const int64_t iy = t % ny;
-    const int64_t iz = t / ny;
+    const int64_t t = dnx.div(i);
+    const int64_t ix = i - t * nx;
+    const int64_t iz = dny.div(t);
+    const int64_t iy = t - iz * ny;
     const int64_t sy = nx, sz = nx * ny;
     const real_t<TC> d = (real_t<TC>)diag[i];
     constexpr bool kCplx = IsComplex<TC>::value;
@@ -264,33 +264,34 @@ static rc_status launch_step_t(rc_ctx* ctx, rc_op* op, const StepArgs& a) {
     } else {
         const double theta = 2.0 * 3.14159265358979323846 * op->flux;
         const R offd = (R)op->offdiag;
+        const RowDiv dnx(op->nx), dny(op->ny);
         if (CP == P64) {
             const double* dg = op->diag64;
             if (op->skind == 27)
                 stencil_step_kernel<double, TX, TZ, TY, TC, 27, CB><<<grid, kStepThreads, 0, ctx->stream>>>(
-                    op->nx, op->ny, op->nz, a.s, dg, offd, theta, x, a.ldx, z, a.ldz, y, a.ldy, alpha, beta,
+                    op->nx, op->ny, op->nz, dnx, dny, a.s, dg, offd, theta, x, a.ldx, z, a.ldz, y, a.ldy, alpha, beta,
                     gamma, scale);
             else if (op->skind == 7)
                 stencil_step_kernel<double, TX, TZ, TY, TC, 7, CB><<<grid, kStepThreads, 0, ctx->stream>>>(
-                    op->nx, op->ny, op->nz, a.s, dg, offd, theta, x, a.ldx, z, a.ldz, y, a.ldy, alpha, beta,
+                    op->nx, op->ny, op->nz, dnx, dny, a.s, dg, offd, theta, x, a.ldx, z, a.ldz, y, a.ldy, alpha, beta,
                     gamma, scale);
             else
                 stencil_step_kernel<double, TX, TZ, TY, TC, 5, CB><<<grid, kStepThreads, 0, ctx->stream>>>(
-                    op->nx, op->ny, op->nz, a.s, dg, offd, theta, x, a.ldx, z, a.ldz, y, a.ldy, alpha, beta,
+                    op->nx, op->ny, op->nz, dnx, dny, a.s, dg, offd, theta, x, a.ldx, z, a.ldz, y, a.ldy, alpha, beta,
                     gamma, scale);
         } else {
             const float* dg = op->diag32;
             if (op->skind == 27)
                 stencil_step_kernel<float, TX, TZ, TY, TC, 27, CB><<<grid, kStepThreads, 0, ctx->stream>>>(
-                    op->nx, op->ny, op->nz, a.s, dg, offd, theta, x, a.ldx, z, a.ldz, y, a.ldy, alpha, beta,
+                    op->nx, op->ny, op->nz, dnx, dny, a.s, dg, offd, theta, x, a.ldx, z, a.ldz, y, a.ldy, alpha, beta,
                     gamma, scale);
             else if (op->skind == 7)
                 stencil_step_kernel<float, TX, TZ, TY, TC, 7, CB><<<grid, kStepThreads, 0, ctx->stream>>>(
-                    op->nx, op->ny, op->nz, a.s, dg, offd, theta, x, a.ldx, z, a.ldz, y, a.ldy, alpha, beta,
+                    op->nx, op->ny, op->nz, dnx, dny, a.s, dg, offd, theta, x, a.ldx, z, a.ldz, y, a.ldy, alpha, beta,
                     gamma, scale);
             else
                 stencil_step_kernel<float, TX, TZ, TY, TC, 5, CB><<<grid, kStepThreads, 0, ctx->stream>>>(
-                    op->nx, op->ny, op->nz, a.s, dg, offd, theta, x, a.ldx, z, a.ldz, y, a.ldy, alpha, beta,
+                    op->nx, op->ny, op->nz, dnx, dny, a.s, dg, offd, theta, x, a.ldx, z, a.ldz, y, a.ldy, alpha, beta,
                     gamma, scale);
         }
     }

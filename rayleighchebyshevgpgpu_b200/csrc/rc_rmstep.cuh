@@ -383,7 +383,8 @@ __device__ __forceinline__ void rm_step_rows27(const StencilRows<TD, TC, 27>& op
     };
     TC qm[W * V], q0[W * V], qp[W * V];
     for (int64_t i = i0; i < i1; ++i) {
-        const int64_t ix = i % nx, t = i / nx, iy = t % ny, iz = t / ny;
+        int64_t ix, iy, iz;
+        op.coords(i, ix, iy, iz);
         const bool vym = iy > 0, vyp = iy + 1 < ny, vzm = iz > 0, vzp = iz + 1 < nz;
         if (i == i0 || ix == 0) {  // (re)start the window at the run's first row or a new x-line
             if (ix > 0) cross(i - 1, vym, vyp, vzm, vzp, qm);

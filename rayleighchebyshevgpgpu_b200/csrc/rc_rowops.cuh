@@ -61,12 +61,20 @@ struct StencilRows {
     double offd;
     double theta;
     const TC* ph = nullptr;  // complex: phase table exp(i theta x), x < nx (else evaluated per row)
+    RowDiv dx, dy;           // division by nx and ny (grids of fewer than 2^32 points)
+    RC_HD StencilRows(int64_t nx_, int64_t ny_, int64_t nz_, const TD* diag_, double offd_, double theta_)
+        : nx(nx_), ny(ny_), nz(nz_), diag(diag_), offd(offd_), theta(theta_), dx(nx_), dy(ny_) {}
+    // grid coordinates of row i
+    __device__ __forceinline__ void coords(int64_t i, int64_t& ix, int64_t& iy, int64_t& iz) const {
+        const int64_t t = dx.div(i);
+        ix = i - t * nx;
+        iz = dy.div(t);
+        iy = t - iz * ny;
+    }
     template <class F>
     __device__ __forceinline__ void row(int64_t i, F&& f) const {
-        const int64_t ix = i % nx;
-        const int64_t t = i / nx;
-        const int64_t iy = t % ny;
-        const int64_t iz = t / ny;
+        int64_t ix, iy, iz;
+        coords(i, ix, iy, iz);
         const int64_t sy = nx, sz = nx * ny;
         f(i, s_from<TC>((double)diag[i], 0.0));
         const TC w = s_from<TC>(offd, 0.0);
