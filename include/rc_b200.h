@@ -74,7 +74,8 @@ rc_status rc_ctx_synchronize(rc_ctx* ctx);
 /* Number of kernels this library launched through ctx since creation (or last reset). */
 rc_status rc_ctx_launch_count(rc_ctx* ctx, int64_t* launches, int reset);
 /* A named counter of ctx since creation: "launches" (as rc_ctx_launch_count), "staged_launches"
- * (degree steps that ran with their operands staged in shared memory by asynchronous copies). */
+ * (degree steps that ran with their operands staged in shared memory by asynchronous copies),
+ * "pair_launches" (launches that ran two correction-filter degree steps in one pass). */
 rc_status rc_ctx_counter(rc_ctx* ctx, const char* name, int64_t* value);
 /* Device bytes currently held by ctx (workspaces + operators created on it). */
 rc_status rc_ctx_device_bytes(rc_ctx* ctx, int64_t* bytes);

@@ -142,6 +142,7 @@ rc_status rc_ctx_create(int device, rc_ctx** out) {
     if (const char* v = std::getenv("RCB200_STAGED")) c->staged = std::atoi(v) != 0 ? 1 : 0;
     if (const char* v = std::getenv("RCB200_JACOBI_CTAS")) c->jacobi_ctas = std::max(0, std::atoi(v));
     if (const char* v = std::getenv("RCB200_RM_RR")) c->rm_rr = std::atoi(v) != 0 ? 1 : 0;
+    if (const char* v = std::getenv("RCB200_CORR_PAIR")) c->corr_pair = std::atoi(v) != 0 ? 1 : 0;
     if (const char* v = std::getenv("RCB200_STAGED_ROWS")) c->staged_rows = std::max(0, std::atoi(v) / 4 * 4);
     if (const char* v = std::getenv("RCB200_STAGED_STAGES")) c->staged_stages = std::max(0, std::min(4, std::atoi(v)));
     c->pf_rows = 4096;
@@ -192,6 +193,7 @@ rc_status rc_ctx_counter(rc_ctx* ctx, const char* name, int64_t* value) {
     if (!ctx || !name || !value) return RC_ERR_INVALID;
     if (!std::strcmp(name, "launches")) *value = ctx->launches;
     else if (!std::strcmp(name, "staged_launches")) *value = ctx->staged_launches;
+    else if (!std::strcmp(name, "pair_launches")) *value = ctx->pair_launches;
     else return rc_fail(ctx, RC_ERR_INVALID, std::string("rc_ctx_counter: unknown counter ") + name);
     return RC_OK;
 }

@@ -43,6 +43,78 @@ rm_step_src_kernel(Pol op, int64_t n, int nseg, int64_t ld, int groups, const TM
                                                gamma, pf_z, pf_x, src, sig);
 }
 
+// Two consecutive degree steps of the correction filter in one pass:
+//   e_k     = a A e_{k-1} + b e_{k-1} + gA e_{k-2} + sig_k R        (phase A, into Y0; Y0 = Z in place)
+//   e_{k+1} = a A e_k     + b e_k     -    e_{k-1} + sig_{k+1} R    (phase B, into Y1; Y1 = X1 in place, or a
+//                                                                   separate block when X1 is R)
+// Work items are blocks of `groups` row groups (the rows rm_step_rows gives CTA index b), taken in
+// order from a ticket counter by persistent CTAs. Ticket t runs phase A of block t, then phase B of
+// block t - lag. Phase B of block u reads e_k of the rows within `band` of it and overwrites e_{k-1} of
+// its own rows, which phase A of those same neighbour rows reads: it waits until phase A is complete
+// for every block within band_blocks of u, counted per group of `grp` blocks (grp_cnt). Those blocks
+// hold earlier tickets, whose phase A never waits, so the kernel cannot deadlock; the waits are also
+// bounded (on a timeout *err is set and every CTA stops). Phase A reads e_{k-2} (the block it
+// overwrites with e_k) through L2 only, so no SM caches a line of it in L1 before it is final, and
+// phase B gathers e_k through the read-only path; the waits extend one block past the band, past any
+// line a gather brings in. e_k is read back from L2 shortly after it is written: the two steps move
+// five block passes through DRAM instead of eight, with the same arithmetic per row as two launches
+// of rm_step_src_kernel (bit-identical results).
+constexpr long long kPairSpins = 1ll << 20;
+// Resident CTAs per SM of rm_corr2_kernel (the two steps' code spills at the 40 registers of 6).
+#ifndef RC_PAIR_MIN_BLOCKS
+#define RC_PAIR_MIN_BLOCKS 5
+#endif
+
+template <class Pol, class TS, class TC, int W, class IX, class TM>
+__global__ void __launch_bounds__(kRmThreads, RC_PAIR_MIN_BLOCKS)
+rm_corr2_kernel(Pol op, int64_t n, int nseg, int64_t ld, int groups, const TM* X1, const TM* Z, TM* Y0, TM* Y1,
+                TC alpha, TC beta, TC gammaA, const TM* __restrict__ R, const float* __restrict__ sigA,
+                const float* __restrict__ sigB, int64_t pf_z, int64_t pf_x, int64_t nblk, int64_t lag,
+                int64_t band_blocks, int grp, unsigned long long* ticket, unsigned* grp_cnt, int* err) {
+    __shared__ long long s_t;
+    const TC m1 = s_from<TC>(-1.0, 0.0);
+    for (;;) {
+        if (threadIdx.x == 0) s_t = (long long)atomicAdd(ticket, 1ull);
+        __syncthreads();
+        const int64_t t = s_t;
+        __syncthreads();
+        if (t >= nblk + lag) break;
+        if (t < nblk) {
+            rm_step_rows<Pol, TS, TC, W, IX, true, TM, true>(op, n, nseg, ld, groups, t, X1, Z, Y0, alpha, beta,
+                                                             gammaA, pf_z, pf_x, R, sigA);
+            __threadfence();  // this thread's rows of e_k, before the block is counted complete
+            __syncthreads();
+            if (threadIdx.x == 0) atomicAdd(&grp_cnt[t / grp], 1u);
+        }
+        if (t >= lag) {
+            const int64_t u = t - lag;
+            // the groups of blocks u - band_blocks .. u + band_blocks, polled in parallel (thread j polls
+            // groups g0 + j, g0 + j + blockDim.x, ...)
+            const int64_t b_lo = u - band_blocks > 0 ? u - band_blocks : 0;
+            const int64_t b_hi = u + band_blocks < nblk - 1 ? u + band_blocks : nblk - 1;
+            const int64_t g0 = b_lo / grp, g1 = b_hi / grp;
+            long long spins = 0;
+            for (;;) {
+                int mine = 1;
+                for (int64_t g = g0 + threadIdx.x; g <= g1; g += blockDim.x) {
+                    const unsigned need = (unsigned)(nblk - g * grp < grp ? nblk - g * grp : grp);
+                    mine &= *(volatile const unsigned*)(grp_cnt + g) >= need;
+                }
+                if (__syncthreads_and(mine)) break;
+                // thread 0 decides whether to give up, the same answer for every thread
+                if (__syncthreads_or(threadIdx.x == 0 && (++spins > kPairSpins || *(volatile const int*)err != 0))) {
+                    if (threadIdx.x == 0) atomicExch(err, 1);
+                    return;
+                }
+                __nanosleep(64);
+            }
+            __threadfence();
+            rm_step_rows<Pol, TS, TC, W, IX, true, TM>(op, n, nseg, ld, groups, u, Y0, X1, Y1, alpha, beta, m1, pf_z,
+                                                       pf_x, R, sigB);
+        }
+    }
+}
+
 // The 27-point steps with the box sum reused along x (rm_step_rows27).
 // RC_RM27_MIN_BLOCKS resident CTAs per SM (default 4, 64 registers): the three cross-section sums
 // need more than the 40 registers of the per-row steps.
@@ -266,6 +338,52 @@ static void launch_step(rc_ctx* ctx, const Pol& pol, int64_t n, int nseg, int64_
     ctx->launches++;
 }
 
+// One launch of rm_corr2_kernel: persistent CTAs (the resident count of rm_corr2_kernel), work items
+// of `groups` row groups, a lag of the CTA count plus the band (in blocks) plus a group. scratch: the
+// S_PAIR slot of pair_scratch_bytes(): ticket (8 bytes), the error word (at 8, zeroed by the caller
+// once per filter application), the group counters (from 64); the ticket and counters are zeroed here.
+inline size_t pair_scratch_bytes(int64_t n, int64_t rb) {
+    const int64_t ngrp = ((n + rb - 1) / rb + 15) / 16;
+    return 64 + (size_t)ngrp * sizeof(unsigned);
+}
+
+template <class Pol, class TS, class TC, int W, class IX, class TM>
+static rc_status launch_pair(rc_ctx* ctx, const Pol& pol, int64_t n, int nseg, int64_t ld, int groups,
+                             const TM* x1, const TM* z, TM* y0, TM* y1, TC a, TC b, TC ga, const TM* R,
+                             const float* sigA, const float* sigB, int64_t pf_z, int64_t pf_x, int64_t band,
+                             void* scratch) {
+    const int rows_per_iter = kRmThreads / nseg;
+    const int64_t rb = (int64_t)groups * rows_per_iter;
+    const int64_t nblk = (n + rb - 1) / rb;
+    constexpr int kGrp = 16;
+    static std::atomic<int> per_sm{0};
+    if (per_sm.load() == 0) {
+        int v = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, rm_corr2_kernel<Pol, TS, TC, W, IX, TM>, kRmThreads,
+                                                          0) != cudaSuccess ||
+            v < 1) {
+            cudaGetLastError();
+            v = 1;
+        }
+        per_sm.store(v);
+    }
+    const int64_t grid = std::min<int64_t>(nblk, (int64_t)per_sm.load() * ctx->sm_count);
+    const int64_t band_blocks = (band + rb - 1) / rb + 1;
+    const int64_t lag = grid + band_blocks + kGrp + 1;
+    unsigned long long* ticket = (unsigned long long*)scratch;
+    int* err = (int*)((char*)scratch + 8);
+    unsigned* cnt = (unsigned*)((char*)scratch + 64);
+    RC_CU(ctx, cudaMemsetAsync(ticket, 0, 8, ctx->stream));
+    RC_CU(ctx, cudaMemsetAsync(cnt, 0, pair_scratch_bytes(n, rb) - 64, ctx->stream));
+    rm_corr2_kernel<Pol, TS, TC, W, IX, TM><<<(unsigned)grid, kRmThreads, 0, ctx->stream>>>(
+        pol, n, nseg, ld, groups, x1, z, y0, y1, a, b, ga, R, sigA, sigB, pf_z, pf_x, nblk, lag, band_blocks, kGrp,
+        ticket, cnt, err);
+    ctx->launches++;
+    ctx->pair_launches++;
+    RC_CU(ctx, cudaGetLastError());
+    return RC_OK;
+}
+
 // Scalar recurrence of the correction filter, one thread per column c:
 //   c_0 = 1, c_1 = a lam_c + b, c_k = (a lam_c + b) c_{k-1} - c_{k-2};
 //   sig[k*ld + c] = c_{k-1} for 2 <= k <= m (the source coefficient of step k),
@@ -285,13 +403,16 @@ __global__ void corr_coef_kernel(int64_t s, int64_t ld, int64_t m, double a, dou
     }
 }
 
+// fail (optional): the two-step kernel's error word; when set, V is filled with NaN so the failure
+// reaches the caller (the solver's finite-residual check).
 template <class TM, class TV>
 __global__ void __launch_bounds__(256)
 corr_to_cm_kernel(int64_t n, int64_t s, const TM* __restrict__ E, int64_t ld, TV* __restrict__ Vc, int64_t ldv,
-                  const double* __restrict__ coef, double beta) {
+                  const double* __restrict__ coef, double beta, const int* fail) {
     __shared__ CorrTile<TM> tile[32][33];
-    corr_to_cm_tile<TM, TV>(n, s, E, ld, Vc, ldv, coef, beta, (int64_t)blockIdx.x * 32, (int64_t)blockIdx.y * 32,
-                            tile);
+    const double nan = __longlong_as_double(0x7ff8000000000000ll);
+    corr_to_cm_tile<TM, TV>(n, s, E, ld, Vc, ldv, coef, fail && *fail ? nan : beta, (int64_t)blockIdx.x * 32,
+                            (int64_t)blockIdx.y * 32, tile);
 }
 
 
@@ -302,7 +423,9 @@ corr_to_cm_kernel(int64_t n, int64_t s, const TM* __restrict__ E, int64_t ld, TV
 template <class TM>
 __global__ void __launch_bounds__(256)
 corr_to_rm_kernel(int64_t n, int64_t s, const double* __restrict__ Yrm, int64_t ldy, const TM* __restrict__ E,
-                  int64_t lde, double* __restrict__ Vf, int64_t ldf, const double* __restrict__ coef, double beta) {
+                  int64_t lde, double* __restrict__ Vf, int64_t ldf, const double* __restrict__ coef, double beta,
+                  const int* fail) {
+    if (fail && *fail) beta = __longlong_as_double(0x7ff8000000000000ll);  // NaN out (see corr_to_cm_kernel)
     const int64_t pairs = ldf / 2;
     const int64_t total = n * pairs;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
@@ -414,12 +537,34 @@ static rc_status run_rm_corr(rc_ctx* ctx, const Pol& pol, int64_t n, TV* V, int6
     constexpr bool kCsr = Pol::kIsCsr;
     const int groups = ctx->rm_groups > 0 ? ctx->rm_groups : (kCsr ? 4 : 8);
     step_mark(ctx);
-    for (int64_t k = 2; k <= degree; ++k) {
+    // pairs of steps in one pass (rm_corr2_kernel) where the per-row kernels run; the 27-point stencil
+    // and the staged kernel take one step per launch
+    const bool pairs = ctx->corr_pair && degree >= 3 && !IsStencil27<Pol>::value && !(ctx->staged && so && so->n > 0);
+    void* pscr = nullptr;
+    const int* fail = nullptr;  // the two-step kernel's error word: the combination below writes NaN if set
+    if (pairs) {
+        RC_TRY(rc_slot(ctx, S_PAIR, pair_scratch_bytes(n, (int64_t)groups * (kRmThreads / nseg)), &pscr));
+        RC_CU(ctx, cudaMemsetAsync((char*)pscr + 8, 0, 8, ctx->stream));
+        fail = (const int*)((char*)pscr + 8);
+    }
+    for (int64_t k = 2; k <= degree;) {
         const TM* xk1 = k == 2 ? R : ((k - 1) % 2 == 0 ? A : B);   // e_{k-1}
         TM* y = k % 2 == 0 ? A : B;                                  // e_k
         const TM* z = k == 2 ? nullptr : (k == 3 ? R : y);           // e_{k-2}
+        if (pairs && k + 1 <= degree) {
+          if constexpr (!IsStencil27<Pol>::value) {
+            TM* y1 = (k + 1) % 2 == 0 ? A : B;                       // e_{k+1}, over e_{k-1} unless that is R
+            const rc_status st = launch_pair<Pol, TS, TC, W, IX, TM>(ctx, pol, n, nseg, ld, groups, xk1, z, y, y1, ta,
+                                                                     tb, k == 2 ? s_zero(TC()) : tm1, R, sig + k * ld,
+                                                                     sig + (k + 1) * ld, pf_z, pf_x, band, pscr);
+            if (st != RC_OK) return st;
+            k += 2;
+            continue;
+          }
+        }
         launch_step<Pol, TS, TC, W, IX, true, TM>(ctx, pol, n, nseg, ld, groups, xk1, z, y, ta, tb,
                                                   k == 2 ? s_zero(TC()) : tm1, pf_z, pf_x, R, sig + k * ld, so);
+        ++k;
     }
     RC_CU(ctx, cudaGetLastError());
     step_mark(ctx);
@@ -431,12 +576,12 @@ static rc_status run_rm_corr(rc_ctx* ctx, const Pol& pol, int64_t n, TV* V, int6
             const int64_t total = n * (ro.ldf / 2);
             const unsigned grid = (unsigned)std::min<int64_t>((total + 255) / 256, (int64_t)ctx->sm_count * 16);
             corr_to_rm_kernel<TM><<<grid, 256, 0, ctx->stream>>>(n, s, ro.yrm, ro.ldy, em, ld, ro.vf, ro.ldf, coef,
-                                                                 a / (double)(degree + 1));
+                                                                 a / (double)(degree + 1), fail);
         }
     } else {
         const dim3 tgrid((unsigned)((n + 31) / 32), (unsigned)((s + 31) / 32)), tblk(32, 8);
         corr_to_cm_kernel<TM, TV><<<tgrid, tblk, 0, ctx->stream>>>(n, s, em, ld, V, ldv, coef,
-                                                                   a / (double)(degree + 1));
+                                                                   a / (double)(degree + 1), fail);
     }
     ctx->launches++;
     RC_CU(ctx, cudaGetLastError());

@@ -78,6 +78,11 @@ struct rc_ctx {
     // Rayleigh-Ritz of the correction filter's output on row-major blocks (the filtered block and
     // W = A V formed row-major, no transposes): 1 (default) or 0, from RCB200_RM_RR.
     int rm_rr = 1;
+    // Correction-filter degree steps two per launch (rm_corr2_kernel): 1, or 0 (default: one step per
+    // launch, measured faster on the 128^3 CSR workload and equal on the stencil form), from
+    // RCB200_CORR_PAIR; pair_launches counts those launches.
+    int corr_pair = 0;
+    int64_t pair_launches = 0;
     int64_t staged_launches = 0;
     // staged step shape: rows per chunk (multiple of 4) and pipeline stages; 0 = the largest that
     // fit. RCB200_STAGED_ROWS, RCB200_STAGED_STAGES.
@@ -99,7 +104,7 @@ struct rc_ctx {
 
 enum Slot {
     S_V = 0, S_W, S_T1, S_T2, S_FOUND, S_PART, S_SMALL, S_LANCZOS, S_RPART, S_IO, S_CB, S_EIG, S_FA, S_FB,
-    S_R32, S_CORR, S_YRM, S_BATCH, S_VFRM, S_WRM, S_COUNT
+    S_R32, S_CORR, S_YRM, S_BATCH, S_VFRM, S_WRM, S_PAIR, S_COUNT
 };
 
 struct rc_op {

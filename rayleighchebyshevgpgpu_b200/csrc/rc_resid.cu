@@ -109,11 +109,14 @@ __device__ __forceinline__ void resid_rows27(const StencilRows<double, double, 2
     }
 }
 
-// 4 resident CTAs per SM (64 registers): the residual epilogue keeps per-column sums in registers,
-// which spill at the filter steps' 40 (the Ritz values are re-read from L1 per row). T = double
-// (real) or double2 (complex).
+// RC_RESID_MIN_BLOCKS resident CTAs per SM (default 4, 64 registers): the residual epilogue keeps
+// per-column sums in registers, which spill at the filter steps' 40 (the Ritz values are re-read from
+// L1 per row). T = double (real) or double2 (complex).
+#ifndef RC_RESID_MIN_BLOCKS
+#define RC_RESID_MIN_BLOCKS 4
+#endif
 template <class Pol, class T, int W, class IX>
-__global__ void __launch_bounds__(kRmThreads, 4)
+__global__ void __launch_bounds__(kRmThreads, RC_RESID_MIN_BLOCKS)
 resid_rm_kernel(Pol op, int64_t n, int64_t s, int nseg, int64_t ld, int groups, const T* __restrict__ Y,
                 const double* __restrict__ lam, int res_count, double* __restrict__ part, void* __restrict__ Rout,
                 int64_t ldr) {

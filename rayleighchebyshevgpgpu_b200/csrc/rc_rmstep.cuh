@@ -85,6 +85,11 @@ template <class TS, class TM>
 __device__ __forceinline__ Slice<TS, TM> ldv_ro(const TM* p) {
     return slice_from<TS, TM>(__ldg(reinterpret_cast<const uint4*>(p)));
 }
+// The same through L2 only (ld.global.cg): for blocks that other CTAs write during the kernel.
+template <class TS, class TM>
+__device__ __forceinline__ Slice<TS, TM> ldv_cg(const TM* p) {
+    return slice_from<TS, TM>(__ldcg(reinterpret_cast<const uint4*>(p)));
+}
 template <class TS, class TM>
 __device__ __forceinline__ Slice<TS, TM> ldv(const TM* p) {
     return slice_from<TS, TM>(*reinterpret_cast<const uint4*>(p));
@@ -187,7 +192,10 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
 // SRC (the correction filter): y also gets sig[c] * src(i, c), where src is a row-major block
 // with the same leading dimension and sig holds one coefficient per column (ld entries).
 // TM: element type of x, z, y and src in memory (TS, or bfloat16 for FP32 steps).
-template <class Pol, class TS, class TC, int W, class IX, bool SRC = false, class TM = TS>
+// ZCG: z is read through L2 only (ld.global.cg), so that no SM holds a line of it in L1 when other
+// CTAs of the same kernel overwrite it (the first step of rm_corr2_kernel, whose result the second
+// step gathers through the read-only path).
+template <class Pol, class TS, class TC, int W, class IX, bool SRC = false, class TM = TS, bool ZCG = false>
 __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg, int64_t ld, int groups, int64_t cta,
                                              const TM* __restrict__ x, const TM* z, TM* y, TC alpha, TC beta,
                                              TC gamma, int64_t pf_z, int64_t pf_x,
@@ -263,7 +271,8 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
             Slice<TS, TM> out;
             if constexpr (SRC && kPacked) {
                 const Slice<TS, TM> si = ldv_ro<TS, TM>(src + o);
-                const Slice<TS, TM> zi = z ? ldv<TS, TM>(z + o) : Slice<TS, TM>{};
+                const Slice<TS, TM> zi =
+                    z ? (ZCG ? ldv_cg<TS, TM>(z + o) : ldv<TS, TM>(z + o)) : Slice<TS, TM>{};
                 const float* sgp = sig + off + w * wstride;
 #pragma unroll
                 for (int v = 0; v < V; v += 2) {
@@ -278,7 +287,8 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
                 }
             } else if constexpr (kCplxSrc) {
                 const Slice<TS, TM> si = ldv_ro<TS, TM>(src + o);
-                const Slice<TS, TM> zi = z ? ldv<TS, TM>(z + o) : Slice<TS, TM>{};
+                const Slice<TS, TM> zi =
+                    z ? (ZCG ? ldv_cg<TS, TM>(z + o) : ldv<TS, TM>(z + o)) : Slice<TS, TM>{};
 #pragma unroll
                 for (int v = 0; v < V; ++v) {
                     const float sgv = __ldg(sig + off + w * wstride + v);
@@ -291,7 +301,8 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
                 }
             } else if (SRC) {
                 const Slice<TS, TM> si = ldv_ro<TS, TM>(src + o);
-                const Slice<TS, TM> zi = z ? ldv<TS, TM>(z + o) : Slice<TS, TM>{};
+                const Slice<TS, TM> zi =
+                    z ? (ZCG ? ldv_cg<TS, TM>(z + o) : ldv<TS, TM>(z + o)) : Slice<TS, TM>{};
 #pragma unroll
                 for (int v = 0; v < V; ++v) {
                     TC r = s_mul(alpha, acc[w * V + v]);

@@ -207,3 +207,37 @@ def test_correction_filter_rejects_unsupported(ctx):
         R.filter_correction(ctx, op, Vd, s, np.zeros(s), 3, 0.1, 1.0)
     assert e.value.status == 8  # RC_ERR_UNSUPPORTED
     op.close()
+
+
+@pytest.mark.parametrize("name", ["csr7", "st7", "st5", "cst7", "ccsr7"])
+@pytest.mark.parametrize("m", [3, 8, 13])
+def test_two_step_kernel_equals_one_step_launches_bitwise(name, m):
+    """The correction filter's degree steps two per launch (rm_corr2_kernel: phase A of a block, phase B
+    of a block behind it, ordered by per-group completion counters) give the same bits as one launch
+    per step (RCB200_CORR_PAIR=0): the same arithmetic per row, e_k read back before DRAM. Odd and even
+    step counts (the last step of an even count runs alone)."""
+    import os
+    import torch
+    Q, A, w, U = _problem(name)
+    s = 24 if name.startswith("c") else 40
+    Y, lam, rn = _ritz_pairs(A, U, s, 1e-5, seed=m)
+    g1, g2 = _coefficients(w, s, m)
+    out = []
+    for flag in ("1", "0"):
+        old = os.environ.get("RCB200_CORR_PAIR")
+        os.environ["RCB200_CORR_PAIR"] = flag
+        try:
+            c = R.Context(0)
+        finally:
+            if old is None:
+                os.environ.pop("RCB200_CORR_PAIR", None)
+            else:
+                os.environ["RCB200_CORR_PAIR"] = old
+        op = _op(c, Q, name)
+        got = _gpu(c, op, Y, s, lam, m, g1, g2)
+        assert (c.counter("pair_launches") > 0) == (flag == "1")
+        out.append(got)
+        op.close()
+        c.close()
+    assert np.array_equal(out[0], out[1])
+    _check(A, Y, lam, rn, m, g1, g2, out[0])
