@@ -41,6 +41,28 @@ def build_ref(reference_dir: str | None = None, targets=("_ref/ref_harness",)) -
 CONTAINERS_BIN = os.path.join(ORACLE_DIR, "_ref", "lmcuda_reference_containers")
 
 
+GPU_SOLVE_BIN = os.path.join(ORACLE_DIR, "_ref", "ref_gpu_solve")
+
+
+def build_gpu_solve(reference_dir: str | None = None) -> bool:
+    """The reference's own FP64 GPU solver on a cuSPARSE operator (oracle/ref_gpu_solve.cu)."""
+    if reference_present(reference_dir):
+        build_ref(reference_dir, targets=("_ref/ref_gpu_solve",))
+    return os.path.exists(GPU_SOLVE_BIN)
+
+
+def run_gpu_solve(problem_path: str, k: int, incr: int, buffer: int, tol: float, repeats: int = 1,
+                  timeout: float = 1800) -> dict:
+    """Run the reference's GPU solver on a problem file; its JSON line as a dict."""
+    if not os.path.exists(GPU_SOLVE_BIN):
+        raise RuntimeError("oracle/_ref/ref_gpu_solve is not built")
+    cmd = [GPU_SOLVE_BIN, problem_path, str(k), str(incr), str(buffer), repr(float(tol)), str(repeats)]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(f"ref_gpu_solve failed ({r.returncode}): {r.stderr[-2000:]}")
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
 def build_containers_driver(reference_dir: str | None = None) -> bool:
     """The drop-in driver over the reference's own containers (needs the built library)."""
     if reference_present(reference_dir):
