@@ -75,7 +75,8 @@ rc_status rc_ctx_synchronize(rc_ctx* ctx);
 rc_status rc_ctx_launch_count(rc_ctx* ctx, int64_t* launches, int reset);
 /* A named counter of ctx since creation: "launches" (as rc_ctx_launch_count), "staged_launches"
  * (degree steps that ran with their operands staged in shared memory by asynchronous copies),
- * "pair_launches" (launches that ran two correction-filter degree steps in one pass). */
+ * "pair_launches" (launches that ran two correction-filter degree steps in one pass),
+ * "jacobi_sweeps" (Jacobi sweeps of the last rc_small_eigh call). */
 rc_status rc_ctx_counter(rc_ctx* ctx, const char* name, int64_t* value);
 /* Device bytes currently held by ctx (workspaces + operators created on it). */
 rc_status rc_ctx_device_bytes(rc_ctx* ctx, int64_t* bytes);
@@ -233,7 +234,7 @@ rc_status rc_small_eigh(rc_ctx* ctx, int dtype, int64_t s, const void* H, double
  * device-memory budget negotiated at start-up, where a cudaMalloc can fail or take memory another
  * tenant of the GPU counts on, and callbacks invoked from another library's allocator or from an
  * operator apply(), where allocating would re-enter that library. Same arguments and results, but
- * the device staging and work memory come from one fixed array of this library (about 1 MiB, held
+ * the device staging and work memory come from one fixed array of this library (about 1.3 MiB, held
  * on every GPU that loads the library until the process exits), and no cudaMalloc/cudaFree is
  * called. s must be at most 128 (RC_ERR_INVALID otherwise). The first call on a device (and the
  * first after its CUDA context is re-created) looks up the array's device address, which may load

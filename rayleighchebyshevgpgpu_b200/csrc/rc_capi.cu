@@ -141,6 +141,11 @@ rc_status rc_ctx_create(int device, rc_ctx** out) {
     }
     if (const char* v = std::getenv("RCB200_STAGED")) c->staged = std::atoi(v) != 0 ? 1 : 0;
     if (const char* v = std::getenv("RCB200_JACOBI_CTAS")) c->jacobi_ctas = std::max(0, std::atoi(v));
+    if (const char* v = std::getenv("RCB200_JACOBI_THREADS")) {
+        // whole warps, 64 to 1024
+        const int t = std::atoi(v) / 32 * 32;
+        c->jacobi_threads = t >= 64 && t <= 1024 ? t : 0;
+    }
     if (const char* v = std::getenv("RCB200_RM_RR")) c->rm_rr = std::atoi(v) != 0 ? 1 : 0;
     if (const char* v = std::getenv("RCB200_CORR_PAIR")) c->corr_pair = std::atoi(v) != 0 ? 1 : 0;
     if (const char* v = std::getenv("RCB200_STAGED_ROWS")) c->staged_rows = std::max(0, std::atoi(v) / 4 * 4);
@@ -194,6 +199,7 @@ rc_status rc_ctx_counter(rc_ctx* ctx, const char* name, int64_t* value) {
     if (!std::strcmp(name, "launches")) *value = ctx->launches;
     else if (!std::strcmp(name, "staged_launches")) *value = ctx->staged_launches;
     else if (!std::strcmp(name, "pair_launches")) *value = ctx->pair_launches;
+    else if (!std::strcmp(name, "jacobi_sweeps")) *value = ctx->jacobi_sweeps;
     else return rc_fail(ctx, RC_ERR_INVALID, std::string("rc_ctx_counter: unknown counter ") + name);
     return RC_OK;
 }
@@ -553,7 +559,10 @@ rc_status rc_small_eigh(rc_ctx* ctx, int dtype, int64_t s, const void* H, double
     RC_TRY(rcb::small_eigh(ctx, dtype, s, Hd, Qd, dl, di));
     RC_CU(ctx, cudaMemcpyAsync(evals, dl, s * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     if (Q) RC_CU(ctx, cudaMemcpyAsync(Q, Qd, mat, cudaMemcpyDeviceToHost, ctx->stream));
+    int sweeps = 0;
+    RC_CU(ctx, cudaMemcpyAsync(&sweeps, di, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     RC_CU(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->jacobi_sweeps = sweeps;
     return RC_OK;
 }
 

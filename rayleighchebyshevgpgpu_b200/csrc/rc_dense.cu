@@ -485,6 +485,40 @@ __device__ __forceinline__ void rr_pair(int r, int i, int M, int sp, int& p, int
     }
 }
 
+// Whether pair (p, q) rotates: |a_pq| above the absolute and the relative threshold.
+template <class T>
+__device__ __forceinline__ bool jac_rotates(T apq, double app, double aqq, double abs_tol, double rel_tol) {
+    if constexpr (!IsComplex<T>::value) {
+        const double mag = fabs(s_real(apq));
+        return mag > abs_tol && mag * mag > rel_tol * rel_tol * fabs(app * aqq);
+    } else {
+        const double mag = sqrt(s_abs2(apq));
+        return mag > abs_tol && mag > rel_tol * sqrt(fabs(app * aqq));
+    }
+}
+
+// Whether any pair of the s x s working copy A (leading dimension ld) would rotate: if none does, a
+// sweep would change nothing. All threads of the CTA call it and get the same answer.
+template <class T>
+__device__ __forceinline__ bool jac_any_rotation(const T* A, int s, int ld, double abs_tol, double rel_tol) {
+    int any = 0;
+    for (int e = threadIdx.x; e < s * s; e += blockDim.x) {
+        const int p = e % s, q = e / s;
+        if (p < q && jac_rotates<T>(A[p + q * ld], s_real(A[p + p * ld]), s_real(A[q + q * ld]), abs_tol, rel_tol))
+            any = 1;
+    }
+    return __syncthreads_or(any) != 0;
+}
+
+// Upper-triangle block index e -> (bi, bj), bi <= bj, bj-major: e = bj (bj + 1) / 2 + bi.
+__device__ __forceinline__ void jac_tri(int e, int& bi, int& bj) {
+    int j = (int)((sqrtf(8.0f * (float)e + 1.0f) - 1.0f) * 0.5f);
+    while ((j + 1) * (j + 2) / 2 <= e) ++j;
+    while (j * (j + 1) / 2 > e) --j;
+    bj = j;
+    bi = e - j * (j + 1) / 2;
+}
+
 // Rotation angle of pair (p, q) from a_pq, a_pp, a_qq; *sn = 0 (no rotation) when |a_pq| is below
 // the absolute or relative threshold.
 template <class T>
@@ -493,11 +527,12 @@ __device__ __forceinline__ void jac_angle(T apq, double app, double aqq, double 
     c = 1.0;
     sn = 0.0;
     u = s_from<T>(1.0, 0.0);
+    if (!jac_rotates<T>(apq, app, aqq, abs_tol, rel_tol)) return;
     if constexpr (!IsComplex<T>::value) {
         // real: u = sign(apq), and the angle from one square root and one division,
         // t = sign(d) 2|apq| / (|d| + sqrt(d^2 + 4 apq^2)) with d = aqq - app
         const double mag = fabs(s_real(apq));
-        if (mag > abs_tol && mag * mag > rel_tol * rel_tol * fabs(app * aqq)) {
+        {
             u = s_from<T>(s_real(apq) >= 0.0 ? 1.0 : -1.0, 0.0);
             const double d = aqq - app;
             const double t = copysign(2.0 * mag, d) / (fabs(d) + sqrt(d * d + 4.0 * mag * mag));
@@ -506,7 +541,7 @@ __device__ __forceinline__ void jac_angle(T apq, double app, double aqq, double 
         }
     } else {
         const double mag = sqrt(s_abs2(apq));
-        if (mag > abs_tol && mag > rel_tol * sqrt(fabs(app * aqq))) {
+        {
             u = s_rscale(1.0 / mag, apq);
             const double tau = (aqq - app) / (2.0 * mag);
             const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
@@ -575,7 +610,6 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
     }
     Q = A + (size_t)sp * ld;
     const int tid = threadIdx.x, nt = blockDim.x;
-    const int tx = tid & 31, ty = tid >> 5, nwy = nt >> 5;  // lanes walk rows, warps walk columns
     for (int e = tid; e < sp * sp; e += nt) {
         const int i = e % sp, j = e / sp;
         A[i + j * ld] = (i < s && j < s) ? Ain[i + (int64_t)j * s] : s_zero(T());
@@ -595,7 +629,10 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
     const double rel_tol = 1e-15;
     const int M = sp - 1;
     int sweep = 0;
+    const int nblk = npair * (npair + 1) / 2;  // 2x2 blocks with bi <= bj
     for (; sweep < max_sweeps; ++sweep) {
+        // a sweep in which no pair rotates changes nothing: stop before it
+        if (!jac_any_rotation<T>(A, s, ld, abs_tol, rel_tol)) break;
         if (tid == 0) {
             s_rot = 0;
             s_maxsn = 0ull;
@@ -630,9 +667,11 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
             }
             __syncthreads();
             // A <- G^H A G on 2x2 blocks (row pair bi, column pair bj); A stays Hermitian, so
-            // only the blocks with bi <= bj are formed and each is mirrored into (bj, bi)
-            for (int bj = ty; bj < npair; bj += nwy)
-            for (int bi = tx; bi <= bj; bi += 32) {
+            // only the blocks with bi <= bj are formed and each is mirrored into (bj, bi). The
+            // blocks are spread evenly over the threads (bj-major upper-triangle order).
+            for (int e = tid; e < nblk; e += nt) {
+                int bi, bj;
+                jac_tri(e, bi, bj);
                 const double si = rsn[bi], sj = rsn[bj];
                 if (si == 0.0 && sj == 0.0) continue;
                 const int pi = pp[bi], qi = qq[bi], pj = pp[bj], qj = qq[bj];
@@ -650,9 +689,10 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
                     A[qj + qi * ld] = s_conj(a_qq);
                 }
             }
-            // Q <- Q G_j (columns p_j, q_j of rows 0..s-1)
-            for (int bj = ty; bj < npair; bj += nwy)
-            for (int row = tx; row < s; row += 32) {
+            // Q <- Q G_j (columns p_j, q_j of rows 0..s-1), the (row, pair) entries spread evenly
+            // over the threads, rows fastest
+            for (int e = tid; e < npair * s; e += nt) {
+                const int bj = e / s, row = e - bj * s;
                 const double sj = rsn[bj];
                 if (sj == 0.0) continue;
                 const int pj = pp[bj], qj = qq[bj];
@@ -694,7 +734,11 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
 // contiguous share of the 2x2 blocks (bi <= bj) and of the (row, pair) entries of Q, then all CTAs
 // meet at a grid barrier. Every CTA computes all the round's angles itself from the same entries,
 // so the rotations, the convergence test and the number of sweeps agree in every CTA without
-// further communication. Global reads and writes of the working copies bypass L1 (ld/st .cg):
+// further communication. A is kept twice: a round reads one copy and writes every entry of the
+// other (blocks without a rotation are copied), because the CTAs leave the barrier at different
+// times and one CTA's block updates must not reach the entries another CTA is still reading for
+// its angles. Each (row, pair) entry of Q is read and written by one thread only, so Q is kept
+// once. Global reads and writes of the working copies bypass L1 (ld/st .cg):
 // another SM may have written them since the last barrier. The grid is launched cooperatively
 // (all CTAs resident); the barrier's spin is bounded all the same, and on a timeout the kernel
 // stops, writes -1 to info[0] and NaN eigenvalues.
@@ -740,8 +784,9 @@ jacobi_grid_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, doubl
     const int sp = s + (s & 1);
     const int npair = sp / 2;
     const int ld = sp + 1;
-    T* A = work;
-    T* Q = A + (size_t)sp * ld;
+    T* const Abuf[2] = {work, work + (size_t)sp * ld};  // the round's source and destination copies of A
+    T* Q = work + 2 * (size_t)sp * ld;
+    int par = 0;                                        // Abuf[par] holds the current A
     unsigned* bar = reinterpret_cast<unsigned*>(info + 1);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* rc = (double*)smem_raw;
@@ -761,7 +806,7 @@ jacobi_grid_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, doubl
         const int64_t tot = (int64_t)sp * sp;
         for (int64_t e = (int64_t)b * nt + tid; e < tot; e += (int64_t)G * nt) {
             const int i = (int)(e % sp), j = (int)(e / sp);
-            __stcg(A + i + (int64_t)j * ld, (i < s && j < s) ? Ain[i + (int64_t)j * s] : s_zero(T()));
+            __stcg(Abuf[0] + i + (int64_t)j * ld, (i < s && j < s) ? Ain[i + (int64_t)j * s] : s_zero(T()));
             __stcg(Q + i + (int64_t)j * ld, s_from<T>(i == j ? 1.0 : 0.0, 0.0));
         }
     }
@@ -779,12 +824,28 @@ jacobi_grid_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, doubl
     ok = jac_grid_barrier(bar, G, gen);
     int sweep = 0;
     for (; ok && sweep < max_sweeps; ++sweep) {
+        // a sweep in which no pair rotates changes nothing: stop before it (every CTA reads the same
+        // entries, written before the last barrier and not again before the next one, so all stop
+        // together)
+        {
+            const T* A = Abuf[par];
+            int any = 0;
+            for (int e = tid; e < s * s; e += nt) {
+                const int p = e % s, q = e / s;
+                if (p < q && jac_rotates<T>(__ldcg(A + p + (int64_t)q * ld), s_real(__ldcg(A + p + (int64_t)p * ld)),
+                                            s_real(__ldcg(A + q + (int64_t)q * ld)), abs_tol, rel_tol))
+                    any = 1;
+            }
+            if (!__syncthreads_or(any)) break;
+        }
         if (tid == 0) {
             s_rot = 0;
             s_maxsn = 0ull;
         }
         __syncthreads();
         for (int r = 0; r < M && ok; ++r) {
+            const T* A = Abuf[par];   // read by every CTA during this round, written by none
+            T* An = Abuf[par ^ 1];    // this round's result
             unsigned long long snbits = 0ull;
             for (int i = tid; i < npair; i += nt) {
                 int p, q;
@@ -819,23 +880,36 @@ jacobi_grid_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, doubl
                 while ((int64_t)bj * (bj + 1) / 2 > e) --bj;
                 const int bi = (int)(e - (int64_t)bj * (bj + 1) / 2);
                 const double si = rsn[bi], sj = rsn[bj];
-                if (si == 0.0 && sj == 0.0) continue;
                 const int pi = pp[bi], qi = qq[bi], pj = pp[bj], qj = qq[bj];
-                T* a0 = A + pi + (int64_t)pj * ld;
-                T* a1 = A + qi + (int64_t)pj * ld;
-                T* a2 = A + pi + (int64_t)qj * ld;
-                T* a3 = A + qi + (int64_t)qj * ld;
-                T a_pp = __ldcg(a0), a_qp = __ldcg(a1), a_pq = __ldcg(a2), a_qq = __ldcg(a3);
+                const int64_t o0 = pi + (int64_t)pj * ld, o1 = qi + (int64_t)pj * ld;
+                const int64_t o2 = pi + (int64_t)qj * ld, o3 = qi + (int64_t)qj * ld;
+                T a_pp = __ldcg(A + o0), a_qp = __ldcg(A + o1), a_pq = __ldcg(A + o2), a_qq = __ldcg(A + o3);
+                const int64_t m0 = pj + (int64_t)pi * ld, m1 = pj + (int64_t)qi * ld;
+                const int64_t m2 = qj + (int64_t)pi * ld, m3 = qj + (int64_t)qi * ld;
+                if (si == 0.0 && sj == 0.0) {
+                    // no rotation touches this block: both halves carried over unchanged
+                    __stcg(An + o0, a_pp);
+                    __stcg(An + o1, a_qp);
+                    __stcg(An + o2, a_pq);
+                    __stcg(An + o3, a_qq);
+                    if (bi != bj) {
+                        __stcg(An + m0, __ldcg(A + m0));
+                        __stcg(An + m1, __ldcg(A + m1));
+                        __stcg(An + m2, __ldcg(A + m2));
+                        __stcg(An + m3, __ldcg(A + m3));
+                    }
+                    continue;
+                }
                 jac_block<T>(a_pp, a_qp, a_pq, a_qq, rc[bi], si, ru[bi], rc[bj], sj, ru[bj], bi == bj);
-                __stcg(a0, a_pp);
-                __stcg(a1, a_qp);
-                __stcg(a2, a_pq);
-                __stcg(a3, a_qq);
+                __stcg(An + o0, a_pp);
+                __stcg(An + o1, a_qp);
+                __stcg(An + o2, a_pq);
+                __stcg(An + o3, a_qq);
                 if (bi != bj) {
-                    __stcg(A + pj + (int64_t)pi * ld, s_conj(a_pp));
-                    __stcg(A + pj + (int64_t)qi * ld, s_conj(a_qp));
-                    __stcg(A + qj + (int64_t)pi * ld, s_conj(a_pq));
-                    __stcg(A + qj + (int64_t)qi * ld, s_conj(a_qq));
+                    __stcg(An + m0, s_conj(a_pp));
+                    __stcg(An + m1, s_conj(a_qp));
+                    __stcg(An + m2, s_conj(a_pq));
+                    __stcg(An + m3, s_conj(a_qq));
                 }
             }
             // this CTA's (row, pair) entries of Q <- Q G_j, rows fastest (coalesced columns)
@@ -851,6 +925,7 @@ jacobi_grid_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, doubl
                 __stcg(qqp, qv);
             }
             ok = jac_grid_barrier(bar, G, gen);
+            par ^= 1;
         }
         const int rot = s_rot;
         const double maxsn = __longlong_as_double((long long)s_maxsn);
@@ -867,6 +942,7 @@ jacobi_grid_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, doubl
         return;
     }
     // ascending order (rank sort, ties by index); CTA b writes the columns i = b, b + G, ...
+    const T* A = Abuf[par];
     for (int i = b; i < s; i += G) {
         const double li = s_real(__ldcg(A + i + (int64_t)i * ld));
         int rank = 0;
@@ -887,7 +963,8 @@ size_t small_eigh_work_bytes(rc_ctx* ctx, int dtype, int64_t s) {
     const int64_t npair = sp / 2;
     const size_t head = (((size_t)npair * (16 + esz + 8) + 15) / 16) * 16;
     const size_t mats = 2 * (size_t)sp * (sp + 1) * esz;
-    return head + mats <= (size_t)ctx->smem_optin - 2048 ? 0 : mats;
+    // in global memory the grid form keeps A twice (3 matrices); the one-CTA kernel uses 2 of them
+    return head + mats <= (size_t)ctx->smem_optin - 2048 ? 0 : 3 * (size_t)sp * (sp + 1) * esz;
 }
 
 rc_status small_eigh(rc_ctx* ctx, int dtype, int64_t s, void* A, void* Q, double* evals, int* info) {
@@ -922,15 +999,16 @@ rc_status small_eigh_work(rc_ctx* ctx, int dtype, int64_t s, void* A, void* Q, d
         ctx->launches++;
         return RC_OK;
     }
+    const int nthr = ctx->jacobi_threads > 0 ? ctx->jacobi_threads : RC_JACOBI_THREADS;
     if (dtype == RC_COMPLEX128) {
         if (dyn > 48 * 1024)
             RC_CU(ctx, allow_max_smem(ctx, jacobi_kernel<double2>));
-        jacobi_kernel<double2><<<1, RC_JACOBI_THREADS, dyn, ctx->stream>>>((int)s, (const double2*)A, (double2*)Q, evals, info,
+        jacobi_kernel<double2><<<1, nthr, dyn, ctx->stream>>>((int)s, (const double2*)A, (double2*)Q, evals, info,
                                                               (double2*)work, fit ? 1 : 0, sweeps);
     } else {
         if (dyn > 48 * 1024)
             RC_CU(ctx, allow_max_smem(ctx, jacobi_kernel<double>));
-        jacobi_kernel<double><<<1, RC_JACOBI_THREADS, dyn, ctx->stream>>>((int)s, (const double*)A, (double*)Q, evals, info,
+        jacobi_kernel<double><<<1, nthr, dyn, ctx->stream>>>((int)s, (const double*)A, (double*)Q, evals, info,
                                                              (double*)work, fit ? 1 : 0, sweeps);
     }
     ctx->launches++;

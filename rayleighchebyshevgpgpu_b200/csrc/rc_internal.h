@@ -75,6 +75,10 @@ struct rc_ctx {
     // CTAs of the Jacobi eigensolve when its working copies live in global memory (0 = 32; 1 = the
     // one-CTA kernel), from RCB200_JACOBI_CTAS.
     int jacobi_ctas = 0;
+    // Threads of the one-CTA Jacobi kernel (0 = 1024), from RCB200_JACOBI_THREADS; jacobi_sweeps is
+    // the number of sweeps the last rc_small_eigh call ran.
+    int jacobi_threads = 0;
+    int64_t jacobi_sweeps = 0;
     // Rayleigh-Ritz of the correction filter's output on row-major blocks (the filtered block and
     // W = A V formed row-major, no transposes): 1 (default) or 0, from RCB200_RM_RR.
     int rm_rr = 1;

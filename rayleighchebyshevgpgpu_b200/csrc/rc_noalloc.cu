@@ -7,7 +7,7 @@
 // cudaMalloc there can fail or push another tenant of the GPU out of memory), and callbacks
 // invoked from another library's allocator or from an operator apply(), where allocating again
 // would re-enter that library. For them, rc_small_eigh_noalloc uses one file-scope device array
-// of fixed size instead (about 1 MiB on every GPU that loads this library, held until the
+// of fixed size instead (about 1.3 MiB on every GPU that loads this library, held until the
 // process exits) and calls no cudaMalloc or cudaFree.
 //
 // Set-up: the first call on a device (and the first after that device's CUDA context was
@@ -25,7 +25,7 @@ constexpr int64_t kNoAllocMaxS = 128;                                      // la
 constexpr size_t kEsz = 16;                                                // complex double (the wider scalar)
 constexpr size_t kMat = (size_t)kNoAllocMaxS * kNoAllocMaxS * kEsz;       // staging for H and for Q
 constexpr size_t kEvals = (size_t)kNoAllocMaxS * sizeof(double) + 256;     // eigenvalues + sweep count
-constexpr size_t kWork = 2 * (size_t)kNoAllocMaxS * (kNoAllocMaxS + 1) * kEsz;  // Jacobi working copies
+constexpr size_t kWork = 3 * (size_t)kNoAllocMaxS * (kNoAllocMaxS + 1) * kEsz;  // Jacobi working copies (A twice, Q)
 constexpr size_t kScratchBytes = 2 * kMat + kEvals + kWork;
 
 // Shared by every call on a device; calls whose work overlaps on the GPU race on it.

@@ -210,6 +210,35 @@ def test_grid_jacobi_matches_one_cta_kernel(complex_):
     np.testing.assert_allclose(out[0], out[1], atol=1e-14)
 
 
+@pytest.mark.parametrize("s,complex_", [(200, False), (128, True)])
+def test_grid_jacobi_is_repeatable(ctx, s, complex_):
+    """The grid Jacobi's CTAs leave each barrier at different times; a round reads one copy of A and
+    writes the other, so no CTA's angles can see another CTA's updates of the same round. Repeated
+    calls on the same matrix must then give bitwise the same eigenvalues and vectors."""
+    rng = np.random.default_rng(s + 3)
+    H = rng.standard_normal((s, s)) + (1j * rng.standard_normal((s, s)) if complex_ else 0)
+    H = H + H.conj().T
+    ev0, Q0 = R.small_eigh(ctx, H)
+    ref = np.linalg.eigvalsh(H)
+    assert np.abs(ev0 - ref).max() < 1e-13 * np.abs(ref).max() * s
+    for _ in range(40):
+        ev, Qm = R.small_eigh(ctx, H)
+        assert np.array_equal(ev, ev0)
+        assert np.array_equal(Qm, Q0)
+
+
+def test_small_eigh_sweep_counter(ctx):
+    """rc_ctx_counter("jacobi_sweeps") reports the sweeps of the last call: a diagonal matrix needs
+    none, a random one several."""
+    s = 40
+    R.small_eigh(ctx, np.diag(np.arange(1.0, s + 1.0)))
+    assert ctx.counter("jacobi_sweeps") == 0
+    rng = np.random.default_rng(5)
+    H = rng.standard_normal((s, s))
+    R.small_eigh(ctx, H + H.T)
+    assert 3 <= ctx.counter("jacobi_sweeps") <= 20
+
+
 def test_rayleigh_ritz_matches_dense(ctx):
     Q = problems.small_laplacian((14, 13, 12), seed=8)
     A = O.csr_matrix(*Q.csr())
