@@ -19,12 +19,24 @@
 namespace rcb {
 
 // Two FP32 values of the residual block at p: two real columns, or the real and imaginary part of
-// one complex column.
+// one complex column. Written once: evict-first when RC_STREAM_HINTS is 1 (by default these
+// bfloat16 or FP32 stores take no hint, as the correction filter's blocks).
 __device__ __forceinline__ void corr_store2(void* p, float a, float b) {
 #if RC_CORR_BF16
-    *reinterpret_cast<__nv_bfloat162*>(p) = __floats2bfloat162_rn(a, b);
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+#if RC_STREAM_HINTS == 1
+    unsigned u;
+    memcpy(&u, &h, 4);
+    __stcs(reinterpret_cast<unsigned*>(p), u);
+#else
+    *reinterpret_cast<__nv_bfloat162*>(p) = h;
+#endif
+#else
+#if RC_STREAM_HINTS == 1
+    __stcs(reinterpret_cast<float2*>(p), make_float2(a, b));
 #else
     *reinterpret_cast<float2*>(p) = make_float2(a, b);
+#endif
 #endif
 }
 __device__ __forceinline__ double resid_sub(double lm, double y, double acc) { return fma(-lm, y, acc); }

@@ -94,8 +94,30 @@ template <class TS, class TM>
 __device__ __forceinline__ Slice<TS, TM> ldv(const TM* p) {
     return slice_from<TS, TM>(*reinterpret_cast<const uint4*>(p));
 }
+// Blocks that a step reads or writes once (x_{k-2}, the source block, the result) go through the
+// caches with the evict-first policy (ld/st .cs), so that the L1 and L2 lines they take are the
+// first to go and the rows of x_{k-1}, which the gathers of later rows read again, stay. Measured on
+// the 128^3 7-point CSR operator with 96 FP64 columns: the step moves the same DRAM bytes either way
+// (3.46 GB read, 1.6 GB written, its algorithmic traffic), but takes 1.04 ms instead of 1.45 ms.
+// For bfloat16 blocks (the correction filter) the hints made the step about 1 % slower, so by
+// default (RC_STREAM_HINTS 2) only blocks stored in FP64 take them; 1 hints every block, 0 none.
+#ifndef RC_STREAM_HINTS
+#define RC_STREAM_HINTS 2
+#endif
 template <class TS, class TM>
-__device__ __forceinline__ void stv(TM* p, const Slice<TS, TM>& v) {
+constexpr bool stream_hint() {
+    return RC_STREAM_HINTS == 1 ||
+           (RC_STREAM_HINTS == 2 && std::is_same<TS, TM>::value && sizeof(real_t<TS>) == 8);
+}
+template <class TS, class TM>
+__device__ __forceinline__ Slice<TS, TM> ldv_once(const TM* p) {
+    if constexpr (stream_hint<TS, TM>())
+        return slice_from<TS, TM>(__ldcs(reinterpret_cast<const uint4*>(p)));
+    else
+        return slice_from<TS, TM>(*reinterpret_cast<const uint4*>(p));
+}
+template <class TS, class TM>
+__device__ __forceinline__ uint4 slice_pack(const Slice<TS, TM>& v) {
     uint4 u;
     if constexpr (std::is_same<TM, TS>::value) {
         memcpy(&u, &v, 16);
@@ -110,7 +132,18 @@ __device__ __forceinline__ void stv(TM* p, const Slice<TS, TM>& v) {
         u.z = bf2_pack(v.v[4], v.v[5]);
         u.w = bf2_pack(v.v[6], v.v[7]);
     }
-    *reinterpret_cast<uint4*>(p) = u;
+    return u;
+}
+template <class TS, class TM>
+__device__ __forceinline__ void stv(TM* p, const Slice<TS, TM>& v) {
+    *reinterpret_cast<uint4*>(p) = slice_pack<TS, TM>(v);
+}
+template <class TS, class TM>
+__device__ __forceinline__ void stv_once(TM* p, const Slice<TS, TM>& v) {
+    if constexpr (stream_hint<TS, TM>())
+        __stcs(reinterpret_cast<uint4*>(p), slice_pack<TS, TM>(v));
+    else
+        *reinterpret_cast<uint4*>(p) = slice_pack<TS, TM>(v);
 }
 // Two FP32 fused multiply-adds in one packed instruction (sm_100 fma.rn.f32x2): c_q = a_q x_q + c_q
 // rounded as two fmaf, so the packed and scalar forms give the same bits.
@@ -270,9 +303,9 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
             const Slice<TS, TM> xi = ldv_ro<TS, TM>(x + o);
             Slice<TS, TM> out;
             if constexpr (SRC && kPacked) {
-                const Slice<TS, TM> si = ldv_ro<TS, TM>(src + o);
+                const Slice<TS, TM> si = ldv_once<TS, TM>(src + o);
                 const Slice<TS, TM> zi =
-                    z ? (ZCG ? ldv_cg<TS, TM>(z + o) : ldv<TS, TM>(z + o)) : Slice<TS, TM>{};
+                    z ? (ZCG ? ldv_cg<TS, TM>(z + o) : ldv_once<TS, TM>(z + o)) : Slice<TS, TM>{};
                 const float* sgp = sig + off + w * wstride;
 #pragma unroll
                 for (int v = 0; v < V; v += 2) {
@@ -286,9 +319,9 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
                     out.v[v + 1] = r1;
                 }
             } else if constexpr (kCplxSrc) {
-                const Slice<TS, TM> si = ldv_ro<TS, TM>(src + o);
+                const Slice<TS, TM> si = ldv_once<TS, TM>(src + o);
                 const Slice<TS, TM> zi =
-                    z ? (ZCG ? ldv_cg<TS, TM>(z + o) : ldv<TS, TM>(z + o)) : Slice<TS, TM>{};
+                    z ? (ZCG ? ldv_cg<TS, TM>(z + o) : ldv_once<TS, TM>(z + o)) : Slice<TS, TM>{};
 #pragma unroll
                 for (int v = 0; v < V; ++v) {
                     const float sgv = __ldg(sig + off + w * wstride + v);
@@ -300,9 +333,9 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
                     out.v[v] = make_float2(r0, r1);
                 }
             } else if (SRC) {
-                const Slice<TS, TM> si = ldv_ro<TS, TM>(src + o);
+                const Slice<TS, TM> si = ldv_once<TS, TM>(src + o);
                 const Slice<TS, TM> zi =
-                    z ? (ZCG ? ldv_cg<TS, TM>(z + o) : ldv<TS, TM>(z + o)) : Slice<TS, TM>{};
+                    z ? (ZCG ? ldv_cg<TS, TM>(z + o) : ldv_once<TS, TM>(z + o)) : Slice<TS, TM>{};
 #pragma unroll
                 for (int v = 0; v < V; ++v) {
                     TC r = s_mul(alpha, acc[w * V + v]);
@@ -314,7 +347,7 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
                     out.v[v] = s_cvt<TS>(r);
                 }
             } else if (z) {
-                const Slice<TS, TM> zi = ldv<TS, TM>(z + o);
+                const Slice<TS, TM> zi = ldv_once<TS, TM>(z + o);
 #pragma unroll
                 for (int v = 0; v < V; ++v) {
                     TC r = s_mul(alpha, acc[w * V + v]);
@@ -330,7 +363,7 @@ __device__ __forceinline__ void rm_step_rows(const Pol& op, int64_t n, int nseg,
                     out.v[v] = s_cvt<TS>(r);
                 }
             }
-            stv<TS, TM>(y + o, out);
+            stv_once<TS, TM>(y + o, out);
         }
         p0 = p1;
         p1 = p2;
@@ -424,8 +457,8 @@ __device__ __forceinline__ void rm_step_rows27(const StencilRows<TD, TC, 27>& op
             const IX o = oi + w * wstride;
             const Slice<TS, TM> xi = ldv_ro<TS, TM>(x + o);
             Slice<TS, TM> zi{}, si{};
-            if (z) zi = ldv<TS, TM>(z + o);
-            if (SRC) si = ldv_ro<TS, TM>(src + o);
+            if (z) zi = ldv_once<TS, TM>(z + o);
+            if (SRC) si = ldv_once<TS, TM>(src + o);
             Slice<TS, TM> out;
 #pragma unroll
             for (int v = 0; v < V; ++v) {
@@ -442,7 +475,7 @@ __device__ __forceinline__ void rm_step_rows27(const StencilRows<TD, TC, 27>& op
                 }
                 out.v[v] = s_cvt<TS>(r);
             }
-            stv<TS, TM>(y + o, out);
+            stv_once<TS, TM>(y + o, out);
         }
 #pragma unroll
         for (int v = 0; v < W * V; ++v) {
