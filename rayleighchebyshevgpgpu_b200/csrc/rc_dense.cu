@@ -143,6 +143,8 @@ rc_status gram(rc_ctx* ctx, int dtype, int64_t n, int64_t m, int64_t nc, const v
     if (upper && m != nc) return rc_fail(ctx, RC_ERR_INVALID, "gram: upper requires a square result");
     if (upper && gram2_supported(dtype, m))
         return gram2(ctx, n, m, (const double*)X, ldx, (const double*)Y, ldy, (double*)C, nullptr, 0, nullptr);
+    if (upper && ctx->gram_c && gram_c_supported(dtype, m) && (uintptr_t)X % 16 == 0 && (uintptr_t)Y % 16 == 0)
+        return gram_c(ctx, n, m, (const double2*)X, ldx, (const double2*)Y, ldy, (double2*)C);
     if (dtype == RC_COMPLEX128)
         return gram_t<double2>(ctx, n, m, nc, (const double2*)X, ldx, (const double2*)Y, ldy, (double2*)C, upper);
     return gram_t<double>(ctx, n, m, nc, (const double*)X, ldx, (const double*)Y, ldy, (double*)C, upper);

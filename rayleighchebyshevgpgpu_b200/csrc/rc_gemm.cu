@@ -291,6 +291,189 @@ rc_status gram2(rc_ctx* ctx, int64_t n, int64_t m, const double* X, int64_t ldx,
 }
 
 // ---------------------------------------------------------------------------------------
+// gram_c: the complex Hermitian Gram C = X^H Y (m x m, m <= 192) on the same FP64 tensor pipe.
+// A complex column-major block with leading dimension ld is, read as doubles, a real column-major
+// block of 2n rows (real and imaginary part of each entry on consecutive rows) with leading
+// dimension 2 ld. With Xr, Yr those real blocks,
+//   Re C = Xr^T Yr,   Im C = Xr^T (J Yr),   (J Yr)[2r] = Im y_r, (J Yr)[2r+1] = -Re y_r,
+// so both parts are real Gram products over the same shared-memory tiles: the B fragments of the
+// imaginary part are read from row k^1 of the tile and negated on odd rows k (K-tiles start on even
+// rows), which costs no copy. Warp tasks are the upper 32x32 super-blocks of the real part and of
+// the imaginary part (2 x SB(SB+1)/2 tasks); the tasks are split over `groups` CTAs per chunk of
+// rows so that one CTA holds at most 16 warps, and each CTA copies the whole K-tile of X (and of Y,
+// unless Y is X). Per-chunk partials of both parts are summed by gram_c_reduce_kernel in a fixed
+// order (deterministic), which also mirrors C to exact Hermitian symmetry. This replaces the
+// reference's complex cublasZgemm(OP_C, OP_N) of the Rayleigh-Ritz step
+// (RayleighChebyshevLMCuda.h:2139-2161).
+// ---------------------------------------------------------------------------------------
+constexpr int GC_MAX_WARPS = 16;
+
+template <int SB, bool SAME>
+__global__ void __launch_bounds__(32 * GC_MAX_WARPS, 1)
+gram_mma_cplx_kernel(int64_t n2, int m, const double* __restrict__ X, int64_t ldx2, const double* __restrict__ Y,
+                     int64_t ldy2, double* __restrict__ part, int64_t rows, int tpg) {
+    constexpr int NP = SB * (SB + 1) / 2;       // upper super-blocks of one part
+    constexpr int SC = 32 * SB;                 // padded columns
+    constexpr int OPS = SAME ? 1 : 2;           // operand tiles per stage
+    constexpr int OPSZ = SC * GM_KP;            // doubles per operand tile (column by column)
+    constexpr int STAGE = OPS * OPSZ;
+    extern __shared__ __align__(16) double gcs[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int NT = blockDim.x;
+    const int g = lane >> 2, q = lane & 3;
+    const int task = blockIdx.y * tpg + warp;
+    const bool active = task < 2 * NP;
+    const int im = active && task >= NP ? 1 : 0;  // 0: real part, 1: imaginary part
+    int pidx = active ? task - im * NP : 0, bi = 0;
+    while (pidx >= SB - bi) {
+        pidx -= SB - bi;
+        ++bi;
+    }
+    const int bj = bi + pidx;
+    const int64_t r_begin = (int64_t)blockIdx.x * rows;
+    const int64_t r_end = min(n2, r_begin + rows);
+    // zero the padding columns m..SC of every operand of both stages once
+    {
+        const int per = (SC - m) * GM_KP;
+        for (int e = tid; e < 2 * OPS * per; e += NT) {
+            const int op = e / per, f = e - op * per;
+            gcs[op * OPSZ + m * GM_KP + f] = 0.0;
+        }
+    }
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    const int64_t ntiles = r_end > r_begin ? (r_end - r_begin + GM_KT - 1) / GM_KT : 0;
+    auto issue = [&](int64_t t) {
+        double* st = gcs + (t & 1) * STAGE;
+        const int64_t r0 = r_begin + t * GM_KT;
+        load_cols_async<GM_KT, true>(st, GM_KP, X, ldx2, m, r0, r_end, tid, NT);
+        if (!SAME) load_cols_async<GM_KT, true>(st + OPSZ, GM_KP, Y, ldy2, m, r0, r_end, tid, NT);
+    };
+    // B fragment row of this lane (k0 + qb) and its sign: J for the imaginary part
+    const int qb = im ? (q ^ 1) : q;
+    const double sgn = (im && (q & 1)) ? -1.0 : 1.0;
+    if (ntiles > 0) issue(0);
+    cp_async_commit();
+    for (int64_t t = 0; t < ntiles; ++t) {
+        cp_async_wait0();
+        __syncthreads();
+        if (t + 1 < ntiles) issue(t + 1);
+        cp_async_commit();
+        if (active) {
+            const double* st = gcs + (t & 1) * STAGE;
+            const double* xs = st + (bi * 32 + g) * GM_KP + q;
+            const double* ys = st + (SAME ? 0 : OPSZ) + (bj * 32 + g) * GM_KP + qb;
+#pragma unroll
+            for (int k0 = 0; k0 < GM_KT; k0 += 4) {
+                double a[4], b[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) a[i] = xs[i * 8 * GM_KP + k0];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) b[j] = sgn * ys[j * 8 * GM_KP + k0];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+            }
+        }
+    }
+    if (!active) return;
+    double* P = part + ((size_t)im * gridDim.x + blockIdx.x) * (size_t)m * m;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int row = bi * 32 + i * 8 + g, col = bj * 32 + j * 8 + 2 * q + h;
+                if (row < m && col < m) P[row + (int64_t)col * m] = acc[i][j][h];
+            }
+}
+
+// C[i,j] = (sum of the real-part partials, sum of the imaginary-part partials) for i <= j, the
+// diagonal real, mirrored to C[j,i] = conj(C[i,j]).
+__global__ void gram_c_reduce_kernel(int m, int64_t nchunks, const double* __restrict__ part, double2* __restrict__ C) {
+    const int64_t total = (int64_t)m * m;
+    for (int64_t f = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; f < total; f += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(f % m), j = (int)(f / m);
+        if (i > j) continue;
+        double re = 0.0, im = 0.0;
+        const double* pr = part + f;
+        const double* pi = part + (size_t)nchunks * total + f;
+        for (int64_t c = 0; c < nchunks; ++c) {
+            re += pr[(size_t)c * total];
+            im += pi[(size_t)c * total];
+        }
+        if (i == j) im = 0.0;
+        C[f] = make_double2(re, im);
+        C[j + (int64_t)i * m] = make_double2(re, -im);
+    }
+}
+
+bool gram_c_supported(int dtype, int64_t m) { return dtype == RC_COMPLEX128 && m >= 1 && m <= 192; }
+
+template <int SB, bool SAME>
+static rc_status gram_c_launch(rc_ctx* ctx, int64_t n2, int m, const double* X, int64_t ldx2, const double* Y,
+                               int64_t ldy2, double* part, int64_t nchunks, int groups, int tpg, int64_t rows,
+                               size_t smem) {
+    RC_CU(ctx, allow_max_smem(ctx, gram_mma_cplx_kernel<SB, SAME>));
+    gram_mma_cplx_kernel<SB, SAME><<<dim3((unsigned)nchunks, (unsigned)groups), 32 * tpg, smem, ctx->stream>>>(
+        n2, m, X, ldx2, Y, ldy2, part, rows, tpg);
+    return RC_OK;
+}
+
+rc_status gram_c(rc_ctx* ctx, int64_t n, int64_t m, const double2* X, int64_t ldx, const double2* Y, int64_t ldy,
+                 double2* C) {
+    if (!gram_c_supported(RC_COMPLEX128, m)) return rc_fail(ctx, RC_ERR_INVALID, "gram_c: m out of range");
+    const int sb = (int)((m + 31) / 32);
+    const int np = sb * (sb + 1) / 2;
+    const int tasks = 2 * np;
+    const int groups = (tasks + GC_MAX_WARPS - 1) / GC_MAX_WARPS;
+    const int tpg = (tasks + groups - 1) / groups;
+    const bool same = X == Y && ldx == ldy;
+    const int ops = same ? 1 : 2;
+    const size_t smem = (size_t)2 * ops * 32 * sb * GM_KP * sizeof(double);
+    // resident CTAs per SM: by shared memory and by registers (at most 128 per thread)
+    int per_sm = std::max<int>(1, (int)(((size_t)ctx->smem_optin) / (smem + 1024)));
+    per_sm = std::max(1, std::min(per_sm, 65536 / (32 * tpg * 128)));
+    int64_t nchunks = std::max<int64_t>(1, (int64_t)ctx->sm_count * per_sm / groups);
+    const int64_t n2 = 2 * n;
+    int64_t rows = (n2 + nchunks - 1) / nchunks;
+    rows = ((rows + GM_KT - 1) / GM_KT) * GM_KT;
+    nchunks = (n2 + rows - 1) / rows;
+    void* part = nullptr;
+    RC_TRY(rc_slot(ctx, S_PART, (size_t)2 * nchunks * m * m * sizeof(double), &part));
+    const double* xr = reinterpret_cast<const double*>(X);
+    const double* yr = reinterpret_cast<const double*>(Y);
+    double* pp = (double*)part;
+#define RC_GC(SBV)                                                                                               \
+    (same ? gram_c_launch<SBV, true>(ctx, n2, (int)m, xr, 2 * ldx, xr, 2 * ldx, pp, nchunks, groups, tpg, rows, smem) \
+          : gram_c_launch<SBV, false>(ctx, n2, (int)m, xr, 2 * ldx, yr, 2 * ldy, pp, nchunks, groups, tpg, rows, smem))
+    rc_status st;
+    switch (sb) {
+        case 1: st = RC_GC(1); break;
+        case 2: st = RC_GC(2); break;
+        case 3: st = RC_GC(3); break;
+        case 4: st = RC_GC(4); break;
+        case 5: st = RC_GC(5); break;
+        default: st = RC_GC(6); break;
+    }
+#undef RC_GC
+    RC_TRY(st);
+    ctx->launches++;
+    RC_CU(ctx, cudaGetLastError());
+    const int64_t total = m * m;
+    const unsigned gr = (unsigned)std::min<int64_t>((total + 255) / 256, 4 * 148);
+    gram_c_reduce_kernel<<<gr, 256, 0, ctx->stream>>>((int)m, nchunks, (const double*)part, C);
+    ctx->launches++;
+    RC_CU(ctx, cudaGetLastError());
+    return RC_OK;
+}
+
+// ---------------------------------------------------------------------------------------
 // xt2
 // ---------------------------------------------------------------------------------------
 constexpr int XM_RT = 32;         // rows per tile

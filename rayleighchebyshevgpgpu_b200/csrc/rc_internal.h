@@ -78,6 +78,9 @@ struct rc_ctx {
     // Threads of the one-CTA Jacobi kernel (0 = 1024), from RCB200_JACOBI_THREADS; jacobi_sweeps is
     // the number of sweeps the last rc_small_eigh call ran.
     int jacobi_threads = 0;
+    // Complex Hermitian Gram products (m <= 192) on the FP64 tensor pipe (gram_c): 1 (default), or 0
+    // for the FP64 SIMT kernel, from RCB200_GRAM_C.
+    int gram_c = 1;
     int64_t jacobi_sweeps = 0;
     // Rayleigh-Ritz of the correction filter's output on row-major blocks (the filtered block and
     // W = A V formed row-major, no transposes): 1 (default) or 0, from RCB200_RM_RR.
@@ -290,6 +293,11 @@ rc_status xt(rc_ctx* ctx, int dtype, const XtArgs& a);
 // symmetric results. xt2: Y = X T, plus residual norms of W T against lam when W is given, and
 // the residual block W T - Y diag(lam) in row-major FP32 when R32 is given.
 bool gram2_supported(int dtype, int64_t m);
+// Complex Hermitian Gram C = X^H Y (m x m, m <= 192, column-major, upper formed and mirrored) on the
+// FP64 tensor pipe.
+bool gram_c_supported(int dtype, int64_t m);
+rc_status gram_c(rc_ctx* ctx, int64_t n, int64_t m, const double2* X, int64_t ldx, const double2* Y, int64_t ldy,
+                 double2* C);
 rc_status gram2(rc_ctx* ctx, int64_t n, int64_t m, const double* X, int64_t ldx, const double* Y0, int64_t ldy0,
                 double* C0, const double* Y1, int64_t ldy1, double* C1, bool rm = false);
 bool xt2_supported(int dtype, int64_t k, int64_t nc);

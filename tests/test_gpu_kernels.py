@@ -257,6 +257,60 @@ def test_rayleigh_ritz_matches_dense(ctx):
     np.testing.assert_allclose(res, np.linalg.norm(A @ Vn - Vn * ev, axis=0), rtol=1e-8, atol=1e-12)
 
 
+def _ctx_with(env):
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        return R.Context(0)
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+
+
+@pytest.mark.parametrize("s", [17, 40, 96, 150, 192])
+def test_complex_cholqr_block_widths(ctx, s):
+    """Complex Gram G = X^H X on the FP64 tensor pipe (the real view with the pair swap J for the
+    imaginary part), at ragged widths and an odd row count: CholeskyQR2 gives an orthonormal basis of
+    the same span."""
+    rng = np.random.default_rng(s + 100)
+    n = 20011
+    V = (rng.standard_normal((n, s)) + 1j * rng.standard_normal((n, s))) * np.logspace(0, 3, s)
+    Xd = _dev(V.T)
+    R.cholqr(ctx, Xd, n, s, True)
+    Qm = _host(Xd).T
+    assert np.abs(Qm.conj().T @ Qm - np.eye(s)).max() < 1e-12
+    resid = V - Qm @ (Qm.conj().T @ V)
+    assert (np.linalg.norm(resid, axis=0) / np.linalg.norm(V, axis=0)).max() < 1e-10
+
+
+@pytest.mark.parametrize("s", [40, 150, 192])
+def test_complex_rayleigh_ritz_tensor_pipe_matches_dense_and_simt(ctx, s):
+    """H = V^H (A V) for a complex Hermitian operator through rc_rayleigh_ritz: the tensor-pipe Gram
+    gives the eigenvalues of the dense projection, and agrees with the FP64 SIMT Gram
+    (RCB200_GRAM_C=0) to rounding."""
+    Q = problems.small_laplacian((24, 23, 22), seed=s, complex_=True, flux=1 / 17)
+    A = O.csr_matrix(*Q.csr())
+    rng = np.random.default_rng(s)
+    V, _ = np.linalg.qr(rng.standard_normal((Q.n, s)) + 1j * rng.standard_normal((Q.n, s)))
+    H = V.conj().T @ (A @ V)
+    ref_ev = np.linalg.eigvalsh(0.5 * (H + H.conj().T))
+    out = []
+    for c in (ctx, _ctx_with({"RCB200_GRAM_C": "0"})):
+        op = R.operator_from_problem(c, Q, "csr")
+        Vd = _dev(V.T)
+        Wd = _dev(np.zeros((s, Q.n), dtype=np.complex128))
+        ev, res, _ = R.rayleigh_ritz(c, op, Vd, Wd, s, s)
+        np.testing.assert_allclose(ev, ref_ev, rtol=1e-12, atol=1e-12)
+        out.append(ev)
+        op.close()
+        if c is not ctx:
+            c.close()
+    np.testing.assert_allclose(out[0], out[1], rtol=1e-13, atol=1e-13)
+
+
 def test_lanczos_bounds_vs_reference_golden(ctx):
     g = json.load(open(os.path.join(GOLD, "lanczos_config1.json")))
     P = problems.config1()
