@@ -632,6 +632,40 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
     const int M = sp - 1;
     int sweep = 0;
     const int nblk = npair * (npair + 1) / 2;  // 2x2 blocks with bi <= bj
+    // A thread's work is the same in every round: the 2x2 blocks tid, tid + nt, ... of the bj-major
+    // upper triangle (for real matrices the first two mapped here once, any later ones per round;
+    // complex ones, whose updates need more registers, all per round) and the (row, pair) entries
+    // tid, tid + nt, ... of Q, walked by adding nt in (pair, row) form without a division.
+    constexpr int kPre = IsComplex<T>::value ? 0 : 2;
+    int blk_i[2], blk_j[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        blk_i[k] = -1;
+        blk_j[k] = 0;
+        if (k < kPre && tid + k * nt < nblk) jac_tri(tid + k * nt, blk_i[k], blk_j[k]);
+    }
+    const int q_b0 = tid / s, q_r0 = tid - (tid / s) * s;
+    const int q_db = nt / s, q_dr = nt - (nt / s) * s;
+    // A <- G^H A G on the 2x2 block (row pair bi, column pair bj); A stays Hermitian, so only the
+    // blocks with bi <= bj are formed and each is mirrored into (bj, bi)
+    auto block_update = [&](int bi, int bj) {
+        const double si = rsn[bi], sj = rsn[bj];
+        if (si == 0.0 && sj == 0.0) return;
+        const int pi = pp[bi], qi = qq[bi], pj = pp[bj], qj = qq[bj];
+        T a_pp = A[pi + pj * ld], a_qp = A[qi + pj * ld];
+        T a_pq = A[pi + qj * ld], a_qq = A[qi + qj * ld];
+        jac_block<T>(a_pp, a_qp, a_pq, a_qq, rc[bi], si, ru[bi], rc[bj], sj, ru[bj], bi == bj);
+        A[pi + pj * ld] = a_pp;
+        A[qi + pj * ld] = a_qp;
+        A[pi + qj * ld] = a_pq;
+        A[qi + qj * ld] = a_qq;
+        if (bi != bj) {
+            A[pj + pi * ld] = s_conj(a_pp);
+            A[pj + qi * ld] = s_conj(a_qp);
+            A[qj + pi * ld] = s_conj(a_pq);
+            A[qj + qi * ld] = s_conj(a_qq);
+        }
+    };
     for (; sweep < max_sweeps; ++sweep) {
         // a sweep in which no pair rotates changes nothing: stop before it
         if (!jac_any_rotation<T>(A, s, ld, abs_tol, rel_tol)) break;
@@ -668,40 +702,32 @@ jacobi_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, double* __
                 }
             }
             __syncthreads();
-            // A <- G^H A G on 2x2 blocks (row pair bi, column pair bj); A stays Hermitian, so
-            // only the blocks with bi <= bj are formed and each is mirrored into (bj, bi). The
-            // blocks are spread evenly over the threads (bj-major upper-triangle order).
-            for (int e = tid; e < nblk; e += nt) {
+            // the 2x2 blocks, spread evenly over the threads
+#pragma unroll
+            for (int k = 0; k < kPre; ++k)
+                if (blk_i[k] >= 0) block_update(blk_i[k], blk_j[k]);
+            for (int e = tid + kPre * nt; e < nblk; e += nt) {
                 int bi, bj;
                 jac_tri(e, bi, bj);
-                const double si = rsn[bi], sj = rsn[bj];
-                if (si == 0.0 && sj == 0.0) continue;
-                const int pi = pp[bi], qi = qq[bi], pj = pp[bj], qj = qq[bj];
-                T a_pp = A[pi + pj * ld], a_qp = A[qi + pj * ld];
-                T a_pq = A[pi + qj * ld], a_qq = A[qi + qj * ld];
-                jac_block<T>(a_pp, a_qp, a_pq, a_qq, rc[bi], si, ru[bi], rc[bj], sj, ru[bj], bi == bj);
-                A[pi + pj * ld] = a_pp;
-                A[qi + pj * ld] = a_qp;
-                A[pi + qj * ld] = a_pq;
-                A[qi + qj * ld] = a_qq;
-                if (bi != bj) {
-                    A[pj + pi * ld] = s_conj(a_pp);
-                    A[pj + qi * ld] = s_conj(a_qp);
-                    A[qj + pi * ld] = s_conj(a_pq);
-                    A[qj + qi * ld] = s_conj(a_qq);
-                }
+                block_update(bi, bj);
             }
             // Q <- Q G_j (columns p_j, q_j of rows 0..s-1), the (row, pair) entries spread evenly
             // over the threads, rows fastest
-            for (int e = tid; e < npair * s; e += nt) {
-                const int bj = e / s, row = e - bj * s;
+            for (int bj = q_b0, row = q_r0; bj < npair;) {
                 const double sj = rsn[bj];
-                if (sj == 0.0) continue;
-                const int pj = pp[bj], qj = qq[bj];
-                T qp = Q[row + pj * ld], qv = Q[row + qj * ld];
-                jac_qrot<T>(qp, qv, rc[bj], sj, ru[bj]);
-                Q[row + pj * ld] = qp;
-                Q[row + qj * ld] = qv;
+                if (sj != 0.0) {
+                    const int pj = pp[bj], qj = qq[bj];
+                    T qp = Q[row + pj * ld], qv = Q[row + qj * ld];
+                    jac_qrot<T>(qp, qv, rc[bj], sj, ru[bj]);
+                    Q[row + pj * ld] = qp;
+                    Q[row + qj * ld] = qv;
+                }
+                row += q_dr;
+                bj += q_db;
+                if (row >= s) {
+                    row -= s;
+                    ++bj;
+                }
             }
             __syncthreads();
         }
@@ -749,30 +775,44 @@ constexpr int kJacGridThreads = 256;
 constexpr long long kJacBarrierSpins = 1ll << 26;  // ~ seconds with the back-off below
 
 // Grid barrier over `nblocks` CTAs on two words: bar[0] counts arrivals, bar[1] is the generation.
-// Returns false when the wait gave up (and sets bar[2]).
+// Thread 0 arrives with an acquire-release add (after the CTA barrier, it releases the CTA's
+// writes; the last arrival also acquires every other CTA's). The last arrival resets the count and
+// publishes the next generation with a release store; the others poll the generation with acquire
+// loads, so each CTA sees every CTA's writes once it leaves. bar[2] is the give-up flag: a CTA
+// whose wait runs out sets it, and the CTAs waiting at this or a later barrier read it while they
+// poll and stop too. Returns false when this CTA gave up.
+__device__ __forceinline__ unsigned jac_ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned jac_ld_relaxed(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 __device__ __forceinline__ bool jac_grid_barrier(unsigned* bar, unsigned nblocks, unsigned& gen) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        __threadfence();
-        if (atomicAdd(&bar[0], 1u) == nblocks - 1) {
-            atomicExch(&bar[0], 0u);
-            __threadfence();
-            atomicExch(&bar[1], gen + 1);
+        unsigned old;
+        asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(old) : "l"(bar) : "memory");
+        if (old == nblocks - 1) {
+            asm volatile("st.relaxed.gpu.global.u32 [%0], 0;" ::"l"(bar) : "memory");
+            asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(bar + 1), "r"(gen + 1) : "memory");
         } else {
             long long spins = 0;
-            while (atomicAdd(&bar[1], 0u) == gen) {
-                if (++spins > kJacBarrierSpins || atomicAdd(&bar[2], 0u) != 0u) {
+            while (jac_ld_acquire(bar + 1) == gen) {
+                if (++spins > kJacBarrierSpins || jac_ld_relaxed(bar + 2) != 0u) {
                     atomicExch(&bar[2], 1u);
                     ok = 0;
                     break;
                 }
-                __nanosleep(64);
+                if (spins > 64) __nanosleep(32);
             }
         }
-        __threadfence();
-        s_ok = ok && atomicAdd(&bar[2], 0u) == 0;
+        s_ok = ok;
     }
     __syncthreads();
     ++gen;
@@ -823,6 +863,19 @@ jacobi_grid_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, doubl
     const int64_t blk0 = nblk * b / G, blk1 = nblk * (b + 1) / G;  // this CTA's share
     const int64_t nq = (int64_t)s * npair;                         // (row, pair) entries of Q
     const int64_t q0 = nq * b / G, q1 = nq * (b + 1) / G;
+    // the first block and Q entry of this thread, mapped once; later ones are reached by adding nt
+    // (the upper triangle has bj + 1 blocks in column bj; Q entries are (pair, row) with s rows)
+    int blk_bi0 = 0, blk_bj0 = 0;
+    if (blk0 + tid < blk1) {
+        const int64_t e = blk0 + tid;
+        int bj = (int)((sqrt(8.0 * (double)e + 1.0) - 1.0) * 0.5);
+        while ((int64_t)(bj + 1) * (bj + 2) / 2 <= e) ++bj;
+        while ((int64_t)bj * (bj + 1) / 2 > e) --bj;
+        blk_bj0 = bj;
+        blk_bi0 = (int)(e - (int64_t)bj * (bj + 1) / 2);
+    }
+    const int q_b0 = (int)((q0 + tid) / s), q_r0 = (int)((q0 + tid) - (int64_t)q_b0 * s);
+    const int q_db = nt / s, q_dr = nt - (nt / s) * s;
     ok = jac_grid_barrier(bar, G, gen);
     int sweep = 0;
     for (; ok && sweep < max_sweeps; ++sweep) {
@@ -875,12 +928,12 @@ jacobi_grid_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, doubl
             }
             __syncthreads();
             // this CTA's 2x2 blocks: linear index e over bj-major upper triangle (bi <= bj)
-            for (int64_t e = blk0 + tid; e < blk1; e += nt) {
-                // bj = largest with bj (bj + 1) / 2 <= e
-                int bj = (int)((sqrt(8.0 * (double)e + 1.0) - 1.0) * 0.5);
-                while ((int64_t)(bj + 1) * (bj + 2) / 2 <= e) ++bj;
-                while ((int64_t)bj * (bj + 1) / 2 > e) --bj;
-                const int bi = (int)(e - (int64_t)bj * (bj + 1) / 2);
+            int bi = blk_bi0, bj = blk_bj0;
+            for (int64_t e = blk0 + tid; e < blk1; e += nt, bi += nt) {
+                while (bi > bj) {  // step to the block nt further along the triangle
+                    bi -= bj + 1;
+                    ++bj;
+                }
                 const double si = rsn[bi], sj = rsn[bj];
                 const int pi = pp[bi], qi = qq[bi], pj = pp[bj], qj = qq[bj];
                 const int64_t o0 = pi + (int64_t)pj * ld, o1 = qi + (int64_t)pj * ld;
@@ -915,16 +968,23 @@ jacobi_grid_kernel(int s, const T* __restrict__ Ain, T* __restrict__ Qout, doubl
                 }
             }
             // this CTA's (row, pair) entries of Q <- Q G_j, rows fastest (coalesced columns)
+            int qb = q_b0, qr = q_r0;
             for (int64_t e = q0 + tid; e < q1; e += nt) {
-                const int bj = (int)(e / s), row = (int)(e - (int64_t)bj * s);
-                const double sj = rsn[bj];
-                if (sj == 0.0) continue;
-                T* qpp = Q + row + (int64_t)pp[bj] * ld;
-                T* qqp = Q + row + (int64_t)qq[bj] * ld;
-                T qp = __ldcg(qpp), qv = __ldcg(qqp);
-                jac_qrot<T>(qp, qv, rc[bj], sj, ru[bj]);
-                __stcg(qpp, qp);
-                __stcg(qqp, qv);
+                const double sj = rsn[qb];
+                if (sj != 0.0) {
+                    T* qpp = Q + qr + (int64_t)pp[qb] * ld;
+                    T* qqp = Q + qr + (int64_t)qq[qb] * ld;
+                    T qp = __ldcg(qpp), qv = __ldcg(qqp);
+                    jac_qrot<T>(qp, qv, rc[qb], sj, ru[qb]);
+                    __stcg(qpp, qp);
+                    __stcg(qqp, qv);
+                }
+                qr += q_dr;
+                qb += q_db;
+                if (qr >= s) {
+                    qr -= s;
+                    ++qb;
+                }
             }
             ok = jac_grid_barrier(bar, G, gen);
             par ^= 1;
