@@ -35,7 +35,7 @@ rm_step_kernel(Pol op, int64_t n, int nseg, int64_t ld, int groups, const TS* __
 // Degree step of the correction filter: y = alpha A x + beta x + gamma z + sig[c] src, with x, z,
 // y and src stored as TM (FP32, or bfloat16 with FP32 arithmetic).
 template <class Pol, class TS, class TC, int W, class IX, class TM>
-__global__ void __launch_bounds__(kRmThreads, rm_src_min_blocks<TM, IX>())
+__global__ void __launch_bounds__(kRmThreads, rm_src_min_blocks<TM, IX, W>())
 rm_step_src_kernel(Pol op, int64_t n, int nseg, int64_t ld, int groups, const TM* __restrict__ x, const TM* z, TM* y,
                    TC alpha, TC beta, TC gamma, int64_t pf_z, int64_t pf_x, const TM* __restrict__ src,
                    const float* __restrict__ sig) {
@@ -535,7 +535,7 @@ static rc_status run_rm_corr(rc_ctx* ctx, const Pol& pol, int64_t n, TV* V, int6
     const int nseg = (int)(ld / (VEC * W));
     if (nseg > kRmThreads) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "correction filter: block too wide");
     constexpr bool kCsr = Pol::kIsCsr;
-    const int groups = ctx->rm_groups > 0 ? ctx->rm_groups : (kCsr ? 4 : 8);
+    const int groups = ctx->rm_groups > 0 ? ctx->rm_groups : (kCsr ? (W > 1 ? 2 : 4) : 8);
     step_mark(ctx);
     // pairs of steps in one pass (rm_corr2_kernel) where the per-row kernels run; the 27-point stencil
     // and the staged kernel take one step per launch
@@ -650,6 +650,19 @@ static rc_status rm_corr_select(rc_ctx* ctx, const Pol& pol, int64_t n, TV* V, i
                                 int64_t degree, double a, double b, const TM* R, const float* sig,
                                 const double* coef, TM* A, TM* B, int64_t ld, int64_t band,
                                 const StageOffsets* so, const CorrRmOut& ro) {
+    // CSR operators with real bfloat16 blocks: RC_CORR_W 16-byte slices per thread when the padded
+    // width allows it. Measured on the 128^3 CSR operator with 96 columns (4 threads per row instead
+    // of 12, so each row's index data serve 24 columns per thread): the filter phase of the mixed
+    // solve 642-648 ms with 3 slices, 4 resident CTAs and 2 row groups per CTA, against 716-721 ms
+    // with 1 slice; 2, 4 and 6 slices were no faster.
+#ifndef RC_CORR_W
+#define RC_CORR_W 3
+#endif
+    if constexpr (RC_CORR_W > 1 && Pol::kIsCsr && std::is_same<TM, __nv_bfloat16>::value) {
+        if ((n + 1) * ld < ((int64_t)1 << 32) && ld % (Slice<TS, TM>::V * RC_CORR_W) == 0)
+            return run_rm_corr<Pol, TS, TS, RC_CORR_W, uint32_t, TM, TV>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig,
+                                                                         coef, A, B, ld, band, so, ro);
+    }
     if ((n + 1) * ld < ((int64_t)1 << 32))
         return run_rm_corr<Pol, TS, TS, 1, uint32_t, TM, TV>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A, B,
                                                              ld, band, so, ro);

@@ -187,10 +187,16 @@ constexpr int kRmThreads = 256;
 #define RC_RM_MIN_BLOCKS_SRC_BF16 0
 #endif
 // bfloat16 blocks (8 columns per thread, source coefficients re-read from L1): 6 resident CTAs
-// with 32-bit offsets, 5 with 64-bit offsets (which spill at 6), unless the build sets the count
-template <class TM, class IX>
+// with 32-bit offsets, 5 with 64-bit offsets (which spill at 6), unless the build sets the count.
+// Several 16-byte slices per thread (W > 1, the CSR correction step) need more registers: 4 CTAs
+// (64 registers), RC_RM_MIN_BLOCKS_SRC_WIDE.
+#ifndef RC_RM_MIN_BLOCKS_SRC_WIDE
+#define RC_RM_MIN_BLOCKS_SRC_WIDE 4
+#endif
+template <class TM, class IX, int W = 1>
 constexpr int rm_src_min_blocks() {
     return sizeof(TM) != 2               ? RC_RM_MIN_BLOCKS_SRC
+           : W > 1                       ? RC_RM_MIN_BLOCKS_SRC_WIDE
            : RC_RM_MIN_BLOCKS_SRC_BF16 > 0 ? RC_RM_MIN_BLOCKS_SRC_BF16
            : sizeof(IX) == 4             ? 6
                                          : 5;
