@@ -658,6 +658,20 @@ static rc_status rm_corr_select(rc_ctx* ctx, const Pol& pol, int64_t n, TV* V, i
 #ifndef RC_CORR_W
 #define RC_CORR_W 3
 #endif
+    // Complex blocks (bfloat16 pairs, 4 values per slice; CSR and 5/7-point stencils) likewise: on the
+    // 96^3 7-point tight-binding operator with 192 columns (16 threads per row instead of 48, and all
+    // 256 threads of a CTA busy instead of 240) the filter phase took 698-699 ms with 3 slices and 4
+    // resident CTAs, against 807-808 ms with 1 slice at 6, 734-736 ms with 3 slices at 3 and 831 ms
+    // with 2 slices at 4.
+#ifndef RC_CORR_W_CPLX
+#define RC_CORR_W_CPLX 3
+#endif
+    constexpr int kWc = std::is_same<TM, __nv_bfloat162>::value && !IsStencil27<Pol>::value ? RC_CORR_W_CPLX : 1;
+    if constexpr (kWc > 1) {
+        if ((n + 1) * ld < ((int64_t)1 << 32) && ld % (Slice<TS, TM>::V * kWc) == 0)
+            return run_rm_corr<Pol, TS, TS, kWc, uint32_t, TM, TV>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig, coef, A,
+                                                                   B, ld, band, so, ro);
+    }
     if constexpr (RC_CORR_W > 1 && Pol::kIsCsr && std::is_same<TM, __nv_bfloat16>::value) {
         if ((n + 1) * ld < ((int64_t)1 << 32) && ld % (Slice<TS, TM>::V * RC_CORR_W) == 0)
             return run_rm_corr<Pol, TS, TS, RC_CORR_W, uint32_t, TM, TV>(ctx, pol, n, V, ldv, s, degree, a, b, R, sig,

@@ -195,8 +195,8 @@ constexpr int kRmThreads = 256;
 #endif
 template <class TM, class IX, int W = 1>
 constexpr int rm_src_min_blocks() {
-    return sizeof(TM) != 2               ? RC_RM_MIN_BLOCKS_SRC
-           : W > 1                       ? RC_RM_MIN_BLOCKS_SRC_WIDE
+    return W > 1                         ? RC_RM_MIN_BLOCKS_SRC_WIDE
+           : sizeof(TM) != 2             ? RC_RM_MIN_BLOCKS_SRC
            : RC_RM_MIN_BLOCKS_SRC_BF16 > 0 ? RC_RM_MIN_BLOCKS_SRC_BF16
            : sizeof(IX) == 4             ? 6
                                          : 5;
