@@ -148,6 +148,7 @@ rc_status rc_ctx_create(int device, rc_ctx** out) {
     }
     if (const char* v = std::getenv("RCB200_RM_RR")) c->rm_rr = std::atoi(v) != 0 ? 1 : 0;
     if (const char* v = std::getenv("RCB200_GRAM_C")) c->gram_c = std::atoi(v) != 0 ? 1 : 0;
+    if (const char* v = std::getenv("RCB200_ROWS27W")) c->rows27w = std::atoi(v) != 0 ? 1 : 0;
     if (const char* v = std::getenv("RCB200_CORR_PAIR")) c->corr_pair = std::atoi(v) != 0 ? 1 : 0;
     if (const char* v = std::getenv("RCB200_STAGED_ROWS")) c->staged_rows = std::max(0, std::atoi(v) / 4 * 4);
     if (const char* v = std::getenv("RCB200_STAGED_STAGES")) c->staged_stages = std::max(0, std::min(4, std::atoi(v)));

@@ -129,6 +129,15 @@ rm_step27_kernel(StencilRows<TD, TC, 27> op, int64_t n, int nseg, int64_t ld, co
     rm_step_rows27<TD, TS, TC, W, IX, SRC, TM>(op, n, nseg, ld, kRun27, (int64_t)blockIdx.x, x, z, y, alpha, beta,
                                                gamma, pf_z, pf_x, src, sig);
 }
+// The same with the lanes of a warp on consecutive rows (rm_step_rows27w), for rows of at most
+// kMaxSeg27w slices (at least three rows per warp step).
+template <class TD, class TS, class TC, class IX, bool SRC, class TM>
+__global__ void __launch_bounds__(kRmThreads, RC_RM27_MIN_BLOCKS)
+rm_step27w_kernel(StencilRows<TD, TC, 27> op, int64_t n, int nseg, int64_t ld, const TM* __restrict__ x, const TM* z,
+                  TM* y, TC alpha, TC beta, TC gamma, int64_t pf_z, int64_t pf_x, const TM* __restrict__ src,
+                  const float* __restrict__ sig) {
+    rm_step_rows27w<TD, TS, TC, IX, SRC, TM>(op, n, nseg, ld, x, z, y, alpha, beta, gamma, pf_z, pf_x, src, sig);
+}
 
 // ---------------------------------------------------------------------------------------
 // The staged step (rc_staged.cuh): its plan and launch
@@ -319,6 +328,15 @@ static void launch_step(rc_ctx* ctx, const Pol& pol, int64_t n, int nseg, int64_
     const int rows_per_iter = kRmThreads / nseg;
     if constexpr (IsStencil27<Pol>::value) {
         using TD = typename IsStencil27<Pol>::diag_t;
+        if constexpr (W == 1) {
+            if (ctx->rows27w && nseg <= kMaxSeg27w && 32 / nseg >= 3) {
+                const int64_t rows_per_cta = (int64_t)(kRmThreads / 32) * (32 / nseg) * kSteps27w;
+                const unsigned grid = (unsigned)((n + rows_per_cta - 1) / rows_per_cta);
+                rm_step27w_kernel<TD, TS, TC, IX, SRC, TM><<<grid, kRmThreads, 0, ctx->stream>>>(
+                    pol, n, nseg, ld, x, z, y, a, b, g, pf_z, pf_x, src, sig);
+                return;
+            }
+        }
         const int64_t rows_per_cta = (int64_t)kRun27 * rows_per_iter;
         const unsigned grid = (unsigned)((n + rows_per_cta - 1) / rows_per_cta);
         rm_step27_kernel<TD, TS, TC, W, IX, SRC, TM><<<grid, kRmThreads, 0, ctx->stream>>>(pol, n, nseg, ld, x, z, y, a,

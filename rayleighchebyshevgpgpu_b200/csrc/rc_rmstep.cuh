@@ -501,6 +501,154 @@ template <class TD, class TC> struct IsStencil27<StencilRows<TD, TC, 27>> {
 };
 constexpr int kRun27 = 16;  // consecutive rows per thread in rm_step_rows27
 
+// The same 27-point step with the lanes of a warp on consecutive rows (rm_step27w_kernel), for rows
+// of at most kMaxSeg27w 16-byte slices. With RW = 32 / nseg rows per step, lane l < RW * nseg takes
+// slice l % nseg of row base + j * RW + l / nseg at step j, so one gather instruction of the warp
+// reads RW consecutive rows (RW * nseg * 16 contiguous bytes) instead of rows a run apart. Each lane
+// forms P = Q(row + 1), the cross-section sum of the next row with that row's boundary flags; row i
+// then takes Q(i+1) from its own P, Q(i) from the lane nseg below and Q(i-1) from the lane 2 nseg
+// below, by shuffles. The first two rows of a step take them from the last two rows of the previous
+// step, which the warp keeps in shared memory; before the first step the warp forms Q(base) and
+// Q(base - 1) itself. A warp walks kSteps27w steps (RW * kSteps27w consecutive rows), the warps of a
+// CTA consecutive runs. The sums and their order are rm_step_rows27's, so both give the same bits.
+constexpr int kMaxSeg27w = 10;
+constexpr int kSteps27w = 16;
+
+template <class TD, class TS, class TC, class IX, bool SRC, class TM = TS>
+__device__ __forceinline__ void rm_step_rows27w(const StencilRows<TD, TC, 27>& op, int64_t n, int nseg, int64_t ld,
+                                                const TM* __restrict__ x, const TM* z, TM* y, TC alpha, TC beta,
+                                                TC gamma, int64_t pf_z, int64_t pf_x, const TM* __restrict__ src,
+                                                const float* __restrict__ sig) {
+    static_assert(!IsComplex<TC>::value, "the 27-point stencil is real");
+    constexpr int V = Slice<TS, TM>::V;
+    __shared__ TC carry[kRmThreads / 32][2][kMaxSeg27w][V];  // [warp][0: Q(first-1), 1: Q(first)][slice]
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int RW = 32 / nseg;
+    const int rsub = lane / nseg, seg = lane - rsub * nseg;
+    const bool act = rsub < RW;
+    const IX off = (IX)seg * (IX)V;
+    const IX ldx = (IX)ld;
+    const int64_t nx = op.nx, ny = op.ny, nz = op.nz, sy = nx, sz = nx * ny;
+    const TC woff = s_from<TC>(op.offd, 0.0);
+    constexpr bool kSigReg = sizeof(TM) != 2;
+    TC sg[SRC && kSigReg ? V : 1];
+    if (SRC && kSigReg && act) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) sg[v] = s_from<TC>((double)__ldg(sig + off + v), 0.0);
+    }
+    // cross-section sum of row j (over its y, z neighbours; flags of row j) for this lane's slice
+    auto cross = [&](int64_t j, bool vym, bool vyp, bool vzm, bool vzp, TC (&q)[V]) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) q[v] = s_zero(TC());
+#pragma unroll
+        for (int dz = -1; dz <= 1; ++dz) {
+            const bool vz = dz < 0 ? vzm : (dz > 0 ? vzp : true);
+#pragma unroll
+            for (int dy = -1; dy <= 1; ++dy) {
+                const bool vy = dy < 0 ? vym : (dy > 0 ? vyp : true);
+                if (vz && vy) {
+                    const Slice<TS, TM> pk = ldv_ro<TS, TM>(x + ((IX)(j + dy * sy + dz * sz) * ldx + off));
+#pragma unroll
+                    for (int v = 0; v < V; ++v) q[v] = s_add(q[v], s_cvt<TC>(pk.v[v]));
+                }
+            }
+        }
+    };
+    auto cross_at = [&](int64_t j, TC (&q)[V]) {
+        int64_t jx, jy, jz;
+        op.coords(j, jx, jy, jz);
+        cross(j, jy > 0, jy + 1 < ny, jz > 0, jz + 1 < nz, q);
+    };
+    const int64_t base = ((int64_t)blockIdx.x * (kRmThreads / 32) + wib) * (int64_t)RW * kSteps27w;
+    if (base >= n) return;  // the whole warp
+    {
+        TC q[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) q[v] = s_zero(TC());
+        if (act && rsub == 0) cross_at(base, q);
+        if (act && rsub == 1 && base > 0) cross_at(base - 1, q);
+        if (act && rsub <= 1) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) carry[wib][1 - rsub][seg][v] = q[v];
+        }
+    }
+    __syncwarp();
+    const int l1 = lane >= nseg ? lane - nseg : lane;
+    const int l2 = lane >= 2 * nseg ? lane - 2 * nseg : lane;
+    for (int j = 0; j < kSteps27w; ++j) {
+        const int64_t row0 = base + (int64_t)j * RW;
+        if (row0 >= n) break;  // the whole warp
+        const int64_t i = row0 + rsub;
+        const bool live = act && i < n;
+        int64_t ix = 0, iy = 0, iz = 0;
+        TC P[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) P[v] = s_zero(TC());
+        if (live) {
+            op.coords(i, ix, iy, iz);
+            if (i + 1 < n) {
+                int64_t jy = iy, jz = iz;
+                if (ix + 1 == nx && ++jy == ny) {
+                    jy = 0;
+                    ++jz;
+                }
+                cross(i + 1, jy > 0, jy + 1 < ny, jz > 0, jz + 1 < nz, P);
+            }
+        }
+        TC q0[V], qm[V];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            q0[v] = __shfl_sync(0xffffffffu, P[v], l1);
+            qm[v] = __shfl_sync(0xffffffffu, P[v], l2);
+        }
+        if (rsub == 0 && act) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                q0[v] = carry[wib][1][seg][v];
+                qm[v] = carry[wib][0][seg][v];
+            }
+        } else if (rsub == 1 && act) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) qm[v] = carry[wib][1][seg][v];
+        }
+        __syncwarp();  // every lane has read the carries before they are replaced
+        if (act && rsub >= RW - 2) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) carry[wib][rsub - (RW - 2)][seg][v] = P[v];
+        }
+        __syncwarp();
+        if (!live) continue;
+        const IX oi = (IX)i * ldx + off;
+        if (pf_z > 0 && i + pf_z < n && ((off * (IX)sizeof(TM)) & 127) == 0) {
+            if (z) prefetch_l2(z + (IX)(i + pf_z) * ldx + off);
+            if (SRC) prefetch_l2(src + (IX)(i + pf_z) * ldx + off);
+            if (i + pf_x < n) prefetch_l2(x + (IX)(i + pf_x) * ldx + off);
+        }
+        const TC dmw = s_sub(s_from<TC>((double)op.diag[i], 0.0), woff);
+        const bool hm = ix > 0, hp = ix + 1 < nx;
+        const Slice<TS, TM> xi = ldv_ro<TS, TM>(x + oi);
+        Slice<TS, TM> zi{}, si{};
+        if (z) zi = ldv_once<TS, TM>(z + oi);
+        if (SRC) si = ldv_once<TS, TM>(src + oi);
+        Slice<TS, TM> out;
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const TC xv = s_cvt<TC>(xi.v[v]);
+            const TC qmv = hm ? qm[v] : s_zero(TC()), qpv = hp ? P[v] : s_zero(TC());
+            const TC ax = s_fma(woff, s_add(s_add(qmv, q0[v]), qpv), s_mul(dmw, xv));
+            TC r = s_mul(alpha, ax);
+            r = s_fma(beta, xv, r);
+            if (z) r = s_fma(gamma, s_cvt<TC>(zi.v[v]), r);
+            if (SRC) {
+                const TC sgv = kSigReg ? sg[kSigReg ? v : 0] : s_from<TC>((double)__ldg(sig + off + v), 0.0);
+                r = s_fma(sgv, s_cvt<TC>(si.v[v]), r);
+            }
+            out.v[v] = s_cvt<TS>(r);
+        }
+        stv_once<TS, TM>(y + oi, out);
+    }
+}
+
 // Layout change between the caller's column-major FP64 block and the row-major scratch, through
 // 32x32 shared-memory tiles (coalesced on both sides), converting precision and scaling.
 //   to_rm:  R[i*ld + c] = (TS) V[i + c*ldv]

@@ -241,3 +241,39 @@ def test_two_step_kernel_equals_one_step_launches_bitwise(name, m):
         c.close()
     assert np.array_equal(out[0], out[1])
     _check(A, Y, lam, rn, m, g1, g2, out[0])
+
+
+@pytest.mark.parametrize("dims", [(12, 11, 10), (33, 7, 5)])
+@pytest.mark.parametrize("s", [8, 24, 48, 80])
+def test_27_point_warp_rows_equal_thread_runs_bitwise(dims, s):
+    """The 27-point correction step with a warp's lanes on consecutive rows (cross-section sums of
+    neighbouring rows passed by shuffles) gives the same bits as the per-thread runs of 16 rows
+    (RCB200_ROWS27W=0): the same sums in the same order. Rows of 1, 3, 6 and 10 bfloat16 slices (32,
+    10, 5 and 3 rows per warp step), on grids whose x-lines and row counts do not divide the steps."""
+    import os
+    n = int(np.prod(dims))
+    rng = np.random.default_rng(s + n)
+    Q = problems.Problem("st27w", dims, 27, 1.0 + rng.uniform(0.0, 2.0, n), -1.0 / 26.0)
+    A = O.csr_matrix(*Q.csr())
+    X = rng.standard_normal((n, s))
+    Y, _ = np.linalg.qr(X)
+    H = Y.T @ (A @ Y)
+    lam, Qs = np.linalg.eigh(0.5 * (H + H.T))
+    Y = Y @ Qs
+    out = []
+    for flag in ("1", "0"):
+        old = os.environ.get("RCB200_ROWS27W")
+        os.environ["RCB200_ROWS27W"] = flag
+        try:
+            c = R.Context(0)
+        finally:
+            if old is None:
+                os.environ.pop("RCB200_ROWS27W", None)
+            else:
+                os.environ["RCB200_ROWS27W"] = old
+        op = R.operator_from_problem(c, Q, "stencil")
+        out.append(_gpu(c, op, Y, s, lam, 9, -0.3, 1.1))
+        op.close()
+        c.close()
+    assert np.all(np.isfinite(out[0]))
+    assert np.array_equal(out[0], out[1])
