@@ -68,9 +68,10 @@ struct rc_ctx {
     // consecutive row groups per CTA in the row-major filter steps: 0 = by operator kind and
     // storage precision, else 1..64. RCB200_RM_GROUPS.
     int rm_groups = 0;
-    // 27-point steps with a warp's lanes on consecutive rows (rm_step27w_kernel) for narrow rows: 1
-    // (default) or 0, from RCB200_ROWS27W.
-    int rows27w = 1;
+    // 27-point steps with a warp's lanes on consecutive rows (rm_step27w_kernel) for narrow rows: 1,
+    // or 0 (default: the per-thread runs, measured 1.7 % faster on the configuration-5 filter phase,
+    // 3792-3803 ms against 3856-3864 ms), from RCB200_ROWS27W.
+    int rows27w = 0;
     // Degree steps with their operands staged in shared memory (rc_staged.cuh) for
     // stencil-structured operators: 1, or 0 (default: the per-row gather kernels, measured faster
     // on the 128^3 workloads), from RCB200_STAGED.
