@@ -499,7 +499,14 @@ template <class TD, class TC> struct IsStencil27<StencilRows<TD, TC, 27>> {
     static constexpr bool value = true;
     using diag_t = TD;
 };
-constexpr int kRun27 = 16;  // consecutive rows per thread in rm_step_rows27
+// Consecutive rows per thread in rm_step_rows27 (and the 27-point residual walk). A run starts with
+// two extra cross-section sums, so longer runs gather less; the values do not depend on it. Measured
+// on the 256^3 27-point stencil with 48 columns (mixed solve): filter phase 3775 / 3633 / 3509 ms and
+// Rayleigh-Ritz phase 4951 / 4553 / 4382 ms for runs of 16 / 32 / 64 rows.
+#ifndef RC_RUN27
+#define RC_RUN27 64
+#endif
+constexpr int kRun27 = RC_RUN27;
 
 // The same 27-point step with the lanes of a warp on consecutive rows (rm_step27w_kernel), for rows
 // of at most kMaxSeg27w 16-byte slices. With RW = 32 / nseg rows per step, lane l < RW * nseg takes
