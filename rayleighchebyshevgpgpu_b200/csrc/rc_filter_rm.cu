@@ -553,7 +553,10 @@ static rc_status run_rm_corr(rc_ctx* ctx, const Pol& pol, int64_t n, TV* V, int6
     const int nseg = (int)(ld / (VEC * W));
     if (nseg > kRmThreads) return rc_fail(ctx, RC_ERR_UNSUPPORTED, "correction filter: block too wide");
     constexpr bool kCsr = Pol::kIsCsr;
-    const int groups = ctx->rm_groups > 0 ? ctx->rm_groups : (kCsr ? (W > 1 ? 2 : 4) : 8);
+    // row groups per CTA: 2 with several slices per thread (configuration 2, CSR: filter phase 642-648 ms
+    // against 658-665 ms with 4; configuration 3, complex stencil: 624 ms against 637 ms with 4 and 698 ms
+    // with 8), else 4 for CSR and 8 for stencils
+    const int groups = ctx->rm_groups > 0 ? ctx->rm_groups : (W > 1 ? 2 : (kCsr ? 4 : 8));
     step_mark(ctx);
     // pairs of steps in one pass (rm_corr2_kernel) where the per-row kernels run; the 27-point stencil
     // and the staged kernel take one step per launch
